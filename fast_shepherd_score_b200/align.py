@@ -1,0 +1,422 @@
+"""Alignment drivers of the CUDA backend.
+
+:func:`align_packed` is the core: one fused persistent kernel runs every (pair, start)
+pose through all Adam steps (``fss_align``).  The ``coarse_fine_*_align_many`` functions
+keep the signatures and return values of the reference drivers and route to it:
+
+* :func:`coarse_fine_align_many`          (shepherd_score/accel/drivers/shape.py:155-313)
+* :func:`coarse_fine_esp_align_many`      (accel/drivers/esp.py:139-367)
+* :func:`coarse_fine_pharm_align_many`    (accel/drivers/pharm.py:123-517)
+* :func:`coarse_fine_vol_color_align_many`(accel/drivers/vol_color.py:199-518)
+* :func:`coarse_fine_vol_pharm_align_many` -- shape + *directional* pharmacophore with one
+  shared pose (the combination the reference offers only per pair,
+  alignment/_torch.py:1376 ``optimize_vol_color_overlay(directionless=False)``).
+
+Early stop: the fused kernel always runs the full ``steps_fine`` (the reference's early
+stop is batch-global, which makes a pair's result depend on the other pairs of its
+batch; running every step can only raise a pose's running-max best score).  The
+``early_stop_*`` arguments are accepted for signature compatibility.
+
+Two more drivers exist for comparison and for callers that want per-step control:
+:class:`GraphedFineLoop` (per-step kernels captured in one CUDA graph and replayed, the
+reference's ``_graphed.py`` structure) and :func:`align_one_pair_per_launch` (the plain
+form: one overlap launch + one Adam launch per pair per step).
+"""
+from __future__ import annotations
+
+import math
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _lib, kernels
+from ._lib import AlignDesc, check, ptr, stream_ptr
+from .layout import CloudSet, PharmSet, cost_order
+
+_f32, _i32 = torch.float32, torch.int32
+LAM_SCALING = (1e4 / (4 * 55.263 * math.pi)) ** 2   # score/constants.py:16-17
+
+MODE_IDS = {"shape": _lib.MODE_SHAPE, "esp": _lib.MODE_ESP, "pharm": _lib.MODE_PHARM,
+            "shape_pharm": _lib.MODE_SHAPE_PHARM, "shape_color": _lib.MODE_SHAPE_COLOR}
+
+_SCRATCH: dict = {}
+
+
+def _scratch(device) -> torch.Tensor:
+    """Per-device 2-int32 scratch (work counter + status) reused by every launch on it."""
+    key = torch.device(device).index
+    s = _SCRATCH.get(key)
+    if s is None:
+        s = torch.zeros(2, dtype=_i32, device=device)
+        _SCRATCH[key] = s
+    return s
+
+
+class AlignResult(tuple):
+    """(score (P,), q (P,4), t (P,3)) plus optional per-row results in ``.rows``."""
+    rows: Optional[tuple] = None
+
+
+def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, lr: float,
+                 ref: Optional[CloudSet] = None, fit: Optional[CloudSet] = None,
+                 ref_ph: Optional[PharmSet] = None, fit_ph: Optional[PharmSet] = None,
+                 alpha: float = 0.81, lam: Optional[float] = None, color_weight: float = 0.5,
+                 ref_self=None, fit_self=None, ref_self_ph=None, fit_self_ph=None,
+                 order=None, lanes_per_pose: int = 0, chunks: int = 0, cta_per_sm: int = 0,
+                 rows=None, out=None, scratch=None, check_status: bool = True):
+    """Run the fused alignment kernel over packed clouds.
+
+    ``mode`` in {"shape", "esp", "pharm", "shape_pharm", "shape_color"}.  ``seed_q``/``seed_t``
+    are (P,S,4)/(P,S,3).  Returns (score, q, t) per pair; ``rows`` (if given, a tuple of
+    (P*S,), (P*S,4), (P*S,3) tensors) receives every start's best score and pose.
+    Self overlaps default to the kernels' own (:func:`kernels.self_overlap`).
+    """
+    m = MODE_IDS[mode]
+    shape = m != _lib.MODE_PHARM
+    pharm = m in (_lib.MODE_PHARM, _lib.MODE_SHAPE_PHARM, _lib.MODE_SHAPE_COLOR)
+    directional = m in (_lib.MODE_PHARM, _lib.MODE_SHAPE_PHARM)
+    dev = seed_q.device
+    P, S = int(seed_q.shape[0]), int(seed_q.shape[1])
+    if shape and (ref is None or fit is None):
+        raise ValueError(f"mode {mode!r} needs ref and fit clouds")
+    if pharm and (ref_ph is None or fit_ph is None):
+        raise ValueError(f"mode {mode!r} needs ref and fit pharmacophores")
+    if m == _lib.MODE_ESP and lam is None:
+        raise ValueError("esp mode needs lam")
+    pair_ref = torch.as_tensor(pair_ref, device=dev).to(_i32).contiguous()
+    pair_fit = torch.as_tensor(pair_fit, device=dev).to(_i32).contiguous()
+    seed_q = seed_q.to(_f32).contiguous()
+    seed_t = seed_t.to(_f32).contiguous()
+    if pair_ref.shape != (P,) or pair_fit.shape != (P,) or tuple(seed_t.shape) != (P, S, 3) \
+            or tuple(seed_q.shape) != (P, S, 4):
+        raise ValueError("pair_ref/pair_fit must be (P,), seeds (P,S,4) and (P,S,3)")
+    n_ref = ref.n_mol if shape else ref_ph.n_mol
+    n_fit = fit.n_mol if shape else fit_ph.n_mol
+    if shape and pharm and (ref_ph.n_mol != n_ref or fit_ph.n_mol != n_fit):
+        raise ValueError("shape and pharmacophore sets must describe the same molecules")
+    if P:
+        lo = int(torch.minimum(pair_ref.min(), pair_fit.min()))
+        if lo < 0 or int(pair_ref.max()) >= n_ref or int(pair_fit.max()) >= n_fit:
+            raise ValueError("pair index outside the molecule tables")
+    if shape:
+        if ref_self is None:
+            ref_self = kernels.self_overlap(ref, alpha, m == _lib.MODE_ESP, lam)
+        if fit_self is None:
+            fit_self = kernels.self_overlap(fit, alpha, m == _lib.MODE_ESP, lam)
+    if pharm:
+        if m == _lib.MODE_PHARM:
+            if ref_self is None:
+                ref_self = kernels.pharm_self_overlap(ref_ph, directional)
+            if fit_self is None:
+                fit_self = kernels.pharm_self_overlap(fit_ph, directional)
+        else:
+            if ref_self_ph is None:
+                ref_self_ph = kernels.pharm_self_overlap(ref_ph, directional)
+            if fit_self_ph is None:
+                fit_self_ph = kernels.pharm_self_overlap(fit_ph, directional)
+    if order is None and P > 1:
+        pr = pair_ref.cpu().numpy()
+        pf = pair_fit.cpu().numpy()
+        if shape:
+            order = cost_order(ref.counts[pr], fit.counts[pf], dev)
+        else:
+            order = cost_order(ref_ph.counts[pr], fit_ph.counts[pf], dev)
+    if rows is None:
+        rows = (torch.empty(P * S, dtype=_f32, device=dev),
+                torch.empty(P * S, 4, dtype=_f32, device=dev),
+                torch.empty(P * S, 3, dtype=_f32, device=dev))
+    if out is None:
+        out = (torch.empty(P, dtype=_f32, device=dev), torch.empty(P, 4, dtype=_f32, device=dev),
+               torch.empty(P, 3, dtype=_f32, device=dev))
+    scratch = _scratch(dev) if scratch is None else scratch
+    d = AlignDesc()
+    d.mode, d.n_pairs, d.n_starts, d.steps = m, P, S, int(steps)
+    d.pair_ref, d.pair_fit = ptr(pair_ref, _i32), ptr(pair_fit, _i32)
+    d.order = ptr(order, _i32) if order is not None else None
+    if shape:
+        d.ref_pts, d.ref_off = ptr(ref.pts, _f32), ptr(ref.off, _i32)
+        d.fit_pts, d.fit_off = ptr(fit.pts, _f32), ptr(fit.off, _i32)
+        d.max_ref_points, d.max_fit_points = ref.max_points, fit.max_points
+    if pharm:
+        d.ref_anc, d.ref_ph_off = ptr(ref_ph.anc, _f32), ptr(ref_ph.off, _i32)
+        d.fit_anc, d.fit_ph_off = ptr(fit_ph.anc, _f32), ptr(fit_ph.off, _i32)
+        if directional:
+            d.ref_vec, d.fit_vec = ptr(ref_ph.vec, _f32), ptr(fit_ph.vec, _f32)
+        d.max_ref_features, d.max_fit_features = ref_ph.max_points, fit_ph.max_points
+        d.ref_self_ph = ptr(ref_self_ph, _f32) if ref_self_ph is not None else None
+        d.fit_self_ph = ptr(fit_self_ph, _f32) if fit_self_ph is not None else None
+    d.ref_self, d.fit_self = ptr(ref_self, _f32), ptr(fit_self, _f32)
+    d.seed_q, d.seed_t = ptr(seed_q, _f32), ptr(seed_t, _f32)
+    d.alpha = float(alpha)
+    d.inv_lam = 1.0 / float(lam) if (m == _lib.MODE_ESP) else 0.0
+    d.color_weight = float(color_weight)
+    d.lr = float(lr)
+    d.row_score, d.row_q, d.row_t = (ptr(rows[0], _f32), ptr(rows[1], _f32), ptr(rows[2], _f32))
+    d.out_score, d.out_q, d.out_t = (ptr(out[0], _f32), ptr(out[1], _f32), ptr(out[2], _f32))
+    d.lanes_per_pose, d.chunks, d.cta_per_sm = int(lanes_per_pose), int(chunks), int(cta_per_sm)
+    d.scratch = ptr(scratch, _i32)
+    check(_lib.load().fss_align(d, stream_ptr(dev)), f"align[{mode}]")
+    if check_status:
+        status = int(scratch[1].item())
+        if status:
+            raise RuntimeError(f"align[{mode}]: a pair exceeded the staged extents (status {status})")
+    res = AlignResult(out)
+    res.rows = rows
+    return res
+
+
+# ------------------------------------------------------------------------------------------
+# Reference-signature drivers (padded batches in, per-pair best out)
+# ------------------------------------------------------------------------------------------
+def _self_pairs(K, dev):
+    idx = torch.arange(K, dtype=_i32, device=dev)
+    return idx, idx
+
+
+def _default_counts(x, K, pad, dev):
+    if x is None:
+        return torch.full((K,), pad, dtype=torch.int64, device=dev)
+    return torch.as_tensor(x, device=dev).to(torch.int64)
+
+
+def coarse_fine_align_many(A_batch, B_batch, VAA, VBB, *, alpha: float = 0.81,
+                           num_seeds: int = 50, steps_fine: int = 100, lr: float = 0.075,
+                           N_real=None, M_real=None, early_stop_patience: int = 2,
+                           early_stop_tol: float = 1e-5, seeds: Optional[tuple] = None,
+                           prune_after: int = 0, prune_keep: int = 0, **tile):
+    """Batched shape alignment (vol / surf); returns (score (B,), q (B,4), t (B,3))."""
+    K, npad, _ = A_batch.shape
+    dev = A_batch.device
+    N_real = _default_counts(N_real, K, npad, dev)
+    M_real = _default_counts(M_real, K, B_batch.shape[1], dev)
+    ref = CloudSet.from_padded(A_batch, N_real)
+    fit = CloudSet.from_padded(B_batch, M_real)
+    pr, pf = _self_pairs(K, dev)
+    if seeds is None:
+        seeds = kernels.seeds(ref, fit, pr, pf, num_seeds)
+    return align_packed("shape", ref=ref, fit=fit, pair_ref=pr, pair_fit=pf, seed_q=seeds[0],
+                        seed_t=seeds[1], steps=steps_fine, lr=lr, alpha=alpha,
+                        ref_self=VAA.to(_f32).contiguous(), fit_self=VBB.to(_f32).contiguous(),
+                        **tile)
+
+
+def coarse_fine_esp_align_many(A_batch, B_batch, CA_batch, CB_batch, VAA, VBB, *,
+                               alpha: float = 0.81, lam: float = 0.3, num_seeds: int = 50,
+                               trans_centers=None, trans_centers_real=None,
+                               num_repeats_per_trans: int = 10, topk: int = 30,
+                               steps_fine: int = 100, lr: float = 0.075, N_real=None,
+                               M_real=None, early_stop_patience: int = 5,
+                               early_stop_tol: float = 1e-5, seeds: Optional[tuple] = None,
+                               **tile):
+    """Batched ESP alignment; ``lam`` is the kernel lambda (LAM_SCALING*lam for surfaces)."""
+    if trans_centers is not None:
+        raise NotImplementedError("trans_init (coarse translation grid) is not part of the "
+                                  "CUDA backend; use the reference backend for it")
+    K, npad, _ = A_batch.shape
+    dev = A_batch.device
+    N_real = _default_counts(N_real, K, npad, dev)
+    M_real = _default_counts(M_real, K, B_batch.shape[1], dev)
+    ref = CloudSet.from_padded(A_batch, N_real, CA_batch)
+    fit = CloudSet.from_padded(B_batch, M_real, CB_batch)
+    pr, pf = _self_pairs(K, dev)
+    if seeds is None:
+        seeds = kernels.seeds(ref, fit, pr, pf, num_seeds)
+    return align_packed("esp", ref=ref, fit=fit, pair_ref=pr, pair_fit=pf, seed_q=seeds[0],
+                        seed_t=seeds[1], steps=steps_fine, lr=lr, alpha=alpha, lam=lam,
+                        ref_self=VAA.to(_f32).contiguous(), fit_self=VBB.to(_f32).contiguous(),
+                        **tile)
+
+
+def _centroids(X, n):
+    K, npad, _ = X.shape
+    mask = (torch.arange(npad, device=X.device)[None] < n[:, None]).to(X.dtype)
+    return (X * mask.unsqueeze(-1)).sum(1) / n.clamp(min=1).to(X.dtype).unsqueeze(-1)
+
+
+def _quat_rot(q):
+    q = torch.nn.functional.normalize(q, dim=-1)
+    w, x, y, z = q.unbind(-1)
+    return torch.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w),
+                        2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w),
+                        2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)],
+                       -1).reshape(q.shape[:-1] + (3, 3))
+
+
+def coarse_fine_pharm_align_many(anchors_1, anchors_2, vectors_1, vectors_2, types_1, types_2,
+                                 VAA=None, VBB=None, *, similarity: str = "tanimoto",
+                                 extended_points: bool = False, only_extended: bool = False,
+                                 num_seeds: int = 50, trans_centers=None,
+                                 trans_centers_real=None, num_repeats_per_trans: int = 10,
+                                 topk: int = 30, steps_fine: int = 100, lr: float = 0.075,
+                                 N_real=None, M_real=None, early_stop_patience: int = 5,
+                                 early_stop_tol: float = 1e-5, seeds: Optional[tuple] = None,
+                                 **tile):
+    """Batched directional pharmacophore alignment (Tanimoto).
+
+    Clouds are centred on their own centroids first and the translation folded back at the
+    end, as the reference does (pharm.py:205-225, :509-517).  ``seeds`` (if given) are for
+    the centred clouds.  VAA/VBB are recomputed by the kernel, as in the reference kernel path.
+    """
+    if similarity != "tanimoto" or extended_points or only_extended:
+        raise NotImplementedError("the CUDA pharm path implements similarity='tanimoto' "
+                                  "without extended points")
+    if trans_centers is not None:
+        raise NotImplementedError("trans_init is not part of the CUDA backend")
+    K, npad, _ = anchors_1.shape
+    dev = anchors_1.device
+    N_real = _default_counts(N_real, K, npad, dev)
+    M_real = _default_counts(M_real, K, anchors_2.shape[1], dev)
+    a1 = anchors_1.to(_f32)
+    a2 = anchors_2.to(_f32)
+    c_ref = _centroids(a1, N_real)
+    c_fit = _centroids(a2, M_real)
+    a1c = a1 - c_ref[:, None, :]
+    a2c = a2 - c_fit[:, None, :]
+    ref_ph = PharmSet.from_padded(a1c, types_1, vectors_1, N_real)
+    fit_ph = PharmSet.from_padded(a2c, types_2, vectors_2, M_real)
+    pr, pf = _self_pairs(K, dev)
+    if seeds is None:
+        seeds = kernels.seeds(CloudSet.from_padded(a1c, N_real),
+                              CloudSet.from_padded(a2c, M_real), pr, pf, num_seeds)
+    sc, q, t = align_packed("pharm", ref_ph=ref_ph, fit_ph=fit_ph, pair_ref=pr, pair_fit=pf,
+                            seed_q=seeds[0], seed_t=seeds[1], steps=steps_fine, lr=lr, **tile)
+    R = _quat_rot(q)
+    t = t - torch.einsum('bij,bj->bi', R, c_fit) + c_ref
+    return sc, q, t
+
+
+def coarse_fine_vol_color_align_many(centers_1, centers_2, ptype_1, ptype_2, anchors_1,
+                                     anchors_2, VAA, VBB, *, alpha: float = 0.81,
+                                     color_weight: float = 0.5, num_seeds: int = 50,
+                                     trans_centers=None, trans_centers_real=None,
+                                     num_repeats_per_trans: int = 10, topk: int = 30,
+                                     steps_fine: int = 100, lr: float = 0.075,
+                                     N_real_centers=None, M_real_centers=None,
+                                     N_real_pharm=None, M_real_pharm=None,
+                                     early_stop_patience: int = 2, early_stop_tol: float = 1e-5,
+                                     seeds: Optional[tuple] = None, vectors_1=None,
+                                     vectors_2=None, directional: bool = False, **tile):
+    """Shape + pharmacophore alignment with the joint gradient of the two Tanimotos.
+
+    ``directional=False`` is the reference vol_color mode (directionless colour);
+    ``directional=True`` weights same-type pairs by the vector cosine (needs vectors).
+    """
+    if trans_centers is not None:
+        raise NotImplementedError("trans_init is not part of the CUDA backend")
+    K = centers_1.shape[0]
+    dev = centers_1.device
+    Nc = _default_counts(N_real_centers, K, centers_1.shape[1], dev)
+    Mc = _default_counts(M_real_centers, K, centers_2.shape[1], dev)
+    Np = _default_counts(N_real_pharm, K, anchors_1.shape[1], dev)
+    Mp = _default_counts(M_real_pharm, K, anchors_2.shape[1], dev)
+    ref = CloudSet.from_padded(centers_1, Nc)
+    fit = CloudSet.from_padded(centers_2, Mc)
+    ref_ph = PharmSet.from_padded(anchors_1, ptype_1, vectors_1 if directional else None, Np)
+    fit_ph = PharmSet.from_padded(anchors_2, ptype_2, vectors_2 if directional else None, Mp)
+    pr, pf = _self_pairs(K, dev)
+    if seeds is None:
+        seeds = kernels.seeds(ref, fit, pr, pf, num_seeds)
+    return align_packed("shape_pharm" if directional else "shape_color", ref=ref, fit=fit,
+                        ref_ph=ref_ph, fit_ph=fit_ph, pair_ref=pr, pair_fit=pf,
+                        seed_q=seeds[0], seed_t=seeds[1], steps=steps_fine, lr=lr, alpha=alpha,
+                        color_weight=color_weight, ref_self=VAA.to(_f32).contiguous(),
+                        fit_self=VBB.to(_f32).contiguous(), **tile)
+
+
+def coarse_fine_vol_pharm_align_many(centers_1, centers_2, ptype_1, ptype_2, anchors_1,
+                                     anchors_2, vectors_1, vectors_2, VAA, VBB, **kw):
+    """Shape + directional pharmacophore combined alignment (cosine-weighted typed overlap)."""
+    return coarse_fine_vol_color_align_many(centers_1, centers_2, ptype_1, ptype_2, anchors_1,
+                                            anchors_2, VAA, VBB, vectors_1=vectors_1,
+                                            vectors_2=vectors_2, directional=True, **kw)
+
+
+# ------------------------------------------------------------------------------------------
+# Step-by-step drivers (comparison forms)
+# ------------------------------------------------------------------------------------------
+class GraphedFineLoop:
+    """Per-step shape/ESP fine loop captured once in a CUDA graph and replayed ``steps``
+    times (the structure of the reference's accel/drivers/_graphed.py): every step launches
+    the single-evaluation overlap kernel over all pose rows and the Tanimoto/Adam kernel.
+    Rows are the reference's padded per-start expansion (K = pairs x starts)."""
+
+    def __init__(self, A_k, B_k, N_k, M_k, U, q_seed, t_seed, *, alpha, lr, CA_k=None,
+                 CB_k=None, lam=None):
+        self.A, self.B = A_k.contiguous(), B_k.contiguous()
+        self.CA = None if CA_k is None else CA_k.contiguous()
+        self.CB = None if CB_k is None else CB_k.contiguous()
+        self.N, self.M = N_k.to(_i32).contiguous(), M_k.to(_i32).contiguous()
+        self.U = U.to(_f32).contiguous()
+        self.qs, self.ts = q_seed.contiguous(), t_seed.contiguous()
+        self.alpha, self.lr, self.lam = float(alpha), float(lr), lam
+        K = self.qs.shape[0]
+        dev = self.qs.device
+        f = lambda *s: torch.empty(*s, dtype=_f32, device=dev)
+        self.q, self.t = f(K, 4), f(K, 3)
+        self.mq, self.vq, self.mt, self.vt = f(K, 4), f(K, 4), f(K, 3), f(K, 3)
+        self.best, self.bq, self.bt = f(K), f(K, 4), f(K, 3)
+        self.V, self.dQ, self.dT = f(K), f(K, 4), f(K, 3)
+        self.graph = None
+
+    def _reset(self):
+        self.q.copy_(self.qs); self.t.copy_(self.ts)
+        for b in (self.mq, self.vq, self.mt, self.vt):
+            b.zero_()
+        self.best.fill_(-float("inf")); self.bq.copy_(self.qs); self.bt.copy_(self.ts)
+
+    def _step(self):
+        L = _lib.load()
+        K, npad, _ = self.A.shape
+        st = stream_ptr(self.A.device)
+        inv_lam = 0.0 if self.CA is None else 1.0 / float(self.lam)
+        check(L.fss_overlap_grad(ptr(self.A), ptr(self.B), ptr(self.CA), ptr(self.CB),
+                                 ptr(self.q), ptr(self.t), ptr(self.N), ptr(self.M), K, npad,
+                                 self.B.shape[1], self.alpha, inv_lam, 1, ptr(self.V),
+                                 ptr(self.dQ), ptr(self.dT), st), "graph step overlap")
+        check(L.fss_tanimoto_adam_step(ptr(self.V), ptr(self.dQ), ptr(self.dT), ptr(self.U),
+                                       ptr(self.q), ptr(self.t), ptr(self.mq), ptr(self.vq),
+                                       ptr(self.mt), ptr(self.vt), ptr(self.best), ptr(self.bq),
+                                       ptr(self.bt), K, self.lr, st), "graph step adam")
+
+    def capture(self):
+        self._reset()
+        s = torch.cuda.Stream(self.A.device)
+        s.wait_stream(torch.cuda.current_stream(self.A.device))
+        with torch.cuda.stream(s):
+            self._step()  # warm-up (sets the kernels' shared-memory attributes)
+        torch.cuda.current_stream(self.A.device).wait_stream(s)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self._step()
+        return self
+
+    def run(self, steps: int):
+        if self.graph is None:
+            self.capture()
+        self._reset()
+        for _ in range(int(steps)):
+            self.graph.replay()
+        return self.best, self.bq, self.bt
+
+
+def align_one_pair_per_launch(A, B, n, m, U, q_seed, t_seed, *, steps, alpha, lr, CA=None,
+                              CB=None, lam=None):
+    """The plain comparator: one pair at a time, two launches per Adam step (overlap over
+    the pair's S start rows, then the Tanimoto/Adam kernel).  A (N,3), B (M,3) of ONE pair,
+    q_seed (S,4), t_seed (S,3); returns that pair's per-start best score and pose."""
+    S = q_seed.shape[0]
+    dev = q_seed.device
+    A_k = A.to(_f32).expand(S, -1, -1).contiguous()
+    B_k = B.to(_f32).expand(S, -1, -1).contiguous()
+    CA_k = None if CA is None else CA.to(_f32).expand(S, -1).contiguous()
+    CB_k = None if CB is None else CB.to(_f32).expand(S, -1).contiguous()
+    N_k = torch.full((S,), int(n), dtype=_i32, device=dev)
+    M_k = torch.full((S,), int(m), dtype=_i32, device=dev)
+    U_k = torch.full((S,), float(U), dtype=_f32, device=dev)
+    loop = GraphedFineLoop(A_k, B_k, N_k, M_k, U_k, q_seed, t_seed, alpha=alpha, lr=lr,
+                           CA_k=CA_k, CB_k=CB_k, lam=lam)
+    loop._reset()
+    for _ in range(int(steps)):
+        loop._step()
+    return loop.best, loop.bq, loop.bt

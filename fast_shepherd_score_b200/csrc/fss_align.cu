@@ -1,0 +1,446 @@
+// fss_align.cu -- the fused persistent alignment kernel and its helpers.
+//
+// One launch runs every (pair, start) pose for all Adam steps.  Work item = (pair, block
+// of starts); a persistent grid pulls items from a device counter in cost order (costliest
+// pairs first), stages the pair's clouds in shared memory once and keeps every pose's
+// optimiser state in registers for the whole loop.  LPP lanes cooperate on one pose; the
+// poses of one CTA all belong to the same pair so the shared-memory reads of the reference
+// cloud are warp-wide broadcasts and every loop bound is uniform.
+#include <algorithm>
+#include <cmath>
+
+#include "fss_internal.cuh"
+
+namespace fss {
+
+struct AlignParams {
+  int mode, n_pairs, n_starts, steps, chunks, n_items;
+  int maxN, maxM, maxNp, maxMp;
+  const int* pair_ref;
+  const int* pair_fit;
+  const int* order;
+  const float4* ref_pts; const int* ref_off;
+  const float4* fit_pts; const int* fit_off;
+  const float* ref_self; const float* fit_self;
+  const float4* ref_anc; const float4* ref_vec; const int* ref_ph_off;
+  const float4* fit_anc; const float4* fit_vec; const int* fit_ph_off;
+  const float* ref_self_ph; const float* fit_self_ph;
+  const float* seed_q; const float* seed_t;
+  float alpha, k, e, inv2k, Kc, aKc, w, lr;
+  PharmTables tab;
+  float* row_score; float* row_q; float* row_t;
+  int* counter;
+};
+
+constexpr int kMaxThreads = 512;
+
+template <int LPP, int MODE>
+__global__ void __launch_bounds__(kMaxThreads) align_kernel(const AlignParams p) {
+  constexpr bool kShape = MODE == FSS_MODE_SHAPE || MODE == FSS_MODE_ESP ||
+                          MODE == FSS_MODE_SHAPE_PHARM || MODE == FSS_MODE_SHAPE_COLOR;
+  constexpr bool kEsp = MODE == FSS_MODE_ESP;
+  constexpr bool kPharm = MODE == FSS_MODE_PHARM || MODE == FSS_MODE_SHAPE_PHARM ||
+                          MODE == FSS_MODE_SHAPE_COLOR;
+  extern __shared__ __align__(16) float4 smem[];
+  float4* sP = smem;
+  float4* sB = sP + p.maxN;
+  float4* sRA = sB + p.maxM;
+  float4* sRV = sRA + p.maxNp;
+  float4* sFA = sRV + p.maxNp;
+  float4* sFV = sFA + p.maxMp;
+  float* sQc = reinterpret_cast<float*>(sFV + p.maxMp);
+  __shared__ float red[96];
+  __shared__ int s_item;
+
+  const int tid = threadIdx.x;
+  const int grp = tid / LPP, lane = tid % LPP;
+  const int ppc = blockDim.x / LPP;  // poses per CTA
+  constexpr int kGroupsPerWarp = 32 / LPP;
+
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(p.counter, 1);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= p.n_items) break;
+    const int pidx = p.order ? p.order[item / p.chunks] : item / p.chunks;
+    const int chunk = item % p.chunks;
+    const int ri = p.pair_ref[pidx], fi = p.pair_fit[pidx];
+
+    // ---- stage the pair's clouds -------------------------------------------------------
+    int N = 0, M = 0, Np = 0, Mp = 0, r0 = 0, f0 = 0, rp0 = 0, fp0 = 0;
+    if (kShape) {
+      r0 = p.ref_off[ri]; f0 = p.fit_off[fi];
+      N = p.ref_off[ri + 1] - r0;
+      M = p.fit_off[fi + 1] - f0;
+    }
+    if (kPharm) {
+      rp0 = p.ref_ph_off[ri]; fp0 = p.fit_ph_off[fi];
+      Np = p.ref_ph_off[ri + 1] - rp0;
+      Mp = p.fit_ph_off[fi + 1] - fp0;
+    }
+    if (N < 0 || M < 0 || Np < 0 || Mp < 0 || N > p.maxN || M > p.maxM || Np > p.maxNp ||
+        Mp > p.maxMp) {
+      // larger than the tiles this launch was sized for: flag it, leave its rows untouched
+      if (tid == 0) atomicOr(p.counter + 1, 1);
+      __syncthreads();
+      continue;
+    }
+    float3 c = make_float3(0.f, 0.f, 0.f);
+    if (kShape) {
+      c = block_centroid(p.ref_pts + r0, N, red);
+      stage_ref<kEsp>(p.ref_pts + r0, N, c, p.k, p.e, sP, sQc);
+      stage_copy(p.fit_pts + f0, M, sB);
+    }
+    if (kPharm) {
+      if (!kShape) c = block_centroid(p.ref_anc + rp0, Np, red);
+      stage_ref_pharm(p.ref_anc + rp0, p.ref_vec ? p.ref_vec + rp0 : nullptr, Np, c, sRA, sRV);
+      stage_fit_pharm(p.fit_anc + fp0, p.fit_vec ? p.fit_vec + fp0 : nullptr, Mp, sFA, sFV);
+    }
+    __syncthreads();
+
+    const float Us = p.ref_self[ri] + p.fit_self[fi];
+    const float Uc = kShape && kPharm ? p.ref_self_ph[ri] + p.fit_self_ph[fi] : 0.f;
+    const int start = chunk * ppc + grp;
+    const int warp_first = chunk * ppc + (tid >> 5) * kGroupsPerWarp;
+    if (warp_first < p.n_starts) {  // whole idle warps skip the loop; idle groups shadow one
+      const bool active = start < p.n_starts;
+      const size_t row = (size_t)pidx * p.n_starts + (active ? start : p.n_starts - 1);
+      PoseState s;
+      {
+        float q0[4], t0[3];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) q0[i] = p.seed_q[row * 4 + i];
+        t0[0] = p.seed_t[row * 3 + 0] - c.x;
+        t0[1] = p.seed_t[row * 3 + 1] - c.y;
+        t0[2] = p.seed_t[row * 3 + 2] - c.z;
+        pose_init(s, q0, t0);
+      }
+      for (int step = 0; step < p.steps; ++step) {
+        const Rot R = quat_to_rot(s.q);
+        Moments ms;
+        ms.zero();
+        if (kShape) {
+          shape_pose<LPP, kEsp>(sP, sQc, sB, N, M, lane, R, s.t[0], s.t[1], s.t[2], p.k, p.e,
+                                p.inv2k, ms);
+          ms.template group_sum<LPP>();
+          ms.scale(p.Kc, p.aKc);
+        }
+        if (kPharm) {
+          Moments mc;
+          mc.zero();
+          pharm_pose<LPP>(sRA, sRV, sFA, sFV, Np, Mp, lane, R, s.t[0], s.t[1], s.t[2], p.tab,
+                          mc);
+          mc.template group_sum<LPP>();
+          if (kShape) step_combo(s, ms, Us, mc, Uc, p.w, p.lr);
+          else step_single(s, mc, Us, p.lr);
+        } else {
+          step_single(s, ms, Us, p.lr);
+        }
+      }
+      if (active && lane == 0) {
+        const size_t r = (size_t)pidx * p.n_starts + start;
+        p.row_score[r] = s.best;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) p.row_q[r * 4 + i] = s.bq[i];
+        p.row_t[r * 3 + 0] = s.bt[0] + c.x;
+        p.row_t[r * 3 + 1] = s.bt[1] + c.y;
+        p.row_t[r * 3 + 2] = s.bt[2] + c.z;
+      }
+    }
+    __syncthreads();  // shared memory is restaged for the next item
+  }
+}
+
+// Per-pair argmax over starts (first index wins ties, as torch.argmax).
+__global__ void pick_best_kernel(const float* __restrict__ rs, const float* __restrict__ rq,
+                                 const float* __restrict__ rt, int P, int S, float* os, float* oq,
+                                 float* ot) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P) return;
+  int bi = 0;
+  float bs = rs[(size_t)p * S];
+  for (int s = 1; s < S; ++s) {
+    const float v = rs[(size_t)p * S + s];
+    if (v > bs) { bs = v; bi = s; }
+  }
+  const size_t r = (size_t)p * S + bi;
+  os[p] = bs;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) oq[(size_t)p * 4 + i] = rq[r * 4 + i];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) ot[(size_t)p * 3 + i] = rt[r * 3 + i];
+}
+
+// ---------------------------------------------------------------------------------------
+// Self overlaps of packed clouds at the identity pose (one CTA of 32 threads per molecule).
+// ---------------------------------------------------------------------------------------
+template <bool ESP>
+__global__ void self_overlap_kernel(const float4* __restrict__ pts, const int* __restrict__ off,
+                                    int n_mol, int max_n, float k, float e, float inv2k, float Kc,
+                                    float* out) {
+  extern __shared__ __align__(16) float4 smem[];
+  __shared__ float red[96];
+  const int m = blockIdx.x;
+  const int o0 = off[m], n = off[m + 1] - o0;
+  if (n < 0 || n > max_n) {  // larger than the launch's tile: report NaN, touch nothing else
+    if (threadIdx.x == 0) out[m] = __int_as_float(0x7fc00000);
+    return;
+  }
+  float4* sP = smem;
+  float4* sB = sP + n;
+  float* sQc = reinterpret_cast<float*>(sB + n);
+  const float3 c = block_centroid(pts + o0, n, red);
+  stage_ref<ESP>(pts + o0, n, c, k, e, sP, sQc);
+  stage_copy(pts + o0, n, sB);
+  __syncthreads();
+  Rot R;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) R.r[i] = (i % 4 == 0) ? 1.f : 0.f;
+  Moments acc;
+  acc.zero();
+  shape_pose<32, ESP>(sP, sQc, sB, n, n, threadIdx.x, R, -c.x, -c.y, -c.z, k, e, inv2k, acc);
+  acc.group_sum<32>();
+  if (threadIdx.x == 0) out[m] = acc.v * Kc;
+}
+
+__global__ void pharm_self_kernel(const float4* __restrict__ anc, const float4* __restrict__ vec,
+                                  const int* __restrict__ off, int n_mol, int max_n,
+                                  PharmTables tab, float* out) {
+  extern __shared__ __align__(16) float4 smem[];
+  __shared__ float red[96];
+  const int m = blockIdx.x;
+  const int o0 = off[m], n = off[m + 1] - o0;
+  if (n < 0 || n > max_n) {
+    if (threadIdx.x == 0) out[m] = __int_as_float(0x7fc00000);
+    return;
+  }
+  float4* sRA = smem;
+  float4* sRV = sRA + n;
+  float4* sFA = sRV + n;
+  float4* sFV = sFA + n;
+  const float3 c = block_centroid(anc + o0, n, red);
+  stage_ref_pharm(anc + o0, vec ? vec + o0 : nullptr, n, c, sRA, sRV);
+  stage_fit_pharm(anc + o0, vec ? vec + o0 : nullptr, n, sFA, sFV);
+  __syncthreads();
+  Rot R;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) R.r[i] = (i % 4 == 0) ? 1.f : 0.f;
+  Moments acc;
+  acc.zero();
+  pharm_pose<32>(sRA, sRV, sFA, sFV, n, n, threadIdx.x, R, -c.x, -c.y, -c.z, tab, acc);
+  acc.group_sum<32>();
+  if (threadIdx.x == 0) out[m] = acc.v;
+}
+
+PharmTables make_pharm_tables(bool directional) {
+  // P_TYPES order: Acceptor, Donor, Aromatic, Hydrophobe, Halogen, Cation, Anion, ZnBinder,
+  // Dummy (score/constants.py:20); alphas from P_ALPHAS (constants.py:24-34).
+  static const double alphas[9] = {1.0, 1.0, 0.7, 0.7, 1.0, 1.0, 1.0, 1.0, 1.0};
+  static const int cats_dir[9] = {1, 1, 2, 0, 1, 0, 0, 0, 3};
+  PharmTables t;
+  for (int i = 0; i < 9; ++i) {
+    t.alpha[i] = (float)alphas[i];
+    t.K[i] = (float)std::pow(M_PI / (2.0 * alphas[i]), 1.5);
+    t.cat[i] = directional ? cats_dir[i] : (i == 8 ? 3 : 0);
+  }
+  return t;
+}
+
+namespace {
+
+template <int LPP, int MODE>
+int launch_align(const AlignParams& prm, int threads, int cta_per_sm, size_t smem,
+                 cudaStream_t st) {
+  auto kern = align_kernel<LPP, MODE>;
+  cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem);
+  if (ce != cudaSuccess)
+    return set_error(FSS_ERR_CUDA, std::string("fss_align: shared-memory attribute: ") +
+                                       cudaGetErrorString(ce));
+  int occ = 0;
+  ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem);
+  if (ce != cudaSuccess || occ <= 0)
+    return set_error(FSS_ERR_UNSUPPORTED, "fss_align: the tile does not fit on an SM");
+  if (cta_per_sm > 0) occ = std::min(occ, cta_per_sm);
+  const int grid = std::max(1, std::min(prm.n_items, occ * num_sms()));
+  kern<<<grid, threads, smem, st>>>(prm);
+  return check_launch("fss_align");
+}
+
+template <int MODE>
+int dispatch_lpp(int lpp, const AlignParams& prm, int threads, int cps, size_t smem,
+                 cudaStream_t st) {
+  switch (lpp) {
+    case 4: return launch_align<4, MODE>(prm, threads, cps, smem, st);
+    case 8: return launch_align<8, MODE>(prm, threads, cps, smem, st);
+    case 16: return launch_align<16, MODE>(prm, threads, cps, smem, st);
+    case 32: return launch_align<32, MODE>(prm, threads, cps, smem, st);
+    default: return set_error(FSS_ERR_INVALID, "fss_align: lanes_per_pose must be 4, 8, 16 or 32");
+  }
+}
+
+// Default tiling: lanes per pose from the fit size (about 4 fit points per lane for the
+// register tile), start blocks chosen to waste the fewest pose slots.
+void auto_tile(int mode, int max_fit, int n_starts, int* lpp, int* chunks) {
+  int l = *lpp;
+  if (l <= 0) {
+    const int m = mode == FSS_MODE_PHARM ? max_fit * 2 : max_fit;
+    l = m <= 16 ? 4 : (m <= 32 ? 8 : (m <= 64 ? 16 : 32));
+  }
+  *lpp = l;
+  if (*chunks > 0) return;
+  const int max_poses = kMaxThreads / l;
+  int best_c = 1, best_waste = 1 << 30;
+  for (int c = 1; c <= n_starts; ++c) {
+    const int ppc = (n_starts + c - 1) / c;
+    if (ppc > max_poses) continue;
+    const int warps = (ppc * l + 31) / 32;
+    const int waste = warps * 32 / l * c - n_starts;  // idle pose slots
+    if (waste < best_waste) { best_waste = waste; best_c = c; }
+    if (waste == 0) break;
+  }
+  *chunks = best_c;
+}
+
+}  // namespace
+
+int align_launch(const fss_align_desc* d, cudaStream_t st) {
+  if (!d) return set_error(FSS_ERR_INVALID, "fss_align: null descriptor");
+  if (d->mode < FSS_MODE_SHAPE || d->mode > FSS_MODE_SHAPE_COLOR)
+    return set_error(FSS_ERR_INVALID, "fss_align: unknown mode");
+  if (d->n_pairs < 0 || d->n_starts <= 0 || d->steps < 0)
+    return set_error(FSS_ERR_INVALID, "fss_align: needs n_pairs >= 0, n_starts > 0, steps >= 0");
+  if (!d->scratch || !d->row_score || !d->row_q || !d->row_t || !d->seed_q || !d->seed_t ||
+      !d->pair_ref || !d->pair_fit)
+    return set_error(FSS_ERR_INVALID, "fss_align: missing pair, seed, row or scratch buffer");
+  const bool shape = d->mode != FSS_MODE_PHARM;
+  const bool pharm = d->mode >= FSS_MODE_PHARM;
+  if (shape && (!d->ref_pts || !d->ref_off || !d->fit_pts || !d->fit_off || !d->ref_self ||
+                !d->fit_self))
+    return set_error(FSS_ERR_INVALID, "fss_align: shape channel clouds / self overlaps missing");
+  if (pharm && (!d->ref_anc || !d->ref_ph_off || !d->fit_anc || !d->fit_ph_off))
+    return set_error(FSS_ERR_INVALID, "fss_align: pharmacophore channel missing");
+  if (d->mode == FSS_MODE_PHARM && (!d->ref_self || !d->fit_self))
+    return set_error(FSS_ERR_INVALID, "fss_align: pharm self overlaps missing");
+  if (shape && pharm && (!d->ref_self_ph || !d->fit_self_ph))
+    return set_error(FSS_ERR_INVALID, "fss_align: pharm-channel self overlaps missing");
+  if ((d->mode == FSS_MODE_PHARM || d->mode == FSS_MODE_SHAPE_PHARM) && (!d->ref_vec || !d->fit_vec))
+    return set_error(FSS_ERR_INVALID, "fss_align: directional pharm needs vectors");
+  if (shape && !(d->alpha > 0.f)) return set_error(FSS_ERR_INVALID, "fss_align: alpha must be > 0");
+  const int maxN = shape ? d->max_ref_points : 0, maxM = shape ? d->max_fit_points : 0;
+  const int maxNp = pharm ? d->max_ref_features : 0, maxMp = pharm ? d->max_fit_features : 0;
+  if (maxN < 0 || maxM < 0 || maxNp < 0 || maxMp < 0)
+    return set_error(FSS_ERR_INVALID, "fss_align: negative extents");
+  if (maxN > kMaxPoints || maxM > kMaxPoints || maxNp > kMaxPoints || maxMp > kMaxPoints)
+    return set_error(FSS_ERR_UNSUPPORTED, "fss_align: more than fss_max_points() points in a molecule");
+
+  cudaError_t ce = cudaMemsetAsync(d->scratch, 0, 2 * sizeof(int32_t), st);
+  if (ce != cudaSuccess)
+    return set_error(FSS_ERR_CUDA, std::string("fss_align: scratch reset: ") + cudaGetErrorString(ce));
+  if (d->n_pairs == 0) return FSS_OK;
+
+  int lpp = d->lanes_per_pose, chunks = d->chunks;
+  auto_tile(d->mode, shape ? maxM : maxMp, d->n_starts, &lpp, &chunks);
+  if (chunks < 1 || chunks > d->n_starts)
+    return set_error(FSS_ERR_INVALID, "fss_align: chunks must be in [1, n_starts]");
+  const int ppc = (d->n_starts + chunks - 1) / chunks;
+  const int threads = ((ppc * lpp + 31) / 32) * 32;
+  if (threads > kMaxThreads)
+    return set_error(FSS_ERR_INVALID, "fss_align: too many starts per CTA for lanes_per_pose");
+  // every start block must be non-empty
+  chunks = (d->n_starts + ppc - 1) / ppc;
+
+  AlignParams p{};
+  p.mode = d->mode; p.n_pairs = d->n_pairs; p.n_starts = d->n_starts; p.steps = d->steps;
+  p.chunks = chunks; p.n_items = d->n_pairs * chunks;
+  p.maxN = maxN; p.maxM = maxM; p.maxNp = maxNp; p.maxMp = maxMp;
+  p.pair_ref = d->pair_ref; p.pair_fit = d->pair_fit; p.order = d->order;
+  p.ref_pts = reinterpret_cast<const float4*>(d->ref_pts); p.ref_off = d->ref_off;
+  p.fit_pts = reinterpret_cast<const float4*>(d->fit_pts); p.fit_off = d->fit_off;
+  p.ref_self = d->ref_self; p.fit_self = d->fit_self;
+  p.ref_anc = reinterpret_cast<const float4*>(d->ref_anc);
+  p.ref_vec = reinterpret_cast<const float4*>(d->ref_vec); p.ref_ph_off = d->ref_ph_off;
+  p.fit_anc = reinterpret_cast<const float4*>(d->fit_anc);
+  p.fit_vec = reinterpret_cast<const float4*>(d->fit_vec); p.fit_ph_off = d->fit_ph_off;
+  p.ref_self_ph = d->ref_self_ph; p.fit_self_ph = d->fit_self_ph;
+  p.seed_q = d->seed_q; p.seed_t = d->seed_t;
+  const double alpha = shape ? (double)d->alpha : 1.0;
+  p.alpha = (float)alpha;
+  p.k = (float)(0.5 * alpha * 1.4426950408889634);
+  p.e = (float)((double)d->inv_lam * 1.4426950408889634);
+  p.inv2k = (float)(1.0 / (alpha * 1.4426950408889634));
+  p.Kc = (float)(std::pow(M_PI, 1.5) / std::pow(2.0 * alpha, 1.5));
+  p.aKc = (float)(alpha * std::pow(M_PI, 1.5) / std::pow(2.0 * alpha, 1.5));
+  p.w = d->color_weight; p.lr = d->lr;
+  p.tab = make_pharm_tables(d->mode != FSS_MODE_SHAPE_COLOR);
+  p.row_score = d->row_score; p.row_q = d->row_q; p.row_t = d->row_t;
+  p.counter = d->scratch;
+
+  const size_t smem = sizeof(float4) * ((size_t)maxN + maxM + 2 * (size_t)maxNp + 2 * (size_t)maxMp) +
+                      sizeof(float) * (d->mode == FSS_MODE_ESP ? (size_t)maxN : 0) + 16;
+  int rc;
+  switch (d->mode) {
+    case FSS_MODE_SHAPE: rc = dispatch_lpp<FSS_MODE_SHAPE>(lpp, p, threads, d->cta_per_sm, smem, st); break;
+    case FSS_MODE_ESP: rc = dispatch_lpp<FSS_MODE_ESP>(lpp, p, threads, d->cta_per_sm, smem, st); break;
+    case FSS_MODE_PHARM: rc = dispatch_lpp<FSS_MODE_PHARM>(lpp, p, threads, d->cta_per_sm, smem, st); break;
+    case FSS_MODE_SHAPE_PHARM: rc = dispatch_lpp<FSS_MODE_SHAPE_PHARM>(lpp, p, threads, d->cta_per_sm, smem, st); break;
+    default: rc = dispatch_lpp<FSS_MODE_SHAPE_COLOR>(lpp, p, threads, d->cta_per_sm, smem, st); break;
+  }
+  if (rc != FSS_OK) return rc;
+  if (d->out_score && d->out_q && d->out_t)
+    return pick_best_launch(d->row_score, d->row_q, d->row_t, d->n_pairs, d->n_starts,
+                            d->out_score, d->out_q, d->out_t, st);
+  return FSS_OK;
+}
+
+int pick_best_launch(const float* rs, const float* rq, const float* rt, int P, int S, float* os,
+                     float* oq, float* ot, cudaStream_t st) {
+  if (P < 0 || S <= 0 || !rs || !rq || !rt || !os || !oq || !ot)
+    return set_error(FSS_ERR_INVALID, "fss_pick_best: bad arguments");
+  if (P == 0) return FSS_OK;
+  pick_best_kernel<<<(P + 255) / 256, 256, 0, st>>>(rs, rq, rt, P, S, os, oq, ot);
+  return check_launch("fss_pick_best");
+}
+
+int self_overlap_launch(const float* pts, const int32_t* off, int n_mol, int max_n, float alpha,
+                        int esp, float inv_lam, float* out, cudaStream_t st) {
+  if (n_mol < 0 || !pts || !off || !out || !(alpha > 0.f))
+    return set_error(FSS_ERR_INVALID, "fss_self_overlap: bad arguments");
+  if (max_n > kMaxPoints) return set_error(FSS_ERR_UNSUPPORTED, "fss_self_overlap: molecule too large");
+  if (n_mol == 0) return FSS_OK;
+  const double a = alpha;
+  const float k = (float)(0.5 * a * 1.4426950408889634);
+  const float e = (float)((double)inv_lam * 1.4426950408889634);
+  const float inv2k = (float)(1.0 / (a * 1.4426950408889634));
+  const float Kc = (float)(std::pow(M_PI, 1.5) / std::pow(2.0 * a, 1.5));
+  const size_t smem = sizeof(float4) * 2 * (size_t)max_n + sizeof(float) * (size_t)max_n + 16;
+  cudaError_t ce;
+  if (esp) {
+    ce = cudaFuncSetAttribute(self_overlap_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (ce == cudaSuccess)
+      self_overlap_kernel<true><<<n_mol, 32, smem, st>>>(reinterpret_cast<const float4*>(pts), off, n_mol, max_n, k, e, inv2k, Kc, out);
+  } else {
+    ce = cudaFuncSetAttribute(self_overlap_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (ce == cudaSuccess)
+      self_overlap_kernel<false><<<n_mol, 32, smem, st>>>(reinterpret_cast<const float4*>(pts), off, n_mol, max_n, k, 0.f, inv2k, Kc, out);
+  }
+  if (ce != cudaSuccess) return set_error(FSS_ERR_CUDA, std::string("fss_self_overlap: ") + cudaGetErrorString(ce));
+  return check_launch("fss_self_overlap");
+}
+
+int pharm_self_launch(const float* anc, const float* vec, const int32_t* off, int n_mol, int max_n,
+                      int directional, float* out, cudaStream_t st) {
+  if (n_mol < 0 || !anc || !off || !out || (directional && !vec))
+    return set_error(FSS_ERR_INVALID, "fss_pharm_self_overlap: bad arguments");
+  if (max_n > kMaxPoints) return set_error(FSS_ERR_UNSUPPORTED, "fss_pharm_self_overlap: molecule too large");
+  if (n_mol == 0) return FSS_OK;
+  const size_t smem = sizeof(float4) * 4 * (size_t)max_n + 16;
+  cudaError_t ce = cudaFuncSetAttribute(pharm_self_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (ce != cudaSuccess) return set_error(FSS_ERR_CUDA, std::string("fss_pharm_self_overlap: ") + cudaGetErrorString(ce));
+  pharm_self_kernel<<<n_mol, 32, smem, st>>>(reinterpret_cast<const float4*>(anc),
+                                             reinterpret_cast<const float4*>(vec), off, n_mol, max_n,
+                                             make_pharm_tables(directional != 0), out);
+  return check_launch("fss_pharm_self_overlap");
+}
+
+}  // namespace fss

@@ -1,0 +1,371 @@
+// fss_device.cuh -- device building blocks shared by every fast_shepherd_score_b200 kernel.
+//
+// Math conventions (identical to the reference shepherd_score batched path):
+//   * pose = (q, t), q = (w, x, y, z); the fit cloud moves: b' = R(q) b + t
+//   * shape overlap  V = K * sum_ij exp(-alpha/2 |a_i - b'_j|^2),  K = pi^1.5 / (2 alpha)^1.5
+//     (accel/kernels/shape_triton.py:73-188)
+//   * ESP overlap    the same with an extra factor exp(-(c_i - c_j)^2 / lam)
+//     (accel/kernels/esp_triton.py:21-172)
+//   * typed pharmacophore overlap with directional weights (accel/kernels/pharm_triton.py:296-400)
+//   * dV/dt = sum_j f_j,  dV/dq = sum_j f_j . (dR/dq) b_j  with f_j = sum_i alpha g_ij (a_i - b'_j)
+//     (the quaternion tail _quat_grad_tail, shape_triton.py:46-65), evaluated here through the
+//     3x3 moment G = sum_j f_j b_j^T, which is the same linear form regrouped.
+//   * Tanimoto score / Adam tail of accel/kernels/cpu_fused.py:54-167 (no bias correction,
+//     eps inside the sqrt, tangent projection of the quaternion gradient, renormalisation).
+//
+// Arithmetic layout of the pairwise sum (the hot loop): with k = alpha/2 * log2(e) the base-2
+// exponent of one term is
+//       E_ij = P_i.w + F_j.w + P_i.xyz . b'_j            (+ Qc_i * c_j for ESP)
+//   P_i = (2k a_i, -k|a_i|^2 - e c_i^2)   staged once per pair in shared memory
+//   F_j.w = -k|b'_j|^2 - e c_j^2          recomputed per pose and step in registers
+//   Qc_i = 2 e c_i, e = log2(e) / lam
+// so a term costs one ex2 on the MUFU pipe plus 8 FP32 ops (4 for the exponent, 4 for
+// the value / gradient accumulation), against 11+ for the direct difference form.  The
+// reference cloud is centred on its own centroid before staging, which keeps |a|^2 small
+// and the expanded form's cancellation error below 1e-6 relative per term.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fss {
+
+constexpr float kLog2e = 1.4426950408889634f;
+constexpr float kPi15 = 5.568327996831708f;  // pi ** 1.5
+constexpr float kBeta1 = 0.9f;
+constexpr float kBeta2 = 0.999f;
+constexpr float kAdamEps = 1e-8f;
+
+// 2^x on the MUFU pipe (flush-to-zero; -inf -> +0).
+__device__ __forceinline__ float ex2(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+struct Rot {
+  float r[9];
+};
+
+// Rotation matrix from a (w,x,y,z) quaternion, the expression of shape_triton.py:35-43.
+__device__ __forceinline__ Rot quat_to_rot(const float q[4]) {
+  const float qr = q[0], qi = q[1], qj = q[2], qk = q[3];
+  Rot R;
+  R.r[0] = 1.f - 2.f * (qj * qj + qk * qk);
+  R.r[1] = 2.f * (qi * qj - qk * qr);
+  R.r[2] = 2.f * (qi * qk + qj * qr);
+  R.r[3] = 2.f * (qi * qj + qk * qr);
+  R.r[4] = 1.f - 2.f * (qi * qi + qk * qk);
+  R.r[5] = 2.f * (qj * qk - qi * qr);
+  R.r[6] = 2.f * (qi * qk - qj * qr);
+  R.r[7] = 2.f * (qj * qk + qi * qr);
+  R.r[8] = 1.f - 2.f * (qi * qi + qj * qj);
+  return R;
+}
+
+__device__ __forceinline__ float3 rot_apply(const Rot& R, float x, float y, float z) {
+  return make_float3(fmaf(R.r[0], x, fmaf(R.r[1], y, R.r[2] * z)),
+                     fmaf(R.r[3], x, fmaf(R.r[4], y, R.r[5] * z)),
+                     fmaf(R.r[6], x, fmaf(R.r[7], y, R.r[8] * z)));
+}
+
+// Per-lane partial sums of one channel: value, translation force and the 3x3 moment
+// G[r][c] = sum_j f_j[r] * b_j[c] (row-major).
+struct Moments {
+  float v;
+  float f[3];
+  float g[9];
+  __device__ __forceinline__ void zero() {
+    v = 0.f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) f[i] = 0.f;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) g[i] = 0.f;
+  }
+  __device__ __forceinline__ void add_force(float fx, float fy, float fz, float bx, float by,
+                                            float bz) {
+    f[0] += fx; f[1] += fy; f[2] += fz;
+    g[0] = fmaf(fx, bx, g[0]); g[1] = fmaf(fx, by, g[1]); g[2] = fmaf(fx, bz, g[2]);
+    g[3] = fmaf(fy, bx, g[3]); g[4] = fmaf(fy, by, g[4]); g[5] = fmaf(fy, bz, g[5]);
+    g[6] = fmaf(fz, bx, g[6]); g[7] = fmaf(fz, by, g[7]); g[8] = fmaf(fz, bz, g[8]);
+  }
+  // Butterfly sum over an aligned group of `width` lanes; every lane ends with the total.
+  template <int WIDTH>
+  __device__ __forceinline__ void group_sum() {
+#pragma unroll
+    for (int o = WIDTH / 2; o > 0; o >>= 1) {
+      v += __shfl_xor_sync(0xffffffffu, v, o);
+#pragma unroll
+      for (int i = 0; i < 3; ++i) f[i] += __shfl_xor_sync(0xffffffffu, f[i], o);
+#pragma unroll
+      for (int i = 0; i < 9; ++i) g[i] += __shfl_xor_sync(0xffffffffu, g[i], o);
+    }
+  }
+  __device__ __forceinline__ void scale(float sv, float sf) {
+    v *= sv;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) f[i] *= sf;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) g[i] *= sf;
+  }
+};
+
+// dV/dq from the moment G at quaternion q: the reference's per-point tail
+// (shape_triton.py:46-65) summed over points and regrouped by G's entries.
+__device__ __forceinline__ void quat_grad_from_moment(const float q[4], const float G[9],
+                                                      float dq[4]) {
+  const float qr = q[0], qi = q[1], qj = q[2], qk = q[3];
+  const float xx = G[0], xy = G[1], xz = G[2], yx = G[3], yy = G[4], yz = G[5], zx = G[6],
+              zy = G[7], zz = G[8];
+  dq[0] = 2.f * (qk * (yx - xy) + qj * (xz - zx) + qi * (zy - yz));
+  dq[1] = 2.f * (qj * (xy + yx) + qk * (xz + zx) + qr * (zy - yz) - 2.f * qi * (yy + zz));
+  dq[2] = 2.f * (qi * (xy + yx) + qk * (yz + zy) + qr * (xz - zx) - 2.f * qj * (xx + zz));
+  dq[3] = 2.f * (qi * (xz + zx) + qj * (yz + zy) + qr * (yx - xy) - 2.f * qk * (xx + yy));
+}
+
+// Loop-carried optimiser state of one pose.
+struct PoseState {
+  float q[4], t[3];
+  float mq[4], vq[4], mt[3], vt[3];
+  float best, bq[4], bt[3];
+};
+
+__device__ __forceinline__ void pose_init(PoseState& s, const float q0[4], const float t0[3]) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i) { s.q[i] = q0[i]; s.bq[i] = q0[i]; s.mq[i] = 0.f; s.vq[i] = 0.f; }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) { s.t[i] = t0[i]; s.bt[i] = t0[i]; s.mt[i] = 0.f; s.vt[i] = 0.f; }
+  s.best = -INFINITY;
+}
+
+// Best-pose tracking (pre-update pose) + tangent-projected Adam on q, plain Adam on t,
+// quaternion renormalisation: cpu_fused.py:68-108 / shape_triton.py:253-368.
+__device__ __forceinline__ void adam_tail(PoseState& s, float score, const float gq[4],
+                                          const float gt[3], float lr) {
+  if (score > s.best) {  // NaN never replaces the best, as in the reference comparison
+    s.best = score;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) s.bq[i] = s.q[i];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) s.bt[i] = s.t[i];
+  }
+  const float radial = gq[0] * s.q[0] + gq[1] * s.q[1] + gq[2] * s.q[2] + gq[3] * s.q[3];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const float d = gq[i] - s.q[i] * radial;
+    s.mq[i] = kBeta1 * s.mq[i] + (1.f - kBeta1) * d;
+    s.vq[i] = kBeta2 * s.vq[i] + (1.f - kBeta2) * d * d;
+    s.q[i] = s.q[i] - lr * s.mq[i] / sqrtf(s.vq[i] + kAdamEps);
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const float d = gt[i];
+    s.mt[i] = kBeta1 * s.mt[i] + (1.f - kBeta1) * d;
+    s.vt[i] = kBeta2 * s.vt[i] + (1.f - kBeta2) * d * d;
+    s.t[i] = s.t[i] - lr * s.mt[i] / sqrtf(s.vt[i] + kAdamEps);
+  }
+  float qn = sqrtf(s.q[0] * s.q[0] + s.q[1] * s.q[1] + s.q[2] * s.q[2] + s.q[3] * s.q[3]);
+  qn = qn < 1e-12f ? 1e-12f : qn;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) s.q[i] = s.q[i] / qn;
+}
+
+// Tanimoto score V/(U-V) and its derivative scale U/(U-V)^2 (cpu_fused.py:62-67).
+__device__ __forceinline__ void tanimoto(float V, float U, float& score, float& scale) {
+  float denom = U - V;
+  if (denom == 0.f) denom = 1e-12f;
+  score = V / denom;
+  scale = U / (denom * denom);
+}
+
+// Single-channel step: score, best tracking and Adam from the channel's moments.
+__device__ __forceinline__ void step_single(PoseState& s, const Moments& m, float U, float lr) {
+  float score, scale;
+  tanimoto(m.v, U, score, scale);
+  float dq[4];
+  quat_grad_from_moment(s.q, m.g, dq);
+  float gq[4], gt[3];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) gq[i] = -scale * dq[i];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) gt[i] = -scale * m.f[i];
+  adam_tail(s, score, gq, gt, lr);
+}
+
+// Two-channel step (1-w) * shape + w * pharm, the joint gradient of cpu_fused.py:111-167.
+__device__ __forceinline__ void step_combo(PoseState& s, const Moments& ms, float Us,
+                                           const Moments& mc, float Uc, float w, float lr) {
+  float ss, scs, sc, scc;
+  tanimoto(ms.v, Us, ss, scs);
+  tanimoto(mc.v, Uc, sc, scc);
+  const float score = (1.f - w) * ss + w * sc;
+  const float cs = -(1.f - w) * scs, cc = -w * scc;
+  float dqs[4], dqc[4];
+  quat_grad_from_moment(s.q, ms.g, dqs);
+  quat_grad_from_moment(s.q, mc.g, dqc);
+  float gq[4], gt[3];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) gq[i] = cs * dqs[i] + cc * dqc[i];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) gt[i] = cs * ms.f[i] + cc * mc.f[i];
+  adam_tail(s, score, gq, gt, lr);
+}
+
+// ---------------------------------------------------------------------------------------
+// Shape / ESP pairwise sum for one pose.
+//
+// The lanes of one pose group (LPP consecutive lanes) split the fit points j = lane + LPP*u;
+// every lane loops over all N staged reference points.  JB fit points are held in registers
+// per pass so one shared-memory load of P_i feeds JB terms.  Returns the lane's partial
+// moments in "raw" units: v = sum g, f_j = sum_i g (a_i - b'_j) (multiply by K and alpha K).
+// ---------------------------------------------------------------------------------------
+template <int JB, bool ESP>
+__device__ __forceinline__ void shape_chunk(const float4* __restrict__ sP,
+                                            const float* __restrict__ sQc,
+                                            const float4* __restrict__ sB, int N, int M,
+                                            int j0, int stride, const Rot& R, float tx, float ty,
+                                            float tz, float k, float e, float inv2k,
+                                            Moments& acc) {
+  float bx[JB], by[JB], bz[JB], fw[JB], cj[JB];
+  float bx0[JB], by0[JB], bz0[JB];
+  float sg[JB], sx[JB], sy[JB], sz[JB];
+#pragma unroll
+  for (int u = 0; u < JB; ++u) {
+    const int j = j0 + u * stride;
+    const bool ok = j < M;
+    const float4 b = ok ? sB[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+    bx0[u] = b.x; by0[u] = b.y; bz0[u] = b.z; cj[u] = b.w;
+    const float3 p = rot_apply(R, b.x, b.y, b.z);
+    bx[u] = p.x + tx; by[u] = p.y + ty; bz[u] = p.z + tz;
+    float w = -k * (bx[u] * bx[u] + by[u] * by[u] + bz[u] * bz[u]);
+    if (ESP) w = fmaf(-e * b.w, b.w, w);
+    fw[u] = ok ? w : -INFINITY;
+    sg[u] = 0.f; sx[u] = 0.f; sy[u] = 0.f; sz[u] = 0.f;
+  }
+#pragma unroll 2
+  for (int i = 0; i < N; ++i) {
+    const float4 P = sP[i];
+    float qc = 0.f;
+    if (ESP) qc = sQc[i];
+#pragma unroll
+    for (int u = 0; u < JB; ++u) {
+      float E = fmaf(P.x, bx[u], fmaf(P.y, by[u], fmaf(P.z, bz[u], P.w + fw[u])));
+      if (ESP) E = fmaf(qc, cj[u], E);
+      const float g = ex2(E);
+      sg[u] += g;
+      sx[u] = fmaf(g, P.x, sx[u]);
+      sy[u] = fmaf(g, P.y, sy[u]);
+      sz[u] = fmaf(g, P.z, sz[u]);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < JB; ++u) {
+    const float fx = fmaf(sx[u], inv2k, -bx[u] * sg[u]);
+    const float fy = fmaf(sy[u], inv2k, -by[u] * sg[u]);
+    const float fz = fmaf(sz[u], inv2k, -bz[u] * sg[u]);
+    acc.v += sg[u];
+    acc.add_force(fx, fy, fz, bx0[u], by0[u], bz0[u]);
+  }
+}
+
+template <int LPP, bool ESP>
+__device__ __forceinline__ void shape_pose(const float4* __restrict__ sP,
+                                           const float* __restrict__ sQc,
+                                           const float4* __restrict__ sB, int N, int M, int lane,
+                                           const Rot& R, float tx, float ty, float tz, float k,
+                                           float e, float inv2k, Moments& acc) {
+  constexpr int JB = 4;
+  // Trip counts depend only on M and LPP, so every lane of the group (and every group of
+  // the warp, which share one pair) runs the same loop; points past M are masked.
+  int base = 0;
+  for (; base + JB * LPP <= M; base += JB * LPP)
+    shape_chunk<JB, ESP>(sP, sQc, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k, acc);
+  const int rem = (M - base + LPP - 1) / LPP;  // 0..JB points left for the group's lane 0
+  if (rem == 4) {
+    shape_chunk<4, ESP>(sP, sQc, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k, acc);
+  } else if (rem == 3) {
+    shape_chunk<3, ESP>(sP, sQc, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k, acc);
+  } else if (rem == 2) {
+    shape_chunk<2, ESP>(sP, sQc, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k, acc);
+  } else if (rem == 1) {
+    shape_chunk<1, ESP>(sP, sQc, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k, acc);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Typed pharmacophore sum for one pose (pharm_triton.py:296-400, cpu.py:500-582).
+// Anchors are staged as float4 (x, y, z, type bits); vectors are unit (x, y, z, 0).
+// Lanes split the fit features; the same-type test is an exact integer compare.
+// Partial moments in final units (K and alpha folded in per type).
+// ---------------------------------------------------------------------------------------
+struct PharmTables {
+  float alpha[9];
+  float K[9];
+  int cat[9];
+};
+
+template <int LPP>
+__device__ __forceinline__ void pharm_pose(const float4* __restrict__ sRA,
+                                           const float4* __restrict__ sRV,
+                                           const float4* __restrict__ sFA,
+                                           const float4* __restrict__ sFV, int N, int M,
+                                           int lane, const Rot& R, float tx, float ty, float tz,
+                                           const PharmTables& tab, Moments& acc) {
+  for (int j = lane; j < M; j += LPP) {
+    const float4 fa = sFA[j];
+    const int ityp = __float_as_int(fa.w);
+    const int icat = tab.cat[ityp];
+    if (icat == 3) continue;
+    const float ialpha = tab.alpha[ityp], iK = tab.K[ityp];
+    const float nk = -0.5f * ialpha * kLog2e;
+    const float4 fv = sFV[j];
+    const float3 pa = rot_apply(R, fa.x, fa.y, fa.z);
+    const float ax = pa.x + tx, ay = pa.y + ty, az = pa.z + tz;
+    const float3 pv = rot_apply(R, fv.x, fv.y, fv.z);
+    float fx = 0.f, fy = 0.f, fz = 0.f, wx = 0.f, wy = 0.f, wz = 0.f, o = 0.f;
+    for (int i = 0; i < N; ++i) {
+      const float4 ra = sRA[i];
+      if (__float_as_int(ra.w) != ityp) continue;
+      const float dx = ra.x - ax, dy = ra.y - ay, dz = ra.z - az;  // ref - rotfit
+      const float r2 = dx * dx + dy * dy + dz * dz;
+      const float E = ex2(nk * r2);
+      float w = 1.f, c = 0.f;
+      float4 rv = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (icat == 1 || icat == 2) {
+        rv = sRV[i];
+        const float D = pv.x * rv.x + pv.y * rv.y + pv.z * rv.z;
+        if (icat == 1) {
+          const float Dc = fminf(fmaxf(D, 0.f), 1.f);
+          w = (Dc + 2.f) * (1.f / 3.f);
+          c = (D > 0.f && D < 1.f) ? 1.f : 0.f;
+        } else {
+          w = (fabsf(D) + 2.f) * (1.f / 3.f);
+          c = D > 0.f ? 1.f : (D < 0.f ? -1.f : 0.f);
+        }
+      }
+      const float KE = iK * E;
+      const float KwE = KE * w;
+      o += KwE;
+      const float a = ialpha * KwE;
+      fx = fmaf(a, dx, fx); fy = fmaf(a, dy, fy); fz = fmaf(a, dz, fz);
+      const float cf = (1.f / 3.f) * KE * c;
+      wx = fmaf(cf, rv.x, wx); wy = fmaf(cf, rv.y, wy); wz = fmaf(cf, rv.z, wz);
+    }
+    acc.v += o;
+    acc.add_force(fx, fy, fz, fa.x, fa.y, fa.z);
+    // weight force acts through the body-frame vector; it does not move t
+    acc.g[0] = fmaf(wx, fv.x, acc.g[0]); acc.g[1] = fmaf(wx, fv.y, acc.g[1]);
+    acc.g[2] = fmaf(wx, fv.z, acc.g[2]); acc.g[3] = fmaf(wy, fv.x, acc.g[3]);
+    acc.g[4] = fmaf(wy, fv.y, acc.g[4]); acc.g[5] = fmaf(wy, fv.z, acc.g[5]);
+    acc.g[6] = fmaf(wz, fv.x, acc.g[6]); acc.g[7] = fmaf(wz, fv.y, acc.g[7]);
+    acc.g[8] = fmaf(wz, fv.z, acc.g[8]);
+  }
+}
+
+// Unit vector with the reference's 1e-12 norm floor (cpu.py:524-526).
+__device__ __forceinline__ float4 unit4(float x, float y, float z) {
+  float n = sqrtf(x * x + y * y + z * z);
+  const float inv = 1.f / (n > 1e-12f ? n : 1e-12f);
+  return make_float4(x * inv, y * inv, z * inv, 0.f);
+}
+
+}  // namespace fss

@@ -1,0 +1,126 @@
+// fss_internal.cuh -- host/device plumbing shared by the libfss_cuda translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/fss_cuda.h"
+#include "fss_device.cuh"
+
+namespace fss {
+
+// Hard limit of points (or pharmacophore features) per molecule that the fused kernels
+// stage in shared memory.  4096 float4 points = 64 KB per cloud.
+constexpr int kMaxPoints = 4096;
+
+// Thread-local error message + status helpers (fss_capi.cu).
+int set_error(int code, const std::string& msg);
+int check_launch(const char* what);
+
+// Block-wide sum of a float3 (blockDim.x a multiple of 32, <= 1024); every thread gets it.
+__device__ __forceinline__ float3 block_sum3(float3 v, float* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+    v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    v.z += __shfl_xor_sync(0xffffffffu, v.z, o);
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (l == 0) { red[3 * w] = v.x; red[3 * w + 1] = v.y; red[3 * w + 2] = v.z; }
+  __syncthreads();
+  float3 s = make_float3(0.f, 0.f, 0.f);
+  for (int i = 0; i < nw; ++i) { s.x += red[3 * i]; s.y += red[3 * i + 1]; s.z += red[3 * i + 2]; }
+  return s;
+}
+
+// Centroid of n packed points (block cooperative).
+__device__ __forceinline__ float3 block_centroid(const float4* __restrict__ g, int n, float* red) {
+  float3 s = make_float3(0.f, 0.f, 0.f);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const float4 p = g[i];
+    s.x += p.x; s.y += p.y; s.z += p.z;
+  }
+  s = block_sum3(s, red);
+  const float inv = 1.f / (float)(n > 0 ? n : 1);
+  return make_float3(s.x * inv, s.y * inv, s.z * inv);
+}
+
+// Stage a reference cloud (centred on c) in the expanded form P_i = (2k a, -k|a|^2 - e c^2)
+// and, for ESP, Qc_i = 2 e c_i.
+template <bool ESP>
+__device__ __forceinline__ void stage_ref(const float4* __restrict__ g, int n, float3 c, float k,
+                                          float e, float4* sP, float* sQc) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const float4 p = g[i];
+    const float ax = p.x - c.x, ay = p.y - c.y, az = p.z - c.z;
+    float w = -k * (ax * ax + ay * ay + az * az);
+    if (ESP) {
+      w = fmaf(-e * p.w, p.w, w);
+      sQc[i] = 2.f * e * p.w;
+    }
+    sP[i] = make_float4(2.f * k * ax, 2.f * k * ay, 2.f * k * az, w);
+  }
+}
+
+__device__ __forceinline__ void stage_copy(const float4* __restrict__ g, int n, float4* s) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s[i] = g[i];
+}
+
+// Pharmacophore type carried in a float's bits; anything outside the 9-entry tables is
+// treated as Dummy (8), which the kernels skip.
+__device__ __forceinline__ float clamp_type(float w) {
+  const int t = __float_as_int(w);
+  return __int_as_float((t < 0 || t > 8) ? 8 : t);
+}
+
+// Reference pharmacophores: anchors centred on c (type bits kept), unit vectors.
+__device__ __forceinline__ void stage_ref_pharm(const float4* __restrict__ ga,
+                                                const float4* __restrict__ gv, int n, float3 c,
+                                                float4* sA, float4* sV) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const float4 a = ga[i];
+    sA[i] = make_float4(a.x - c.x, a.y - c.y, a.z - c.z, clamp_type(a.w));
+    if (gv) {
+      const float4 v = gv[i];
+      sV[i] = unit4(v.x, v.y, v.z);
+    } else {
+      sV[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  }
+}
+
+// Fit pharmacophores in their body frame: anchors as given, unit vectors.
+__device__ __forceinline__ void stage_fit_pharm(const float4* __restrict__ ga,
+                                                const float4* __restrict__ gv, int n,
+                                                float4* sA, float4* sV) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const float4 a = ga[i];
+    sA[i] = make_float4(a.x, a.y, a.z, clamp_type(a.w));
+    if (gv) {
+      const float4 v = gv[i];
+      sV[i] = unit4(v.x, v.y, v.z);
+    } else {
+      sV[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  }
+}
+
+// Lookup tables of accel/kernels/... build_lookup_tables (analytical_gradients/_torch.py:177-220):
+// alpha per type, K = (pi / (2 alpha))^1.5, category 0 isotropic, 1 directional,
+// 2 aromatic (|cos|), 3 dummy (skipped).  directional = false maps every real type to 0.
+PharmTables make_pharm_tables(bool directional);
+
+int num_sms();
+
+// Launchers behind the C ABI (each validates its arguments and returns an fss_status).
+int align_launch(const fss_align_desc* d, cudaStream_t st);
+int pick_best_launch(const float* rs, const float* rq, const float* rt, int P, int S, float* os,
+                     float* oq, float* ot, cudaStream_t st);
+int self_overlap_launch(const float* pts, const int32_t* off, int n_mol, int max_n, float alpha,
+                        int esp, float inv_lam, float* out, cudaStream_t st);
+int pharm_self_launch(const float* anc, const float* vec, const int32_t* off, int n_mol, int max_n,
+                      int directional, float* out, cudaStream_t st);
+
+}  // namespace fss

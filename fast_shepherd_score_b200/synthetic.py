@@ -1,0 +1,127 @@
+"""Seeded synthetic molecule clouds with the shapes and value distributions of the
+benchmark workloads (no public dataset is used; every workload is generated here).
+
+* ``ball_clouds``     -- atoms rejection-sampled uniformly in a 6 A ball, >= 1.2 A apart
+* ``sphere_clouds``   -- surface points 5 A * u + N(0, 0.3^2), u uniform on S^2, charges N(0, 0.1^2)
+* ``pharm_features``  -- 3-20 pharmacophores per molecule, 8 types uniform, anchors jittered
+  N(0, 0.5^2) around random atoms, unit vectors on S^2 for the directional types
+  (acceptor, donor, aromatic, halogen) and zero for the rest
+* ``shape_pairs`` / ``esp_surface_pairs`` / ``shape_pharm_pairs`` -- the pair batches
+
+All generators are numpy ``default_rng(seed)`` based and vectorised over molecules, so the
+same seed gives the same data on every machine.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+DIRECTIONAL_TYPES = (0, 1, 2, 4)   # Acceptor, Donor, Aromatic, Halogen
+N_PHARM_TYPES = 8                   # real types 0..7; 8 is the Dummy padding type
+
+
+def ball_clouds(rng, counts, radius=6.0, min_dist=1.2, max_tries=200):
+    """Uniform points in a ball with a minimum pairwise spacing, one cloud per count.
+
+    Vectorised over molecules: slot s is proposed for every molecule at once and
+    re-proposed only where it violates the spacing against slots < s.
+    Returns a list of float32 (n_i, 3) arrays.
+    """
+    counts = np.asarray(counts, np.int64)
+    K = len(counts)
+    nmax = int(counts.max()) if K else 0
+    X = np.zeros((K, nmax, 3), np.float64)
+    md2 = min_dist * min_dist
+
+    def propose(n):
+        v = rng.standard_normal((n, 3))
+        v /= np.linalg.norm(v, axis=1, keepdims=True)
+        r = radius * rng.random(n) ** (1.0 / 3.0)
+        return v * r[:, None]
+
+    for s in range(nmax):
+        need = np.nonzero(counts > s)[0]
+        for _ in range(max_tries):
+            if need.size == 0:
+                break
+            cand = propose(need.size)
+            if s == 0:
+                X[need, 0] = cand
+                need = need[:0]
+                break
+            d2 = ((X[need, :s] - cand[:, None, :]) ** 2).sum(-1).min(1)
+            ok = d2 >= md2
+            X[need[ok], s] = cand[ok]
+            need = need[~ok]
+        if need.size:  # crowded ball: accept the last proposal rather than loop forever
+            X[need, s] = propose(need.size)
+    return [X[i, :counts[i]].astype(np.float32) for i in range(K)]
+
+
+def sphere_clouds(rng, counts, radius=5.0, jitter=0.3, charge_sd=0.1):
+    """Surface-like clouds: points 5*u + N(0, 0.3^2) and per-point charges N(0, 0.1^2)."""
+    out = []
+    for n in np.asarray(counts, np.int64):
+        u = rng.standard_normal((n, 3))
+        u /= np.linalg.norm(u, axis=1, keepdims=True)
+        p = radius * u + jitter * rng.standard_normal((n, 3))
+        c = charge_sd * rng.standard_normal(n)
+        out.append((p.astype(np.float32), c.astype(np.float32)))
+    return out
+
+
+def pharm_features(rng, atoms, counts, jitter=0.5):
+    """Pharmacophores near the atoms of each molecule: (types int64, anchors, vectors)."""
+    out = []
+    for X, n in zip(atoms, np.asarray(counts, np.int64)):
+        types = rng.integers(0, N_PHARM_TYPES, n)
+        idx = rng.integers(0, len(X), n)
+        anc = X[idx] + jitter * rng.standard_normal((n, 3))
+        v = rng.standard_normal((n, 3))
+        v /= np.linalg.norm(v, axis=1, keepdims=True)
+        v[~np.isin(types, DIRECTIONAL_TYPES)] = 0.0
+        out.append((types.astype(np.int64), anc.astype(np.float32), v.astype(np.float32)))
+    return out
+
+
+def shape_pairs(n_pairs, seed=0, lo=15, hi=50):
+    """Atom-cloud pairs (ref, fit) with lo..hi atoms each (6 A ball, 1.2 A spacing)."""
+    rng = np.random.default_rng(seed)
+    nr = rng.integers(lo, hi + 1, n_pairs)
+    nf = rng.integers(lo, hi + 1, n_pairs)
+    refs = ball_clouds(rng, nr)
+    fits = ball_clouds(rng, nf)
+    return refs, fits
+
+
+def esp_surface_pairs(n_pairs, seed=1, lo=200, hi=400):
+    """Surface pairs with charges: lists of (points, charges) for ref and fit."""
+    rng = np.random.default_rng(seed)
+    nr = rng.integers(lo, hi + 1, n_pairs)
+    nf = rng.integers(lo, hi + 1, n_pairs)
+    return sphere_clouds(rng, nr), sphere_clouds(rng, nf)
+
+
+def shape_pharm_molecules(n_mol, rng, atom_lo=15, atom_hi=60, ph_lo=3, ph_hi=20):
+    """Molecules of atoms + pharmacophores: list of dicts (atom_pos, pharm_types/ancs/vecs)."""
+    na = rng.integers(atom_lo, atom_hi + 1, n_mol)
+    npf = rng.integers(ph_lo, ph_hi + 1, n_mol)
+    atoms = ball_clouds(rng, na)
+    feats = pharm_features(rng, atoms, npf)
+    return [dict(atom_pos=a, pharm_types=f[0], pharm_ancs=f[1], pharm_vecs=f[2])
+            for a, f in zip(atoms, feats)]
+
+
+def shape_pharm_pairs(n_pairs, seed=2, **kw):
+    """Pairs of shape+pharmacophore molecules (ref list, fit list)."""
+    rng = np.random.default_rng(seed)
+    return shape_pharm_molecules(n_pairs, rng, **kw), shape_pharm_molecules(n_pairs, rng, **kw)
+
+
+def random_rotation(rng):
+    """Uniform random rotation matrix (float64)."""
+    q = rng.standard_normal(4)
+    q /= np.linalg.norm(q)
+    w, x, y, z = q
+    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                     [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                     [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])

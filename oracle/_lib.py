@@ -1,0 +1,61 @@
+"""ctypes binding of ``libfss_oracle.so`` (test infrastructure only; see ``oracle/__init__``)."""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_SO = os.path.join(_HERE, "libfss_oracle.so")
+_LIB = None
+
+MODE_SHAPE, MODE_ESP, MODE_PHARM, MODE_COMBO, MODE_COLOR_COMBO = 0, 1, 2, 3, 4
+
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_vp = ctypes.c_void_p
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with its Makefile (gcc, no GPU needed)."""
+    src = os.path.join(_HERE, "fss_oracle.c")
+    if force or not os.path.exists(_SO) or os.path.getmtime(_SO) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _SO
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(_SO):
+            build()
+        L = ctypes.CDLL(_SO)
+        L.fsso_overlap_grad.argtypes = [ctypes.c_int] * 3 + [_vp] * 6 + [_vp, _vp] + [
+            ctypes.c_double, ctypes.c_double, ctypes.c_int, _vp, _vp, _vp, ctypes.c_int]
+        L.fsso_overlap_grad.restype = None
+        L.fsso_pharm_grad.argtypes = [ctypes.c_int] * 3 + [_vp] * 10 + [_vp] * 3 + [
+            ctypes.c_int, _vp, _vp, _vp, ctypes.c_int]
+        L.fsso_pharm_grad.restype = None
+        L.fsso_fine_loop_flat.argtypes = (
+            [ctypes.c_int] * 4 + [_vp] * 6 + [ctypes.c_int] * 2 + [_vp] * 11 +
+            [ctypes.c_double] * 3 + [_vp] * 4 + [ctypes.c_int, ctypes.c_float, ctypes.c_int,
+                                                  ctypes.c_double] + [_vp] * 3 + [ctypes.c_int])
+        L.fsso_fine_loop_flat.restype = ctypes.c_int
+        L.fsso_max_threads.restype = ctypes.c_int
+        _LIB = L
+    return _LIB
+
+
+def ptr(a):
+    """Raw data pointer of a C-contiguous numpy array (None -> NULL)."""
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "oracle arrays must be C-contiguous"
+    return a.ctypes.data
+
+
+def max_threads() -> int:
+    return int(lib().fsso_max_threads())

@@ -1,0 +1,306 @@
+"""Oracle drivers: the reference's batched alignment restated on CPU (test infrastructure only).
+
+Each ``align_*`` function follows one reference driver on its CPU (numba, fused) branch:
+
+* :func:`align_shape` -- ``coarse_fine_align_many`` (shepherd_score/accel/drivers/shape.py:155-313)
+  through ``cpu_fused_shape`` (accel/kernels/cpu_fused.py:225)
+* :func:`align_esp`   -- ``coarse_fine_esp_align_many`` (accel/drivers/esp.py:139-367) through
+  ``cpu_fused_esp`` (cpu_fused.py:251)
+* :func:`align_pharm` -- ``coarse_fine_pharm_align_many`` (accel/drivers/pharm.py:123-517) through
+  ``cpu_fused_pharm`` (cpu_fused.py:278), including the anchor centring (pharm.py:205-225)
+  and the translation fold-back (pharm.py:509-517)
+* :func:`align_combo` -- shape + directional pharmacophore with one shared pose, composed from
+  ``cpu._overlap_grad_kernel`` + ``cpu._pharm_grad_dq_kernel`` and the two-channel tail
+  ``cpu_fused._tail_vol_color`` (cpu_fused.py:112); with ``directional=False`` it is
+  ``coarse_fine_vol_color_align_many`` (accel/drivers/vol_color.py:199) on its CPU branch.
+
+Early stop: ``es_patience=None`` disables it (the alignment configs run fixed steps);
+an integer follows ``fine_loop_cpu``'s batch-global schedule (cpu_fused.py:208-215).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import _lib
+from .seeds import batched_seeds, quat_to_rotmat
+
+P_TYPES = ('Acceptor', 'Donor', 'Aromatic', 'Hydrophobe', 'Halogen', 'Cation', 'Anion',
+           'ZnBinder', 'Dummy')
+_P_ALPHAS = {'acceptor': 1.0, 'donor': 1.0, 'aromatic': 0.7, 'hydrophobe': 0.7, 'cation': 1.0,
+             'anion': 1.0, 'znbinder': 1.0, 'halogen': 1.0, 'dummy': 1.0}
+_NONDIR = {'hydrophobe', 'znbinder', 'anion', 'cation'}
+_DIR = {'acceptor', 'donor', 'halogen'}
+_AROM = {'aromatic'}
+DUMMY_TYPE = P_TYPES.index('Dummy')
+LAM_SCALING = (1e4 / (4 * 55.263 * np.pi)) ** 2
+
+
+def lookup_tables(directionless: bool = False):
+    """(alphas, Ks, cats) per pharmacophore type (analytical_gradients/_torch.py:177-220).
+
+    The reference builds these as float32 tensors and the numba path widens them to float64
+    (cpu_fused.py:285-286), so the float32 rounding is kept here.
+    """
+    al, ks, cats = [], [], []
+    for p in P_TYPES:
+        pl = p.lower()
+        a = _P_ALPHAS.get(pl, 1.0)
+        al.append(a)
+        ks.append((math.pi / (2.0 * a)) ** 1.5)
+        if pl == 'dummy':
+            cats.append(3)
+        elif directionless or pl in _NONDIR:
+            cats.append(0)
+        elif pl in _DIR:
+            cats.append(1)
+        elif pl in _AROM:
+            cats.append(2)
+        else:
+            cats.append(3)
+    return (np.asarray(al, np.float32).astype(np.float64),
+            np.asarray(ks, np.float32).astype(np.float64),
+            np.asarray(cats, np.int32))
+
+
+def _f32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _i32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _threads(n):
+    return _lib.max_threads() if n is None else int(n)
+
+
+def overlap_grad(A, B, q, t, N_real=None, M_real=None, *, alpha=0.81, CA=None, CB=None,
+                 lam=None, need_grad=True, nthreads=None):
+    """Shape (or ESP when CA/CB given) overlap and dV/dq, dV/dt per pose, float64.
+
+    cpu.py:38-109 (shape) and cpu.py:158-225 (ESP; ``lam`` is the kernel's lambda).
+    """
+    A, B, q, t = _f32(A), _f32(B), _f32(q), _f32(t)
+    K, Npad, _ = A.shape
+    Mpad = B.shape[1]
+    Nr = _i32(np.full(K, Npad) if N_real is None else N_real)
+    Mr = _i32(np.full(K, Mpad) if M_real is None else M_real)
+    CA, CB = _f32(CA), _f32(CB)
+    V = np.zeros(K, np.float64)
+    dQ = np.zeros((K, 4), np.float64)
+    dT = np.zeros((K, 3), np.float64)
+    inv_lam = 0.0 if CA is None else 1.0 / float(lam)
+    P = _lib.ptr
+    _lib.lib().fsso_overlap_grad(K, Npad, Mpad, P(A), P(B), P(CA), P(CB), P(q), P(t), P(Nr),
+                                 P(Mr), float(alpha), inv_lam, int(bool(need_grad)), P(V),
+                                 P(dQ), P(dT), _threads(nthreads))
+    return V, dQ, dT
+
+
+def pharm_grad(A, B, RV, FV, At, Bt, q, t, N_real=None, M_real=None, *, directionless=False,
+               need_grad=True, nthreads=None):
+    """Typed pharmacophore overlap and dO/dq, dO/dt per pose, float64 (cpu.py:412-612)."""
+    A, B, q, t = _f32(A), _f32(B), _f32(q), _f32(t)
+    RV, FV = _f32(RV), _f32(FV)
+    At, Bt = _i32(At), _i32(Bt)
+    K, Npad, _ = A.shape
+    Mpad = B.shape[1]
+    Nr = _i32(np.full(K, Npad) if N_real is None else N_real)
+    Mr = _i32(np.full(K, Mpad) if M_real is None else M_real)
+    al, ks, cats = lookup_tables(directionless)
+    O = np.zeros(K, np.float64)
+    dQ = np.zeros((K, 4), np.float64)
+    dT = np.zeros((K, 3), np.float64)
+    P = _lib.ptr
+    _lib.lib().fsso_pharm_grad(K, Npad, Mpad, P(A), P(B), P(RV), P(FV), P(At), P(Bt), P(q),
+                               P(t), P(Nr), P(Mr), P(al), P(ks), P(cats),
+                               int(bool(need_grad)), P(O), P(dQ), P(dT), _threads(nthreads))
+    return O, dQ, dT
+
+
+def _identity_pose(K):
+    q = np.zeros((K, 4), np.float32)
+    q[:, 0] = 1.0
+    return q, np.zeros((K, 3), np.float32)
+
+
+def self_overlap(X, N_real, *, alpha=0.81, C=None, lam=None, nthreads=None):
+    """V_XX at the identity pose, float32 as the reference returns it (cpu.py:140-148, :615-624)."""
+    q, t = _identity_pose(X.shape[0])
+    V, _, _ = overlap_grad(X, X, q, t, N_real, N_real, alpha=alpha, CA=C, CB=C, lam=lam,
+                           need_grad=False, nthreads=nthreads)
+    return V.astype(np.float32)
+
+
+def pharm_self_overlap(X, V, T, N_real, *, directionless=False, nthreads=None):
+    """Pharmacophore self-overlap via the dq kernel at identity (pharm.py:336-346)."""
+    q, t = _identity_pose(X.shape[0])
+    O, _, _ = pharm_grad(X, X, V, V, T, T, q, t, N_real, N_real, directionless=directionless,
+                         need_grad=False, nthreads=nthreads)
+    return O.astype(np.float32)
+
+
+def fine_loop(mode, q_seed, t_seed, norm_s, *, steps, lr, es_patience=None, es_tol=1e-5,
+              A=None, B=None, CA=None, CB=None, Nr=None, Mr=None, alpha=0.81, lam=None,
+              PA=None, PB=None, PRV=None, PFV=None, PAt=None, PBt=None, PNr=None, PMr=None,
+              directionless=False, norm_c=None, w=0.5, nthreads=None):
+    """Run the fused fine loop over K pose rows (cpu_fused.py:179-217).
+
+    All per-row arrays are already expanded to K = pairs x starts rows.  Returns
+    (best score (K,), best q (K,4), best t (K,3), final q, final t, steps run).
+    """
+    q = np.array(q_seed, np.float32, copy=True, order='C')
+    t = np.array(t_seed, np.float32, copy=True, order='C')
+    K = q.shape[0]
+    best = np.empty(K, np.float32)
+    bq = np.empty((K, 4), np.float32)
+    bt = np.empty((K, 3), np.float32)
+    A, B, CA, CB = _f32(A), _f32(B), _f32(CA), _f32(CB)
+    PA, PB, PRV, PFV = _f32(PA), _f32(PB), _f32(PRV), _f32(PFV)
+    Nr, Mr, PAt, PBt, PNr, PMr = _i32(Nr), _i32(Mr), _i32(PAt), _i32(PBt), _i32(PNr), _i32(PMr)
+    norm_s = _f32(norm_s)
+    norm_c = _f32(norm_c)
+    Npad = A.shape[1] if A is not None else 0
+    Mpad = B.shape[1] if B is not None else 0
+    Ppad = PA.shape[1] if PA is not None else 0
+    Qpad = PB.shape[1] if PB is not None else 0
+    al, ks, cats = lookup_tables(directionless)
+    inv_lam = 0.0 if lam is None else 1.0 / float(lam)
+    P = _lib.ptr
+    n = _lib.lib().fsso_fine_loop_flat(
+        int(mode), K, Npad, Mpad, P(A), P(B), P(CA), P(CB), P(Nr), P(Mr), Ppad, Qpad, P(PA),
+        P(PB), P(PRV), P(PFV), P(PAt), P(PBt), P(PNr), P(PMr), P(al), P(ks), P(cats),
+        float(alpha), inv_lam, float(w), P(norm_s), P(norm_c), P(q), P(t), int(steps),
+        float(np.float32(lr)), -1 if es_patience is None else int(es_patience), float(es_tol),
+        P(best), P(bq), P(bt), _threads(nthreads))
+    if n < 0:
+        raise MemoryError("oracle fine loop could not allocate its Adam state")
+    return best, bq, bt, q, t, n
+
+
+def _rep(x, S):
+    return np.repeat(np.asarray(x), S, axis=0)
+
+
+def _pick(best, bq, bt, nb, S):
+    """Per-pair argmax over starts (shape.py:306-313)."""
+    sc = best.reshape(nb, S)
+    i = sc.argmax(1)
+    ar = np.arange(nb)
+    return sc[ar, i], bq.reshape(nb, S, 4)[ar, i], bt.reshape(nb, S, 3)[ar, i]
+
+
+def align_shape(A, B, N_real, M_real, *, alpha=0.81, num_seeds=50, steps=100, lr=0.075,
+                seeds=None, es_patience=None, es_tol=1e-5, nthreads=None, return_rows=False):
+    """Batched shape alignment (vol / surf): shape.py:155-313 on its CPU fused branch."""
+    A, B = _f32(A), _f32(B)
+    nb = A.shape[0]
+    if seeds is None:
+        seeds = batched_seeds(A, B, N_real, M_real, num_seeds)
+    qs, ts = seeds
+    S = qs.shape[1]
+    norm = (self_overlap(A, N_real, alpha=alpha, nthreads=nthreads)
+            + self_overlap(B, M_real, alpha=alpha, nthreads=nthreads)).astype(np.float32)
+    best, bq, bt, _, _, n = fine_loop(
+        0, qs.reshape(-1, 4), ts.reshape(-1, 3), _rep(norm, S), steps=steps, lr=lr,
+        es_patience=es_patience, es_tol=es_tol, A=_rep(A, S), B=_rep(B, S),
+        Nr=_rep(N_real, S), Mr=_rep(M_real, S), alpha=alpha, nthreads=nthreads)
+    out = _pick(best, bq, bt, nb, S)
+    return (out + ((best, bq, bt),)) if return_rows else out
+
+
+def align_esp(A, B, CA, CB, N_real, M_real, *, alpha=0.81, lam=0.3, num_seeds=50, steps=100,
+              lr=0.075, seeds=None, es_patience=None, es_tol=1e-5, nthreads=None,
+              return_rows=False):
+    """Batched ESP alignment (surf_esp / vol_esp): esp.py:139-367 on its CPU fused branch.
+
+    ``lam`` is the kernel lambda (surf_esp callers pass LAM_SCALING * lam, aligners.py:383).
+    """
+    A, B = _f32(A), _f32(B)
+    nb = A.shape[0]
+    if seeds is None:
+        seeds = batched_seeds(A, B, N_real, M_real, num_seeds)
+    qs, ts = seeds
+    S = qs.shape[1]
+    norm = (self_overlap(A, N_real, alpha=alpha, C=CA, lam=lam, nthreads=nthreads)
+            + self_overlap(B, M_real, alpha=alpha, C=CB, lam=lam, nthreads=nthreads)
+            ).astype(np.float32)
+    best, bq, bt, _, _, n = fine_loop(
+        1, qs.reshape(-1, 4), ts.reshape(-1, 3), _rep(norm, S), steps=steps, lr=lr,
+        es_patience=es_patience, es_tol=es_tol, A=_rep(A, S), B=_rep(B, S), CA=_rep(CA, S),
+        CB=_rep(CB, S), Nr=_rep(N_real, S), Mr=_rep(M_real, S), alpha=alpha, lam=lam,
+        nthreads=nthreads)
+    out = _pick(best, bq, bt, nb, S)
+    return (out + ((best, bq, bt),)) if return_rows else out
+
+
+def center_anchors(X, N_real):
+    """Centroid over real points and the centred cloud (pharm.py:205-225)."""
+    X = _f32(X)
+    npad = X.shape[1]
+    mask = (np.arange(npad)[None] < np.asarray(N_real)[:, None]).astype(np.float32)
+    c = (X * mask[..., None]).sum(1, dtype=np.float32) / np.maximum(
+        np.asarray(N_real, np.float32), 1)[:, None]
+    return c.astype(np.float32), (X - c[:, None, :]).astype(np.float32)
+
+
+def align_pharm(A, B, RV, FV, At, Bt, N_real, M_real, *, num_seeds=50, steps=100, lr=0.075,
+                seeds=None, es_patience=None, es_tol=1e-5, nthreads=None, return_rows=False):
+    """Batched directional pharmacophore alignment: pharm.py:123-517, CPU fused branch.
+
+    Anchors are centred per cloud before seeding and the optimum translation is folded back
+    into the original frame at the end.  ``seeds`` (if given) are for the centred clouds.
+    """
+    nb = np.asarray(A).shape[0]
+    c_ref, A_c = center_anchors(A, N_real)
+    c_fit, B_c = center_anchors(B, M_real)
+    if seeds is None:
+        seeds = batched_seeds(A_c, B_c, N_real, M_real, num_seeds)
+    qs, ts = seeds
+    S = qs.shape[1]
+    norm = (pharm_self_overlap(A_c, RV, At, N_real, nthreads=nthreads)
+            + pharm_self_overlap(B_c, FV, Bt, M_real, nthreads=nthreads)).astype(np.float32)
+    best, bq, bt, _, _, n = fine_loop(
+        2, qs.reshape(-1, 4), ts.reshape(-1, 3), _rep(norm, S), steps=steps, lr=lr,
+        es_patience=es_patience, es_tol=es_tol, PA=_rep(A_c, S), PB=_rep(B_c, S),
+        PRV=_rep(_f32(RV), S), PFV=_rep(_f32(FV), S), PAt=_rep(At, S), PBt=_rep(Bt, S),
+        PNr=_rep(N_real, S), PMr=_rep(M_real, S), nthreads=nthreads)
+    sc, q, t = _pick(best, bq, bt, nb, S)
+    R = quat_to_rotmat(q.astype(np.float32))
+    t = (t - np.einsum('bij,bj->bi', R, c_fit) + c_ref).astype(np.float32)
+    out = (sc, q, t)
+    return (out + ((best, bq, bt),)) if return_rows else out
+
+
+def align_combo(A, B, N_real, M_real, PA, PB, PRV, PFV, PAt, PBt, PN_real, PM_real, *,
+                alpha=0.81, w=0.5, directional=True, num_seeds=50, steps=100, lr=0.075,
+                seeds=None, es_patience=None, es_tol=1e-5, nthreads=None, return_rows=False):
+    """Shape + pharmacophore alignment with one shared pose and the two-channel tail.
+
+    Seeds come from the atom clouds (vol_color.py:248).  ``directional=False`` reproduces the
+    reference vol_color mode (directionless colour channel).
+    """
+    A, B = _f32(A), _f32(B)
+    nb = A.shape[0]
+    if seeds is None:
+        seeds = batched_seeds(A, B, N_real, M_real, num_seeds)
+    qs, ts = seeds
+    S = qs.shape[1]
+    norm_s = (self_overlap(A, N_real, alpha=alpha, nthreads=nthreads)
+              + self_overlap(B, M_real, alpha=alpha, nthreads=nthreads)).astype(np.float32)
+    dl = not directional
+    norm_c = (pharm_self_overlap(PA, PRV, PAt, PN_real, directionless=dl, nthreads=nthreads)
+              + pharm_self_overlap(PB, PFV, PBt, PM_real, directionless=dl, nthreads=nthreads)
+              ).astype(np.float32)
+    best, bq, bt, _, _, n = fine_loop(
+        3 if directional else 4, qs.reshape(-1, 4), ts.reshape(-1, 3), _rep(norm_s, S),
+        steps=steps, lr=lr, es_patience=es_patience, es_tol=es_tol, A=_rep(A, S), B=_rep(B, S),
+        Nr=_rep(N_real, S), Mr=_rep(M_real, S), alpha=alpha, PA=_rep(_f32(PA), S),
+        PB=_rep(_f32(PB), S), PRV=None if PRV is None else _rep(_f32(PRV), S),
+        PFV=None if PFV is None else _rep(_f32(PFV), S), PAt=_rep(PAt, S), PBt=_rep(PBt, S),
+        PNr=_rep(PN_real, S), PMr=_rep(PM_real, S), directionless=dl, norm_c=_rep(norm_c, S),
+        w=w, nthreads=nthreads)
+    out = _pick(best, bq, bt, nb, S)
+    return (out + ((best, bq, bt),)) if return_rows else out

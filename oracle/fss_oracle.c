@@ -1,0 +1,498 @@
+/*
+ * fss_oracle.c -- CPU restatement of the reference's batched alignment path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the parity oracle and the timed CPU
+ * baseline; the product (fast_shepherd_score_b200) never links or calls it.
+ *
+ * It restates, function by function, the numba CPU twins the reference runs when
+ * its batched aligners get CPU tensors (shepherd_score/accel/kernels/cpu.py and
+ * shepherd_score/accel/kernels/cpu_fused.py):
+ *
+ *   fsso_overlap_grad   <- cpu.py:38-87   (_overlap_grad_kernel)
+ *                          cpu.py:158-200 (_overlap_grad_esp_kernel, when CA/CB given)
+ *   fsso_pharm_dq       <- cpu.py:500-582 (_pharm_grad_dq_kernel, directional pharm)
+ *   fsso_pharm_color    <- cpu.py:412-458 (_pharm_color_grad_kernel, directionless)
+ *   tail_tanimoto       <- cpu_fused.py:54-108  (_tail_tanimoto)
+ *   tail_combo          <- cpu_fused.py:111-167 (_tail_vol_color)
+ *   fsso_fine_loop      <- cpu_fused.py:179-217 (fine_loop_cpu) + the per-mode glue
+ *                          cpu_fused.py:225-338
+ *
+ * Precision follows the numba code: every overlap sum is accumulated in double and
+ * rounded to float at the kernel boundary (the `.astype(np.float32)` in
+ * cpu_fused.py:242); the optimiser state (q, t, Adam moments, best pose) is float
+ * and each tail update is evaluated in double and stored as float, as numba does
+ * when a float64 constant (beta1, beta2, eps) meets a float32 array element.
+ * exp() is the C library exp, the same routine numba's math.exp lowers to.
+ *
+ * Poses are independent unless the batch-global early stop is on, so with early
+ * stop disabled the loop runs pose-major (all steps of one pose, then the next),
+ * which is bit-identical to the step-major order and parallelises over poses on
+ * pthreads.  With early stop on it runs step-major exactly as fine_loop_cpu does.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <pthread.h>
+#include <unistd.h>
+
+/* Minimal dynamic parallel-for over [0, n) on `nthreads` pthreads (the build image's
+ * gcc has no usable OpenMP spec, so the oracle carries its own). */
+typedef void (*range_fn)(void *ctx, int i);
+typedef struct { range_fn fn; void *ctx; int n; int chunk; int next; pthread_mutex_t mu; } pfor_t;
+
+static void *pfor_worker(void *arg) {
+    pfor_t *p = (pfor_t *)arg;
+    for (;;) {
+        pthread_mutex_lock(&p->mu);
+        const int i0 = p->next;
+        p->next += p->chunk;
+        pthread_mutex_unlock(&p->mu);
+        if (i0 >= p->n) break;
+        const int i1 = i0 + p->chunk < p->n ? i0 + p->chunk : p->n;
+        for (int i = i0; i < i1; ++i) p->fn(p->ctx, i);
+    }
+    return NULL;
+}
+
+static void parallel_for(int n, int nthreads, int chunk, range_fn fn, void *ctx) {
+    if (nthreads <= 1 || n <= 1) {
+        for (int i = 0; i < n; ++i) fn(ctx, i);
+        return;
+    }
+    if (nthreads > 256) nthreads = 256;
+    pfor_t p = {fn, ctx, n, chunk > 0 ? chunk : 1, 0, PTHREAD_MUTEX_INITIALIZER};
+    pthread_t th[256];
+    int started = 0;
+    for (int i = 0; i < nthreads - 1; ++i)
+        if (pthread_create(&th[started], NULL, pfor_worker, &p) == 0) ++started;
+    pfor_worker(&p);
+    for (int i = 0; i < started; ++i) pthread_join(th[i], NULL);
+}
+
+#define B1 0.9
+#define B2 0.999
+#define ADAM_EPS 1e-8
+
+enum { FSSO_SHAPE = 0, FSSO_ESP = 1, FSSO_PHARM = 2, FSSO_COMBO = 3, FSSO_COLOR_COMBO = 4 };
+
+static const double K_PI15 = 5.568327996831708; /* pi ** 1.5 */
+
+/* Rotation matrix from a (w,x,y,z) quaternion, as cpu.py:56-58 (q assumed unit). */
+static inline void rotmat(const float *q, double R[9]) {
+    const float qr = q[0], qi = q[1], qj = q[2], qk = q[3];
+    R[0] = 1.0 - 2.0 * (double)(qj * qj + qk * qk);
+    R[1] = 2.0 * (double)(qi * qj - qk * qr);
+    R[2] = 2.0 * (double)(qi * qk + qj * qr);
+    R[3] = 2.0 * (double)(qi * qj + qk * qr);
+    R[4] = 1.0 - 2.0 * (double)(qi * qi + qk * qk);
+    R[5] = 2.0 * (double)(qj * qk - qi * qr);
+    R[6] = 2.0 * (double)(qi * qk - qj * qr);
+    R[7] = 2.0 * (double)(qj * qk + qi * qr);
+    R[8] = 1.0 - 2.0 * (double)(qi * qi + qj * qj);
+}
+
+/* d(R(q) b)/dq contracted with a force f, body-frame point b (cpu.py:80-83). */
+static inline void quat_tail(const double f[3], double bx, double by, double bz,
+                             const float *q, double dQ[4]) {
+    const double qr = q[0], qi = q[1], qj = q[2], qk = q[3];
+    const double fx = f[0], fy = f[1], fz = f[2];
+    dQ[0] += fx * (-2.0 * qk * by + 2.0 * qj * bz) + fy * (2.0 * qk * bx - 2.0 * qi * bz)
+           + fz * (-2.0 * qj * bx + 2.0 * qi * by);
+    dQ[1] += fx * (2.0 * qj * by + 2.0 * qk * bz) + fy * (2.0 * qj * bx - 4.0 * qi * by - 2.0 * qr * bz)
+           + fz * (2.0 * qk * bx + 2.0 * qr * by - 4.0 * qi * bz);
+    dQ[2] += fx * (-4.0 * qj * bx + 2.0 * qi * by + 2.0 * qr * bz) + fy * (2.0 * qi * bx + 2.0 * qk * bz)
+           + fz * (-2.0 * qr * bx + 2.0 * qk * by - 4.0 * qj * bz);
+    dQ[3] += fx * (-4.0 * qk * bx - 2.0 * qr * by + 2.0 * qi * bz) + fy * (2.0 * qr * bx - 4.0 * qk * by + 2.0 * qj * bz)
+           + fz * (2.0 * qi * bx + 2.0 * qj * by);
+}
+
+/* One pose of the shape / ESP overlap with its SE(3) gradient.
+ * A (N,3) ref, B (M,3) fit, optional charges CA (N) / CB (M) (ESP when non-NULL).
+ * Mirrors cpu.py:52-86 and cpu.py:166-199. */
+static void pose_overlap(const float *A, const float *B, const float *CA, const float *CB,
+                         const float *q, const float *t, int n_real, int m_real,
+                         double alpha, double inv_lam, int need_grad,
+                         double *V, double dQ[4], double dT[3]) {
+    const double Kc = K_PI15 / pow(2.0 * alpha, 1.5);
+    const double a2 = alpha / 2.0;
+    double R[9];
+    rotmat(q, R);
+    const double tx = t[0], ty = t[1], tz = t[2];
+    double Vacc = 0.0;
+    dT[0] = dT[1] = dT[2] = 0.0;
+    dQ[0] = dQ[1] = dQ[2] = dQ[3] = 0.0;
+    for (int m = 0; m < m_real; ++m) {
+        const double bx0 = B[3 * m], by0 = B[3 * m + 1], bz0 = B[3 * m + 2];
+        const double bx = R[0] * bx0 + R[1] * by0 + R[2] * bz0 + tx;
+        const double by = R[3] * bx0 + R[4] * by0 + R[5] * bz0 + ty;
+        const double bz = R[6] * bx0 + R[7] * by0 + R[8] * bz0 + tz;
+        double f[3] = {0.0, 0.0, 0.0};
+        const float cbm = CB ? CB[m] : 0.0f;
+        for (int n = 0; n < n_real; ++n) {
+            const double dx = A[3 * n] - bx, dy = A[3 * n + 1] - by, dz = A[3 * n + 2] - bz;
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            double g;
+            if (CA) {
+                const float dc = CA[n] - cbm; /* float32 subtraction, as numba */
+                g = Kc * exp(-a2 * r2 - (double)(dc * dc) * inv_lam);
+            } else {
+                g = Kc * exp(-a2 * r2);
+            }
+            Vacc += g;
+            if (need_grad) {
+                const double c = alpha * g;
+                f[0] += c * dx; f[1] += c * dy; f[2] += c * dz;
+            }
+        }
+        if (need_grad) {
+            dT[0] += f[0]; dT[1] += f[1]; dT[2] += f[2];
+            quat_tail(f, bx0, by0, bz0, q, dQ);
+        }
+    }
+    *V = Vacc;
+}
+
+/* Unit vector with the 1e-12 norm floor of cpu.py:524-526. */
+static inline void unit_vec(const float *v, double out[3]) {
+    const float nrm = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    const double inv = 1.0 / (nrm > 1e-12f ? (double)nrm : 1e-12);
+    out[0] = v[0] * inv; out[1] = v[1] * inv; out[2] = v[2] * inv;
+}
+
+/* One pose of the typed pharmacophore overlap with in-register dO/dq (cpu.py:506-581).
+ * A/B anchors, RV/FV vectors, At/Bt int32 types; alphas/Ks/cats are the 9-entry
+ * lookup tables.  directional==0 gives the directionless colour kernel (cpu.py:418-457),
+ * which is the directional one with every real type in category 0. */
+static void pose_pharm(const float *A, const float *B, const float *RV, const float *FV,
+                       const int32_t *At, const int32_t *Bt, const float *q, const float *t,
+                       int n_real, int m_real, const double *alphas, const double *Ks,
+                       const int32_t *cats, int need_grad,
+                       double *O, double dQ[4], double dT[3]) {
+    double R[9];
+    rotmat(q, R);
+    const double tx = t[0], ty = t[1], tz = t[2];
+    double Oacc = 0.0;
+    dT[0] = dT[1] = dT[2] = 0.0;
+    dQ[0] = dQ[1] = dQ[2] = dQ[3] = 0.0;
+    for (int i = 0; i < m_real; ++i) {
+        const int ityp = Bt[i];
+        const int icat = cats[ityp];
+        if (icat == 3) continue;
+        const double ialpha = alphas[ityp], iK = Ks[ityp];
+        const double fax0 = B[3 * i], fay0 = B[3 * i + 1], faz0 = B[3 * i + 2];
+        double fv[3] = {0.0, 0.0, 0.0};
+        if (FV) unit_vec(FV + 3 * i, fv);
+        const double fatx = R[0] * fax0 + R[1] * fay0 + R[2] * faz0 + tx;
+        const double faty = R[3] * fax0 + R[4] * fay0 + R[5] * faz0 + ty;
+        const double fatz = R[6] * fax0 + R[7] * fay0 + R[8] * faz0 + tz;
+        const double fvtx = R[0] * fv[0] + R[1] * fv[1] + R[2] * fv[2];
+        const double fvty = R[3] * fv[0] + R[4] * fv[1] + R[5] * fv[2];
+        const double fvtz = R[6] * fv[0] + R[7] * fv[1] + R[8] * fv[2];
+        double f[3] = {0.0, 0.0, 0.0};   /* positional force sum_j alpha*K*w*E*(ref - rotfit) */
+        double wf[3] = {0.0, 0.0, 0.0};  /* weight force sum_j coeff * ref_vn */
+        for (int j = 0; j < n_real; ++j) {
+            if (At[j] != ityp) continue;
+            const double dx = fatx - A[3 * j], dy = faty - A[3 * j + 1], dz = fatz - A[3 * j + 2];
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            const double E = exp(-ialpha * 0.5 * r2);
+            double rv[3] = {0.0, 0.0, 0.0};
+            double w = 1.0, c = 0.0;
+            if (icat == 1 || icat == 2) {
+                unit_vec(RV + 3 * j, rv);
+                const double D = fvtx * rv[0] + fvty * rv[1] + fvtz * rv[2];
+                if (icat == 1) {
+                    const double Dcl = D < 0.0 ? 0.0 : (D > 1.0 ? 1.0 : D);
+                    w = (Dcl + 2.0) / 3.0;
+                    c = (D > 0.0 && D < 1.0) ? 1.0 : 0.0;
+                } else {
+                    w = (fabs(D) + 2.0) / 3.0;
+                    c = D > 0.0 ? 1.0 : (D < 0.0 ? -1.0 : 0.0);
+                }
+            }
+            const double KwE = iK * w * E;
+            Oacc += KwE;
+            if (need_grad) {
+                const double aKwE = -ialpha * KwE;
+                f[0] += aKwE * dx; f[1] += aKwE * dy; f[2] += aKwE * dz;
+                const double coeff = (1.0 / 3.0) * iK * E * c;
+                wf[0] += coeff * rv[0]; wf[1] += coeff * rv[1]; wf[2] += coeff * rv[2];
+            }
+        }
+        if (need_grad) {
+            dT[0] += f[0]; dT[1] += f[1]; dT[2] += f[2];
+            quat_tail(f, fax0, fay0, faz0, q, dQ);
+            quat_tail(wf, fv[0], fv[1], fv[2], q, dQ);
+        }
+    }
+    *O = Oacc;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Public single-evaluation entry points (value + gradient per pose).          */
+/* Arrays are padded: A (K,Npad,3), B (K,Mpad,3), charges (K,Npad)/(K,Mpad).   */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    int Npad, Mpad;
+    const float *A, *B, *CA, *CB, *q, *t;
+    const int32_t *Nr, *Mr;
+    double alpha, inv_lam;
+    int need_grad;
+    double *V, *dQ, *dT;
+} overlap_args;
+
+static void overlap_one(void *ctx, int k) {
+    const overlap_args *a = (const overlap_args *)ctx;
+    pose_overlap(a->A + (size_t)k * a->Npad * 3, a->B + (size_t)k * a->Mpad * 3,
+                 a->CA ? a->CA + (size_t)k * a->Npad : NULL,
+                 a->CB ? a->CB + (size_t)k * a->Mpad : NULL, a->q + 4 * (size_t)k,
+                 a->t + 3 * (size_t)k, a->Nr[k], a->Mr[k], a->alpha, a->inv_lam,
+                 a->need_grad, a->V + k, a->dQ + 4 * (size_t)k, a->dT + 3 * (size_t)k);
+}
+
+void fsso_overlap_grad(int K, int Npad, int Mpad, const float *A, const float *B,
+                       const float *CA, const float *CB, const float *q, const float *t,
+                       const int32_t *Nr, const int32_t *Mr, double alpha, double inv_lam,
+                       int need_grad, double *V, double *dQ, double *dT, int nthreads) {
+    overlap_args a = {Npad, Mpad, A, B, CA, CB, q, t, Nr, Mr, alpha, inv_lam, need_grad, V, dQ, dT};
+    parallel_for(K, nthreads, 4, overlap_one, &a);
+}
+
+typedef struct {
+    int Npad, Mpad;
+    const float *A, *B, *RV, *FV;
+    const int32_t *At, *Bt;
+    const float *q, *t;
+    const int32_t *Nr, *Mr;
+    const double *alphas, *Ks;
+    const int32_t *cats;
+    int need_grad;
+    double *O, *dQ, *dT;
+} pharm_args;
+
+static void pharm_one(void *ctx, int k) {
+    const pharm_args *a = (const pharm_args *)ctx;
+    pose_pharm(a->A + (size_t)k * a->Npad * 3, a->B + (size_t)k * a->Mpad * 3,
+               a->RV ? a->RV + (size_t)k * a->Npad * 3 : NULL,
+               a->FV ? a->FV + (size_t)k * a->Mpad * 3 : NULL, a->At + (size_t)k * a->Npad,
+               a->Bt + (size_t)k * a->Mpad, a->q + 4 * (size_t)k, a->t + 3 * (size_t)k,
+               a->Nr[k], a->Mr[k], a->alphas, a->Ks, a->cats, a->need_grad, a->O + k,
+               a->dQ + 4 * (size_t)k, a->dT + 3 * (size_t)k);
+}
+
+void fsso_pharm_grad(int K, int Npad, int Mpad, const float *A, const float *B,
+                     const float *RV, const float *FV, const int32_t *At, const int32_t *Bt,
+                     const float *q, const float *t, const int32_t *Nr, const int32_t *Mr,
+                     const double *alphas, const double *Ks, const int32_t *cats,
+                     int need_grad, double *O, double *dQ, double *dT, int nthreads) {
+    pharm_args a = {Npad, Mpad, A, B, RV, FV, At, Bt, q, t, Nr, Mr, alphas, Ks, cats,
+                    need_grad, O, dQ, dT};
+    parallel_for(K, nthreads, 4, pharm_one, &a);
+}
+
+/* ------------------------------------------------------------------------- */
+/* Tails (cpu_fused.py:54-167).  State is float; arithmetic as numba types it. */
+/* ------------------------------------------------------------------------- */
+static inline void adam_update(float *q, float *t, const double gq[4], const double gt[3],
+                               float *mq, float *vq, float *mt, float *vt, float lr) {
+    /* tangent projection dq = g - q (g.q) */
+    const double radial = gq[0] * q[0] + gq[1] * q[1] + gq[2] * q[2] + gq[3] * q[3];
+    double dq[4];
+    for (int c = 0; c < 4; ++c) dq[c] = gq[c] - q[c] * radial;
+    for (int c = 0; c < 4; ++c) {
+        mq[c] = (float)(B1 * mq[c] + (1.0 - B1) * dq[c]);
+        vq[c] = (float)(B2 * vq[c] + (1.0 - B2) * dq[c] * dq[c]);
+    }
+    for (int c = 0; c < 4; ++c) {
+        const float lm = lr * mq[c]; /* float32 * float32 in numba */
+        q[c] = (float)(q[c] - lm / sqrt(vq[c] + ADAM_EPS));
+    }
+    for (int c = 0; c < 3; ++c) {
+        mt[c] = (float)(B1 * mt[c] + (1.0 - B1) * gt[c]);
+        vt[c] = (float)(B2 * vt[c] + (1.0 - B2) * gt[c] * gt[c]);
+    }
+    for (int c = 0; c < 3; ++c) {
+        const float lm = lr * mt[c];
+        t[c] = (float)(t[c] - lm / sqrt(vt[c] + ADAM_EPS));
+    }
+    float qn = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    const double qnd = qn < 1e-12f ? 1e-12 : (double)qn;
+    for (int c = 0; c < 4; ++c) q[c] = (float)(q[c] / qnd);
+}
+
+static inline void track_best(double score, const float *q, const float *t,
+                              float *best, float *bq, float *bt) {
+    if (score > (double)*best) {
+        *best = (float)score;
+        memcpy(bq, q, 4 * sizeof(float));
+        memcpy(bt, t, 3 * sizeof(float));
+    }
+}
+
+/* single-channel Tanimoto tail (cpu_fused.py:54-108) */
+static void tail_tanimoto(float O, const float dQf[4], const float dTf[3], float norm,
+                          float *q, float *t, float *mq, float *vq, float *mt, float *vt,
+                          float *best, float *bq, float *bt, float lr) {
+    float denom32 = norm - O;
+    const double denom = denom32 == 0.0f ? 1e-12 : (double)denom32;
+    const double score = O / denom;
+    const double scale = norm / (denom * denom);
+    track_best(score, q, t, best, bq, bt);
+    double gq[4], gt[3];
+    for (int c = 0; c < 4; ++c) gq[c] = -scale * dQf[c];
+    for (int c = 0; c < 3; ++c) gt[c] = -scale * dTf[c];
+    adam_update(q, t, gq, gt, mq, vq, mt, vt, lr);
+}
+
+/* two-channel tail: (1-w)*shape Tanimoto + w*pharm Tanimoto (cpu_fused.py:111-167) */
+static void tail_combo(float Vs, const float dQs[4], const float dTs[3], float Oc,
+                       const float dQc[4], const float dTc[3], float norm_s, float norm_c,
+                       float w, float *q, float *t, float *mq, float *vq, float *mt, float *vt,
+                       float *best, float *bq, float *bt, float lr) {
+    float ds32 = norm_s - Vs;
+    const double ds = ds32 == 0.0f ? 1e-12 : (double)ds32;
+    const double ss = Vs / ds, scale_s = norm_s / (ds * ds);
+    float dc32 = norm_c - Oc;
+    const double dc = dc32 == 0.0f ? 1e-12 : (double)dc32;
+    const double sc = Oc / dc, scale_c = norm_c / (dc * dc);
+    const double wd = (double)w;
+    const double score = (1.0 - wd) * ss + wd * sc;
+    track_best(score, q, t, best, bq, bt);
+    const double cs = -(1.0 - wd) * scale_s, cc = -wd * scale_c;
+    double gq[4], gt[3];
+    for (int c = 0; c < 4; ++c) gq[c] = cs * dQs[c] + cc * dQc[c];
+    for (int c = 0; c < 3; ++c) gt[c] = cs * dTs[c] + cc * dTc[c];
+    adam_update(q, t, gq, gt, mq, vq, mt, vt, lr);
+}
+
+/* ------------------------------------------------------------------------- */
+/* Fine loop (cpu_fused.py:179-217).                                           */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    int mode;              /* FSSO_SHAPE .. FSSO_COLOR_COMBO */
+    int K, Npad, Mpad;     /* shape (or ESP) channel: poses, padded ref/fit points */
+    const float *A, *B, *CA, *CB;
+    const int32_t *Nr, *Mr;
+    int Ppad, Qpad;        /* pharm channel padding (ref, fit) */
+    const float *PA, *PB, *PRV, *PFV;
+    const int32_t *PAt, *PBt, *PNr, *PMr;
+    const double *alphas, *Ks;
+    const int32_t *cats;
+    double alpha, inv_lam, w;
+    const float *norm_s, *norm_c; /* per pose self-overlap sums */
+} fsso_problem;
+
+/* Evaluate the channels of one pose and apply its tail (one optimisation step). */
+static void pose_step(const fsso_problem *P, int k, float *q, float *t, float *mq, float *vq,
+                      float *mt, float *vt, float *best, float *bq, float *bt, float lr) {
+    double V, dQ[4], dT[3];
+    float Vf = 0.0f, dQf[4] = {0, 0, 0, 0}, dTf[3] = {0, 0, 0};
+    if (P->mode == FSSO_SHAPE || P->mode == FSSO_ESP || P->mode == FSSO_COMBO ||
+        P->mode == FSSO_COLOR_COMBO) {
+        pose_overlap(P->A + (size_t)k * P->Npad * 3, P->B + (size_t)k * P->Mpad * 3,
+                     P->mode == FSSO_ESP ? P->CA + (size_t)k * P->Npad : NULL,
+                     P->mode == FSSO_ESP ? P->CB + (size_t)k * P->Mpad : NULL, q, t,
+                     P->Nr[k], P->Mr[k], P->alpha, P->inv_lam, 1, &V, dQ, dT);
+        Vf = (float)V;
+        for (int c = 0; c < 4; ++c) dQf[c] = (float)dQ[c];
+        for (int c = 0; c < 3; ++c) dTf[c] = (float)dT[c];
+    }
+    if (P->mode == FSSO_SHAPE || P->mode == FSSO_ESP) {
+        tail_tanimoto(Vf, dQf, dTf, P->norm_s[k], q, t, mq, vq, mt, vt, best, bq, bt, lr);
+        return;
+    }
+    double O, dQp[4], dTp[3];
+    float Of, dQpf[4], dTpf[3];
+    pose_pharm(P->PA + (size_t)k * P->Ppad * 3, P->PB + (size_t)k * P->Qpad * 3,
+               P->PRV ? P->PRV + (size_t)k * P->Ppad * 3 : NULL,
+               P->PFV ? P->PFV + (size_t)k * P->Qpad * 3 : NULL,
+               P->PAt + (size_t)k * P->Ppad, P->PBt + (size_t)k * P->Qpad, q, t,
+               P->PNr[k], P->PMr[k], P->alphas, P->Ks, P->cats, 1, &O, dQp, dTp);
+    Of = (float)O;
+    for (int c = 0; c < 4; ++c) dQpf[c] = (float)dQp[c];
+    for (int c = 0; c < 3; ++c) dTpf[c] = (float)dTp[c];
+    if (P->mode == FSSO_PHARM) {
+        tail_tanimoto(Of, dQpf, dTpf, P->norm_s[k], q, t, mq, vq, mt, vt, best, bq, bt, lr);
+        return;
+    }
+    tail_combo(Vf, dQf, dTf, Of, dQpf, dTpf, P->norm_s[k], P->norm_c[k], (float)P->w, q, t,
+               mq, vq, mt, vt, best, bq, bt, lr);
+}
+
+typedef struct {
+    const fsso_problem *P;
+    float *q, *t, *mq, *vq, *mt, *vt, *best, *bq, *bt;
+    float lr;
+    int nsteps;
+} loop_args;
+
+static void pose_all_steps(void *ctx, int k) {
+    const loop_args *a = (const loop_args *)ctx;
+    for (int s = 0; s < a->nsteps; ++s)
+        pose_step(a->P, k, a->q + 4 * (size_t)k, a->t + 3 * (size_t)k, a->mq + 4 * (size_t)k,
+                  a->vq + 4 * (size_t)k, a->mt + 3 * (size_t)k, a->vt + 3 * (size_t)k,
+                  a->best + k, a->bq + 4 * (size_t)k, a->bt + 3 * (size_t)k, a->lr);
+}
+
+/* Runs the fine loop from the seeds (q_io, t_io: in = seed, out = current pose) and
+ * writes best score / best pose per pose.  es_patience < 0 disables early stop;
+ * es_patience >= 0 follows fine_loop_cpu exactly (0 = stop at the first plateau). */
+int fsso_fine_loop(const fsso_problem *P, float *q_io, float *t_io, int steps, float lr,
+                   int es_patience, double es_tol, float *best, float *bq, float *bt,
+                   int nthreads) {
+    const int K = P->K;
+    float *mq = calloc((size_t)K * 4, sizeof(float));
+    float *vq = calloc((size_t)K * 4, sizeof(float));
+    float *mt = calloc((size_t)K * 3, sizeof(float));
+    float *vt = calloc((size_t)K * 3, sizeof(float));
+    if (!mq || !vq || !mt || !vt) { free(mq); free(vq); free(mt); free(vt); return -1; }
+    for (int k = 0; k < K; ++k) {
+        best[k] = -INFINITY;
+        memcpy(bq + 4 * (size_t)k, q_io + 4 * (size_t)k, 4 * sizeof(float));
+        memcpy(bt + 3 * (size_t)k, t_io + 3 * (size_t)k, 3 * sizeof(float));
+    }
+    int steps_run = steps;
+    loop_args la = {P, q_io, t_io, mq, vq, mt, vt, best, bq, bt, lr, steps};
+    if (es_patience < 0) {
+        parallel_for(K, nthreads, 1, pose_all_steps, &la);
+    } else {
+        double prev = -INFINITY;
+        int no_improve = 0;
+        la.nsteps = 1;
+        for (int s = 0; s < steps; ++s) {
+            parallel_for(K, nthreads, 4, pose_all_steps, &la);
+            if (s % 5 == 0) {
+                double cur = -INFINITY;
+                for (int k = 0; k < K; ++k) if (best[k] > cur) cur = best[k];
+                if (cur - prev < es_tol) {
+                    if (++no_improve >= es_patience) { steps_run = s + 1; break; }
+                } else {
+                    no_improve = 0;
+                    prev = cur;
+                }
+            }
+        }
+    }
+    free(mq); free(vq); free(mt); free(vt);
+    return steps_run;
+}
+
+/* Flat-argument wrapper so ctypes callers need no struct layout. */
+int fsso_fine_loop_flat(int mode, int K, int Npad, int Mpad, const float *A, const float *B,
+                        const float *CA, const float *CB, const int32_t *Nr, const int32_t *Mr,
+                        int Ppad, int Qpad, const float *PA, const float *PB, const float *PRV,
+                        const float *PFV, const int32_t *PAt, const int32_t *PBt,
+                        const int32_t *PNr, const int32_t *PMr, const double *alphas,
+                        const double *Ks, const int32_t *cats, double alpha, double inv_lam,
+                        double w, const float *norm_s, const float *norm_c, float *q_io,
+                        float *t_io, int steps, float lr, int es_patience, double es_tol,
+                        float *best, float *bq, float *bt, int nthreads) {
+    fsso_problem P = {mode, K, Npad, Mpad, A, B, CA, CB, Nr, Mr, Ppad, Qpad, PA, PB, PRV, PFV,
+                      PAt, PBt, PNr, PMr, alphas, Ks, cats, alpha, inv_lam, w, norm_s, norm_c};
+    return fsso_fine_loop(&P, q_io, t_io, steps, lr, es_patience, es_tol, best, bq, bt, nthreads);
+}
+
+int fsso_max_threads(void) {
+    const long n = sysconf(_SC_NPROCESSORS_ONLN);
+    return n > 0 ? (int)n : 1;
+}

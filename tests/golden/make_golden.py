@@ -1,0 +1,270 @@
+"""Generate the golden fixtures in this directory by running the REFERENCE implementation.
+
+Run from the repository root on a machine that has the reference source tree:
+
+    python tests/golden/make_golden.py --reference /path/to/fast_shepherd_score
+
+It imports ``shepherd_score`` from that tree (a tiny import-only ``rdkit`` stub is written
+to a temporary directory, because ``shepherd_score.alignment`` imports RDKit at module
+level but the paths used here never call it), runs the reference's own CPU (numba) path
+and its torch scoring functions on small seeded inputs, and writes ``*.npz`` fixtures.
+The fixtures pin the oracle (``tests/test_oracle_golden.py``) and the CUDA path
+(``tests/test_gpu_parity.py``); neither test needs the reference at run time.
+
+Inputs come from ``fast_shepherd_score_b200.synthetic`` with fixed seeds.
+"""
+from __future__ import annotations
+
+import argparse
+import math
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from fast_shepherd_score_b200 import synthetic as syn  # noqa: E402
+
+_STUB = {
+    "rdkit/__init__.py": "",
+    "rdkit/Chem/__init__.py": ("from . import rdchem, rdMolDescriptors, rdMolAlign, AllChem\n"
+                               "def GetPeriodicTable():\n    return None\n"
+                               "def __getattr__(name):\n    return type(name, (), {})\n"),
+    "rdkit/Chem/rdchem.py": "def __getattr__(name):\n    return type(name, (), {})\n",
+    "rdkit/Chem/rdMolDescriptors.py": "def __getattr__(name):\n    return type(name, (), {})\n",
+    "rdkit/Chem/rdMolAlign.py": "def __getattr__(name):\n    return type(name, (), {})\n",
+    "rdkit/Chem/AllChem.py": "def __getattr__(name):\n    return type(name, (), {})\n",
+    "rdkit/Geometry/__init__.py": "",
+    "rdkit/Geometry/rdGeometry.py": "class Point3D:\n    pass\n",
+}
+
+
+def _install_stub():
+    d = tempfile.mkdtemp(prefix="rdkit_stub_")
+    for rel, txt in _STUB.items():
+        p = os.path.join(d, rel)
+        os.makedirs(os.path.dirname(p), exist_ok=True)
+        with open(p, "w") as f:
+            f.write(txt)
+    sys.path.insert(0, d)
+
+
+def pad(clouds, width=None, fill=0.0, dtype=np.float32):
+    """Pad a list of (n_i, ...) arrays into (K, width, ...) plus counts."""
+    n = np.array([len(c) for c in clouds], np.int32)
+    w = int(width or max(n.max(), 1))
+    tail = clouds[0].shape[1:]
+    out = np.full((len(clouds), w) + tail, fill, dtype)
+    for i, c in enumerate(clouds):
+        out[i, :len(c)] = c
+    return out, n
+
+
+def rand_quat(rng, K):
+    q = rng.standard_normal((K, 4)).astype(np.float32)
+    return (q / np.linalg.norm(q, axis=1, keepdims=True)).astype(np.float32)
+
+
+def rotated_copy(rng, X, shift=1.0):
+    R = syn.random_rotation(rng)
+    return ((X @ R.T) + shift * rng.standard_normal(3)).astype(np.float32), R
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=os.environ.get("FSS_REFERENCE", "/root/reference"))
+    args = ap.parse_args()
+    _install_stub()
+    sys.path.insert(0, args.reference)
+    import torch
+    torch.set_num_threads(max(1, os.cpu_count() or 1))
+    from shepherd_score.accel.kernels import cpu as rk
+    from shepherd_score.accel.drivers._common import batched_seeds_torch
+    from shepherd_score.accel.drivers.shape import coarse_fine_align_many
+    from shepherd_score.accel.drivers.esp import coarse_fine_esp_align_many
+    from shepherd_score.accel.drivers.pharm import coarse_fine_pharm_align_many
+    from shepherd_score.accel.drivers.vol_color import coarse_fine_vol_color_align_many
+    from shepherd_score.score.analytical_gradients._torch import build_lookup_tables
+    from shepherd_score.score.constants import LAM_SCALING
+    from shepherd_score.score.gaussian_overlap import get_overlap
+    from shepherd_score.score.electrostatic_scoring import get_overlap_esp
+    from shepherd_score.score.pharmacophore_scoring import get_overlap_pharm, get_pharm_combo_score
+
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a))
+    rng = np.random.default_rng(1234)
+
+    # ---------------- single-evaluation kernels -------------------------------------
+    sizes = [(1, 1), (2, 3), (3, 2), (15, 17), (17, 15), (31, 33), (33, 31), (50, 48)]
+    refs = syn.ball_clouds(rng, [a for a, _ in sizes])
+    fits = syn.ball_clouds(rng, [b for _, b in sizes])
+    A, Nr = pad(refs)
+    B, Mr = pad(fits)
+    K = len(sizes)
+    q = rand_quat(rng, K)
+    t = (0.8 * rng.standard_normal((K, 3))).astype(np.float32)
+    CA = (0.3 * rng.standard_normal(A.shape[:2])).astype(np.float32)
+    CB = (0.3 * rng.standard_normal(B.shape[:2])).astype(np.float32)
+    out = dict(A=A, B=B, N=Nr, M=Mr, q=q, t=t, CA=CA, CB=CB)
+    V, dQ, dT = rk.overlap_score_grad_se3_batch(T(A), T(B), T(q), T(t), alpha=0.81,
+                                                N_real=T(Nr), M_real=T(Mr))
+    out.update(shape_V=V.numpy(), shape_dQ=dQ.numpy(), shape_dT=dT.numpy())
+    for tag, lam in (("esp_surf", 0.3 * LAM_SCALING), ("esp_raw", 0.3)):
+        V, dQ, dT = rk.overlap_score_grad_esp_se3_batch(
+            T(A), T(B), T(CA), T(CB), T(q), T(t), alpha=0.81, lam=lam, N_real=T(Nr), M_real=T(Mr))
+        out.update({f"{tag}_lam": np.float64(lam), f"{tag}_V": V.numpy(),
+                    f"{tag}_dQ": dQ.numpy(), f"{tag}_dT": dT.numpy()})
+    out["self_shape_A"] = rk._batch_self_overlap(T(A), T(Nr), 0.81).numpy()
+    out["self_esp_A"] = rk._batch_self_overlap_esp(T(A), T(CA), T(Nr), 0.81, 0.3).numpy()
+
+    # pharmacophore kernels (directional + directionless colour)
+    psz = [(1, 1), (3, 4), (7, 5), (12, 20), (20, 12), (20, 20)]
+    PA_l, PB_l, PRV_l, PFV_l, PAt_l, PBt_l = [], [], [], [], [], []
+    for na, nb in psz:
+        fr = syn.pharm_features(rng, [refs[-1]], [na])[0]
+        ff = syn.pharm_features(rng, [fits[-1]], [nb])[0]
+        PAt_l.append(fr[0]); PA_l.append(fr[1]); PRV_l.append(fr[2])
+        PBt_l.append(ff[0]); PB_l.append(ff[1]); PFV_l.append(ff[2])
+    PA, PN = pad(PA_l); PB, PM = pad(PB_l)
+    PRV, _ = pad(PRV_l); PFV, _ = pad(PFV_l)
+    PAt, _ = pad(PAt_l, fill=8, dtype=np.int64); PBt, _ = pad(PBt_l, fill=8, dtype=np.int64)
+    Kp = len(psz)
+    pq = rand_quat(rng, Kp)
+    pt = (0.5 * rng.standard_normal((Kp, 3))).astype(np.float32)
+    out.update(PA=PA, PB=PB, PRV=PRV, PFV=PFV, PAt=PAt, PBt=PBt, PN=PN, PM=PM, pq=pq, pt=pt)
+    al, ks, cats = build_lookup_tables(torch.device("cpu"), torch.float32)
+    O, dQ, dT = rk.pharm_grad_dq_se3_batch(T(pq), T(pt), T(PAt), T(PBt), T(PA), T(PB), T(PRV),
+                                           T(PFV), al, ks, cats, N_real=T(PN), M_real=T(PM))
+    out.update(pharm_O=O.numpy(), pharm_dQ=dQ.numpy(), pharm_dT=dT.numpy())
+    al0, ks0, cats0 = build_lookup_tables(torch.device("cpu"), torch.float32, directionless=True)
+    O, dQ, dT = rk.pharm_color_score_grad_se3_batch(T(PA), T(PB), T(pq), T(pt), T(PAt), T(PBt),
+                                                    al0, ks0, cats0, N_real=T(PN), M_real=T(PM))
+    out.update(color_O=O.numpy(), color_dQ=dQ.numpy(), color_dT=dT.numpy())
+    np.savez_compressed(os.path.join(HERE, "kernels.npz"), **out)
+    print("kernels.npz", {k: v.shape for k, v in out.items()})
+
+    # ---------------- seeds ----------------------------------------------------------
+    out = {}
+    srefs = syn.ball_clouds(rng, [20, 2, 35, 9, 50, 1])
+    sfits = syn.ball_clouds(rng, [25, 18, 3, 40, 12, 30])
+    SA, SN = pad(srefs); SB, SM = pad(sfits)
+    out.update(A=SA, B=SB, N=SN, M=SM)
+    for ns in (1, 3, 8, 10, 16, 32, 50):
+        qq, tt = batched_seeds_torch(T(SA), T(SB), T(SN), T(SM), num_seeds=ns)
+        out[f"q_{ns}"] = qq.numpy(); out[f"t_{ns}"] = tt.numpy()
+    np.savez_compressed(os.path.join(HERE, "seeds.npz"), **out)
+    print("seeds.npz")
+
+    # ---------------- batched alignment drivers (numba CPU path, early stop off) --------
+    ES = 10 ** 9
+    out = {}
+    arefs, afits = syn.shape_pairs(6, seed=11)
+    # two self-copies (rotated + shifted): the optimum is a Tanimoto of 1
+    for i in (0, 1):
+        afits[i], _ = rotated_copy(rng, arefs[i])
+    AA, AN = pad(arefs); AB, AM = pad(afits)
+    VAA = rk._batch_self_overlap(T(AA), T(AN), 0.81)
+    VBB = rk._batch_self_overlap(T(AB), T(AM), 0.81)
+    qs, ts = batched_seeds_torch(T(AA), T(AB), T(AN), T(AM), num_seeds=20)
+    sc, bq, bt = coarse_fine_align_many(T(AA), T(AB), VAA, VBB, alpha=0.81, num_seeds=20,
+                                        steps_fine=80, lr=0.1, N_real=T(AN), M_real=T(AM),
+                                        early_stop_patience=ES, seeds=(qs, ts))
+    out.update(shape_A=AA, shape_B=AB, shape_N=AN, shape_M=AM, shape_seeds_q=qs.numpy(),
+               shape_seeds_t=ts.numpy(), shape_score=sc.numpy(), shape_q=bq.numpy(),
+               shape_t=bt.numpy())
+
+    erefs, efits = syn.esp_surface_pairs(4, seed=12, lo=40, hi=90)
+    efits[0] = (rotated_copy(rng, erefs[0][0])[0], erefs[0][1].copy())
+    EA, EN = pad([p for p, _ in erefs]); EB, EM = pad([p for p, _ in efits])
+    ECA, _ = pad([c for _, c in erefs]); ECB, _ = pad([c for _, c in efits])
+    lam_s = 0.3 * LAM_SCALING
+    VAA = rk._batch_self_overlap_esp(T(EA), T(ECA), T(EN), 0.81, lam_s)
+    VBB = rk._batch_self_overlap_esp(T(EB), T(ECB), T(EM), 0.81, lam_s)
+    sc, bq, bt = coarse_fine_esp_align_many(
+        T(EA), T(EB), T(ECA), T(ECB), VAA, VBB, alpha=0.81, lam=lam_s, num_seeds=10,
+        steps_fine=60, lr=0.1, N_real=T(EN), M_real=T(EM), early_stop_patience=ES)
+    qs, ts = batched_seeds_torch(T(EA), T(EB), T(EN), T(EM), num_seeds=10)
+    out.update(esp_A=EA, esp_B=EB, esp_CA=ECA, esp_CB=ECB, esp_N=EN, esp_M=EM,
+               esp_lam=np.float64(lam_s), esp_seeds_q=qs.numpy(), esp_seeds_t=ts.numpy(),
+               esp_score=sc.numpy(), esp_q=bq.numpy(), esp_t=bt.numpy())
+
+    prefs, pfits = syn.shape_pharm_pairs(5, seed=13)
+    pfits[0] = dict(prefs[0])
+    Rr = syn.random_rotation(rng)
+    sh = rng.standard_normal(3)
+    pfits[0]["pharm_ancs"] = (prefs[0]["pharm_ancs"] @ Rr.T + sh).astype(np.float32)
+    pfits[0]["pharm_vecs"] = (prefs[0]["pharm_vecs"] @ Rr.T).astype(np.float32)
+    pfits[0]["atom_pos"] = (prefs[0]["atom_pos"] @ Rr.T + sh).astype(np.float32)
+    PA, PN = pad([m["pharm_ancs"] for m in prefs]); PB, PM = pad([m["pharm_ancs"] for m in pfits])
+    PRV, _ = pad([m["pharm_vecs"] for m in prefs]); PFV, _ = pad([m["pharm_vecs"] for m in pfits])
+    PAt, _ = pad([m["pharm_types"] for m in prefs], fill=0, dtype=np.int64)
+    PBt, _ = pad([m["pharm_types"] for m in pfits], fill=0, dtype=np.int64)
+    dummyV = torch.zeros(len(prefs))
+    sc, bq, bt = coarse_fine_pharm_align_many(
+        T(PA), T(PB), T(PRV), T(PFV), T(PAt), T(PBt), dummyV, dummyV, num_seeds=16,
+        steps_fine=60, lr=0.1, N_real=T(PN), M_real=T(PM), early_stop_patience=ES)
+    out.update(pharm_A=PA, pharm_B=PB, pharm_RV=PRV, pharm_FV=PFV, pharm_At=PAt, pharm_Bt=PBt,
+               pharm_N=PN, pharm_M=PM, pharm_score=sc.numpy(), pharm_q=bq.numpy(),
+               pharm_t=bt.numpy())
+
+    CA_, CN = pad([m["atom_pos"] for m in prefs]); CB_, CM = pad([m["atom_pos"] for m in pfits])
+    PAt8, _ = pad([m["pharm_types"] for m in prefs], fill=8, dtype=np.int64)
+    PBt8, _ = pad([m["pharm_types"] for m in pfits], fill=8, dtype=np.int64)
+    VAA = rk._batch_self_overlap(T(CA_), T(CN), 0.81)
+    VBB = rk._batch_self_overlap(T(CB_), T(CM), 0.81)
+    sc, bq, bt = coarse_fine_vol_color_align_many(
+        T(CA_), T(CB_), T(PAt8), T(PBt8), T(PA), T(PB), VAA, VBB, alpha=0.81, color_weight=0.5,
+        num_seeds=16, steps_fine=60, lr=0.1, N_real_centers=T(CN), M_real_centers=T(CM),
+        N_real_pharm=T(PN), M_real_pharm=T(PM), early_stop_patience=ES)
+    out.update(color_A=CA_, color_B=CB_, color_N=CN, color_M=CM, color_At=PAt8, color_Bt=PBt8,
+               color_score=sc.numpy(), color_q=bq.numpy(), color_t=bt.numpy())
+    np.savez_compressed(os.path.join(HERE, "align.npz"), **out)
+    print("align.npz")
+
+    # ---------------- fp64 torch scoring + autograd coordinate/charge gradients --------
+    out = {}
+    cref = syn.ball_clouds(rng, [24])[0].astype(np.float64)
+    cfit = syn.ball_clouds(rng, [19])[0].astype(np.float64)
+    sref, sfit = syn.sphere_clouds(rng, [60, 70])
+    out.update(c_ref=cref, c_fit=cfit, s_ref=sref[0].astype(np.float64),
+               s_fit=sfit[0].astype(np.float64), q_ref=sref[1].astype(np.float64),
+               q_fit=sfit[1].astype(np.float64))
+    x1 = torch.tensor(cref, requires_grad=True); x2 = torch.tensor(cfit, requires_grad=True)
+    s = get_overlap(x1, x2, alpha=0.81)
+    s.backward()
+    out.update(vol_score=s.detach().numpy(), vol_grad_ref=x1.grad.numpy(),
+               vol_grad_fit=x2.grad.numpy())
+    for tag, lam in (("esp_surf", 0.3 * LAM_SCALING), ("esp_raw", 0.3)):
+        p1 = torch.tensor(out["s_ref"], requires_grad=True)
+        p2 = torch.tensor(out["s_fit"], requires_grad=True)
+        c1 = torch.tensor(out["q_ref"], requires_grad=True)
+        c2 = torch.tensor(out["q_fit"], requires_grad=True)
+        s = get_overlap_esp(p1, p2, c1, c2, alpha=1.216, lam=lam)
+        s.backward()
+        out.update({f"{tag}_lam": np.float64(lam), f"{tag}_score": s.detach().numpy(),
+                    f"{tag}_grad_ref": p1.grad.numpy(), f"{tag}_grad_fit": p2.grad.numpy(),
+                    f"{tag}_gradq_ref": c1.grad.numpy(), f"{tag}_gradq_fit": c2.grad.numpy()})
+    pr = syn.pharm_features(rng, [cref.astype(np.float32)], [9])[0]
+    pf = syn.pharm_features(rng, [cfit.astype(np.float32)], [11])[0]
+    out.update(pt_ref=pr[0], pa_ref=pr[1].astype(np.float64), pv_ref=pr[2].astype(np.float64),
+               pt_fit=pf[0], pa_fit=pf[1].astype(np.float64), pv_fit=pf[2].astype(np.float64))
+    for dl in (False, True):
+        s = get_overlap_pharm(torch.tensor(pr[0]), torch.tensor(pf[0]), torch.tensor(out["pa_ref"]),
+                              torch.tensor(out["pa_fit"]), torch.tensor(out["pv_ref"]),
+                              torch.tensor(out["pv_fit"]), directionless=dl)
+        out[f"pharm_score_dl{int(dl)}"] = s.detach().numpy()
+        s = get_pharm_combo_score(torch.tensor(cref), torch.tensor(cfit), torch.tensor(pr[0]),
+                                  torch.tensor(pf[0]), torch.tensor(out["pa_ref"]),
+                                  torch.tensor(out["pa_fit"]), torch.tensor(out["pv_ref"]),
+                                  torch.tensor(out["pv_fit"]), alpha=0.81, color_weight=0.5,
+                                  directionless=dl)
+        out[f"combo_score_dl{int(dl)}"] = s.detach().numpy()
+    np.savez_compressed(os.path.join(HERE, "scores.npz"), **out)
+    print("scores.npz")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,227 @@
+"""GPU parity of the fused persistent alignment against the reference (golden fixtures)
+and the oracle.  An alignment counts as equal when its best score is within 1e-4 of the
+reference's; Adam's normalised update amplifies fp32 rounding chaotically once a pose has
+converged, so trajectories are compared step-exact only for the first steps and by best
+score afterwards."""
+import numpy as np
+import pytest
+import torch
+
+from fast_shepherd_score_b200 import align as al
+from fast_shepherd_score_b200 import kernels as K
+from fast_shepherd_score_b200 import synthetic as syn
+from fast_shepherd_score_b200.layout import CloudSet, PharmSet
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-4
+
+
+def assert_parity(got, ref, frac=0.75, worst=1e-3):
+    """Best-score parity: most pairs within 1e-4 of the reference, none more than `worst`
+    below it (a higher score is a better alignment found from the same seeds)."""
+    got, ref = np.asarray(got, np.float64), np.asarray(ref, np.float64)
+    eq = np.abs(got - ref) <= TOL
+    assert eq.mean() >= frac, (eq.mean(), got - ref)
+    assert np.max(ref - got) <= worst, (got - ref)
+
+
+def _t(a, dev, dtype=None):
+    t = torch.as_tensor(np.ascontiguousarray(a), device=dev)
+    return t if dtype is None else t.to(dtype)
+
+
+def _pad(clouds, fill=0.0, dtype=np.float32):
+    n = np.array([len(c) for c in clouds])
+    out = np.full((len(clouds), max(n.max(), 1)) + clouds[0].shape[1:], fill, dtype)
+    for i, c in enumerate(clouds):
+        out[i, :len(c)] = c
+    return out, n
+
+
+def test_shape_align_matches_reference(golden, cuda):
+    g = golden["align"]
+    A, B = _t(g["shape_A"], cuda), _t(g["shape_B"], cuda)
+    N, M = _t(g["shape_N"], cuda), _t(g["shape_M"], cuda)
+    VAA = K._batch_self_overlap(A, N, 0.81)
+    VBB = K._batch_self_overlap(B, M, 0.81)
+    seeds = (_t(g["shape_seeds_q"], cuda), _t(g["shape_seeds_t"], cuda))
+    sc, q, t = al.coarse_fine_align_many(A, B, VAA, VBB, alpha=0.81, steps_fine=80, lr=0.1,
+                                         N_real=N, M_real=M, seeds=seeds)
+    sc = sc.cpu().numpy()
+    assert_parity(sc, g["shape_score"])
+    assert (sc[:2] > 0.99).all()
+
+
+def test_shape_rows_track_oracle_stepwise(golden, cuda):
+    """Step 1 (the seeds' own scores) matches the oracle to fp32 rounding; after 3 steps
+    the trajectories still agree to 1e-4 (Adam's normalisation has not amplified yet)."""
+    from oracle import align as oa
+    g = golden["align"]
+    qs, ts = g["shape_seeds_q"], g["shape_seeds_t"]
+    A, B, N, M = g["shape_A"], g["shape_B"], g["shape_N"], g["shape_M"]
+    ref = CloudSet.from_padded(_t(A, cuda), _t(N, cuda))
+    fit = CloudSet.from_padded(_t(B, cuda), _t(M, cuda))
+    idx = torch.arange(len(N), dtype=torch.int32, device=cuda)
+    S = qs.shape[1]
+    for steps in (1, 3):
+        res = al.align_packed("shape", ref=ref, fit=fit, pair_ref=idx, pair_fit=idx,
+                              seed_q=_t(qs, cuda), seed_t=_t(ts, cuda), steps=steps, lr=0.1)
+        rows = res.rows[0].cpu().numpy()
+        _, _, _, (best, _, _) = oa.align_shape(A, B, N, M, alpha=0.81, steps=steps, lr=0.1,
+                                               seeds=(qs, ts), return_rows=True)
+        tol = dict(rtol=2e-5, atol=1e-6) if steps == 1 else dict(rtol=0, atol=1e-4)
+        np.testing.assert_allclose(rows, best, **tol)
+        assert rows.shape == (len(N) * S,)
+
+
+def test_esp_align_matches_reference(golden, cuda):
+    g = golden["align"]
+    A, B = _t(g["esp_A"], cuda), _t(g["esp_B"], cuda)
+    CA, CB = _t(g["esp_CA"], cuda), _t(g["esp_CB"], cuda)
+    N, M = _t(g["esp_N"], cuda), _t(g["esp_M"], cuda)
+    lam = float(g["esp_lam"])
+    VAA = K._batch_self_overlap_esp(A, CA, N, 0.81, lam)
+    VBB = K._batch_self_overlap_esp(B, CB, M, 0.81, lam)
+    seeds = (_t(g["esp_seeds_q"], cuda), _t(g["esp_seeds_t"], cuda))
+    sc, q, t = al.coarse_fine_esp_align_many(A, B, CA, CB, VAA, VBB, alpha=0.81, lam=lam,
+                                             steps_fine=60, lr=0.1, N_real=N, M_real=M,
+                                             seeds=seeds)
+    sc = sc.cpu().numpy()
+    assert_parity(sc, g["esp_score"])
+    assert sc[0] > 0.99
+
+
+def test_pharm_align_matches_oracle(golden, cuda):
+    from oracle import align as oa
+    g = golden["align"]
+    args = [g[k] for k in ("pharm_A", "pharm_B", "pharm_RV", "pharm_FV", "pharm_At",
+                           "pharm_Bt", "pharm_N", "pharm_M")]
+    o_sc, _, _ = oa.align_pharm(*args, num_seeds=16, steps=150, lr=0.1)
+    A, B, RV, FV, At, Bt, N, M = [_t(a, cuda) for a in args]
+    sc, q, t = al.coarse_fine_pharm_align_many(A, B, RV, FV, At, Bt, num_seeds=16,
+                                               steps_fine=150, lr=0.1, N_real=N, M_real=M)
+    sc = sc.cpu().numpy()
+    assert sc[0] > 0.99
+    assert_parity(sc, o_sc, frac=0.6)
+    # the returned pose reproduces the score in the ORIGINAL frames (fold-back is right)
+    from oracle import scores as osc
+    R = al._quat_rot(q).cpu().numpy()
+    tt = t.cpu().numpy()
+    for i in range(len(sc)):
+        n, m = int(args[6][i]), int(args[7][i])
+        fa = args[1][i, :m] @ R[i].T + tt[i]
+        fv = args[3][i, :m] @ R[i].T
+        s = osc.pharm_tanimoto(args[4][i, :n], args[5][i, :m], args[0][i, :n], fa,
+                               args[2][i, :n], fv)
+        assert abs(s - sc[i]) < 2e-4, (i, s, sc[i])
+
+
+def test_vol_color_align_matches_reference(golden, cuda):
+    g = golden["align"]
+    CA_, CB_ = _t(g["color_A"], cuda), _t(g["color_B"], cuda)
+    CN, CM = _t(g["color_N"], cuda), _t(g["color_M"], cuda)
+    VAA = K._batch_self_overlap(CA_, CN, 0.81)
+    VBB = K._batch_self_overlap(CB_, CM, 0.81)
+    sc, q, t = al.coarse_fine_vol_color_align_many(
+        CA_, CB_, _t(g["color_At"], cuda), _t(g["color_Bt"], cuda), _t(g["pharm_A"], cuda),
+        _t(g["pharm_B"], cuda), VAA, VBB, alpha=0.81, color_weight=0.5, num_seeds=16,
+        steps_fine=60, lr=0.1, N_real_centers=CN, M_real_centers=CM,
+        N_real_pharm=_t(g["pharm_N"], cuda), M_real_pharm=_t(g["pharm_M"], cuda))
+    sc = sc.cpu().numpy()
+    assert_parity(sc, g["color_score"])
+    assert sc[0] > 0.99
+
+
+def test_directional_combo_matches_oracle(cuda):
+    from oracle import align as oa
+    refs, fits = syn.shape_pharm_pairs(6, seed=21)
+    fits[0] = dict(refs[0])
+    A, N = _pad([m["atom_pos"] for m in refs]); B, M = _pad([m["atom_pos"] for m in fits])
+    PA, PN = _pad([m["pharm_ancs"] for m in refs]); PB, PM = _pad([m["pharm_ancs"] for m in fits])
+    RV, _ = _pad([m["pharm_vecs"] for m in refs]); FV, _ = _pad([m["pharm_vecs"] for m in fits])
+    At, _ = _pad([m["pharm_types"] for m in refs], 8, np.int64)
+    Bt, _ = _pad([m["pharm_types"] for m in fits], 8, np.int64)
+    o_sc, _, _ = oa.align_combo(A, B, N, M, PA, PB, RV, FV, At, Bt, PN, PM, alpha=0.81, w=0.5,
+                                directional=True, num_seeds=20, steps=120, lr=0.1)
+    Ad, Bd, Nd, Md = _t(A, cuda), _t(B, cuda), _t(N, cuda), _t(M, cuda)
+    VAA = K._batch_self_overlap(Ad, Nd, 0.81)
+    VBB = K._batch_self_overlap(Bd, Md, 0.81)
+    sc, _, _ = al.coarse_fine_vol_pharm_align_many(
+        Ad, Bd, _t(At, cuda), _t(Bt, cuda), _t(PA, cuda), _t(PB, cuda), _t(RV, cuda),
+        _t(FV, cuda), VAA, VBB, alpha=0.81, color_weight=0.5, num_seeds=20, steps_fine=120,
+        lr=0.1, N_real_centers=Nd, M_real_centers=Md, N_real_pharm=_t(PN, cuda),
+        M_real_pharm=_t(PM, cuda))
+    sc = sc.cpu().numpy()
+    assert sc[0] > 0.99
+    assert_parity(sc, o_sc, frac=0.5)
+
+
+@pytest.mark.parametrize("lpp", [4, 8, 16, 32])
+def test_tiling_does_not_change_results(golden, cuda, lpp):
+    """Every lanes-per-pose tiling agrees (to fp32 reordering) after a few steps."""
+    g = golden["align"]
+    ref = CloudSet.from_padded(_t(g["shape_A"], cuda), _t(g["shape_N"], cuda))
+    fit = CloudSet.from_padded(_t(g["shape_B"], cuda), _t(g["shape_M"], cuda))
+    idx = torch.arange(len(g["shape_N"]), dtype=torch.int32, device=cuda)
+    kw = dict(ref=ref, fit=fit, pair_ref=idx, pair_fit=idx,
+              seed_q=_t(g["shape_seeds_q"], cuda), seed_t=_t(g["shape_seeds_t"], cuda),
+              steps=3, lr=0.1)
+    base = al.align_packed("shape", lanes_per_pose=32, **kw).rows[0].cpu().numpy()
+    got = al.align_packed("shape", lanes_per_pose=lpp, **kw).rows[0].cpu().numpy()
+    np.testing.assert_allclose(got, base, rtol=2e-5)
+
+
+def test_edge_sizes_and_degenerate_pairs(cuda):
+    """Tiny and empty clouds, tile remainders (M = 1..33), and pairs below 3 points."""
+    rng = np.random.default_rng(5)
+    sizes = [(1, 1), (2, 2), (3, 1), (0, 5), (5, 0), (4, 33), (33, 17), (17, 31), (64, 65)]
+    refs = [rng.standard_normal((n, 3)).astype(np.float32) * 2 for n, _ in sizes]
+    fits = [rng.standard_normal((m, 3)).astype(np.float32) * 2 for _, m in sizes]
+    ref = CloudSet.from_arrays(refs, device=cuda)
+    fit = CloudSet.from_arrays(fits, device=cuda)
+    idx = torch.arange(len(sizes), dtype=torch.int32, device=cuda)
+    sq, st = K.seeds(ref, fit, idx, idx, 10)
+    res = al.align_packed("shape", ref=ref, fit=fit, pair_ref=idx, pair_fit=idx, seed_q=sq,
+                          seed_t=st, steps=20, lr=0.1)
+    sc = res[0].cpu().numpy()
+    assert np.all(np.isfinite(sc))
+    assert np.all((sc >= 0) & (sc <= 1.0 + 1e-5))
+    assert sc[3] == 0 and sc[4] == 0     # an empty cloud overlaps nothing
+
+
+def test_cotenant_independence(cuda):
+    """A pair's result does not depend on which other pairs share the launch."""
+    refs, fits = syn.shape_pairs(12, seed=31)
+    ref = CloudSet.from_arrays(refs, device=cuda)
+    fit = CloudSet.from_arrays(fits, device=cuda)
+    idx = torch.arange(12, dtype=torch.int32, device=cuda)
+    sq, st = K.seeds(ref, fit, idx, idx, 20)
+    kw = dict(ref=ref, fit=fit, steps=60, lr=0.1, lanes_per_pose=8, chunks=1)
+    full = al.align_packed("shape", pair_ref=idx, pair_fit=idx, seed_q=sq, seed_t=st, **kw)
+    for sub in ([3], [0, 7, 11], [5, 6]):
+        s = torch.tensor(sub, dtype=torch.int32, device=cuda)
+        part = al.align_packed("shape", pair_ref=s, pair_fit=s, seed_q=sq[s.long()],
+                               seed_t=st[s.long()], **kw)
+        assert torch.equal(part[0], full[0][s.long()])   # same tiling -> bit-identical
+
+
+def test_graphed_and_plain_loops_agree_with_fused(golden, cuda):
+    g = golden["align"]
+    A, B = _t(g["shape_A"], cuda), _t(g["shape_B"], cuda)
+    N, M = _t(g["shape_N"], cuda), _t(g["shape_M"], cuda)
+    qs, ts = _t(g["shape_seeds_q"], cuda), _t(g["shape_seeds_t"], cuda)
+    S = qs.shape[1]
+    VAA = K._batch_self_overlap(A, N, 0.81)
+    VBB = K._batch_self_overlap(B, M, 0.81)
+    fused = al.coarse_fine_align_many(A, B, VAA, VBB, steps_fine=3, lr=0.1, N_real=N,
+                                      M_real=M, seeds=(qs, ts)).rows[0]
+    rep = lambda x: x.repeat_interleave(S, 0)
+    loop = al.GraphedFineLoop(rep(A), rep(B), rep(N), rep(M), rep(VAA + VBB), qs.reshape(-1, 4),
+                              ts.reshape(-1, 3), alpha=0.81, lr=0.1)
+    best, _, _ = loop.run(3)
+    torch.testing.assert_close(best, fused, rtol=2e-5, atol=1e-6)
+    i = 2
+    best1, _, _ = al.align_one_pair_per_launch(A[i], B[i], int(N[i]), int(M[i]),
+                                               float(VAA[i] + VBB[i]), qs[i], ts[i], steps=3,
+                                               alpha=0.81, lr=0.1)
+    torch.testing.assert_close(best1, fused[i * S:(i + 1) * S], rtol=2e-5, atol=1e-6)
