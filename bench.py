@@ -1,0 +1,490 @@
+"""Benchmark of the fused alignment path (one JSON line on rank 0).
+
+Workload (default): the ragged ESP surface batch -- 4096 pairs of surface clouds with
+200-400 points each (5 A sphere + N(0, 0.3) jitter, charges N(0, 0.1)), surf_esp scoring
+(alpha 0.81, lam 0.3 -> lam * LAM_SCALING), 50 starts x 200 Adam steps, lr 0.1.  Seeded
+synthetic data; no dataset.  A *step* is one pass of the hot path over the whole batch:
+self overlaps, seeds, the fused alignment kernel and the per-pair pick.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
+                  [--workload surf_esp|vol|vol_pharm] [--pairs P]
+
+value      aligned pairs/s with the inputs resident in HBM (device-timed, CUDA events),
+           L2 flushed between timed steps (a 256 MB write, outside the timed windows)
+e2e        the same through the host-array public API (fast_shepherd_score_b200.api.align_host)
+           with pinned host inputs: H2D of the packed clouds + compute + D2H of the results
+roofline   achieved pair-terms/s of the fused kernel against the MUFU ex2 roof measured on
+           this GPU by the probe kernel (1 ex2 per pair-term)
+cpu_baseline  the CPU oracle (C restatement of the reference's numba path, all host
+           threads) on a bounded sample of the same workload
+--impl reference  times only that CPU implementation (rank 0; other ranks exit 0)
+Multi-GPU: one process per GPU (torchrun), each rank aligns its own batch (weak scaling),
+time = max over ranks of the device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "surf_esp": dict(mode="surf_esp", pairs=4096, lo=200, hi=400, starts=50, steps=200,
+                     lr=0.1, alpha=0.81, lam=0.3,
+                     desc="ragged ESP surface batch: 4096 pairs, 200-400 pts, surf_esp, "
+                          "50 starts x 200 Adam steps"),
+    "vol": dict(mode="vol", pairs=256, lo=15, hi=50, starts=50, steps=200, lr=0.1, alpha=0.81,
+                lam=0.0, desc="plain shape alignment: 256 pairs, 15-50 atoms, vol, "
+                              "50 starts x 200 Adam steps"),
+    "vol_pharm": dict(mode="vol_pharm", pairs=16384, lo=15, hi=60, starts=50, steps=200,
+                      lr=0.1, alpha=0.81, lam=0.0,
+                      desc="combined shape+pharmacophore: 16384 pairs, 15-60 atoms + 3-20 "
+                           "features, 50 starts x 200 Adam steps"),
+}
+
+
+def make_inputs(wl, n_pairs, seed):
+    from fast_shepherd_score_b200 import synthetic as syn
+    from fast_shepherd_score_b200.api import HostBatch
+    if wl["mode"] == "surf_esp":
+        refs, fits = syn.esp_surface_pairs(n_pairs, seed=seed, lo=wl["lo"], hi=wl["hi"])
+        ref = HostBatch.from_lists([p for p, _ in refs], [c for _, c in refs])
+        fit = HostBatch.from_lists([p for p, _ in fits], [c for _, c in fits])
+        raw = (refs, fits)
+    elif wl["mode"] == "vol":
+        refs, fits = syn.shape_pairs(n_pairs, seed=seed, lo=wl["lo"], hi=wl["hi"])
+        ref, fit = HostBatch.from_lists(refs), HostBatch.from_lists(fits)
+        raw = (refs, fits)
+    else:
+        refs, fits = syn.shape_pharm_pairs(n_pairs, seed=seed, atom_lo=wl["lo"], atom_hi=wl["hi"])
+        mk = lambda ms: HostBatch.from_lists([m["atom_pos"] for m in ms], None,
+                                             [m["pharm_types"] for m in ms],
+                                             [m["pharm_ancs"] for m in ms],
+                                             [m["pharm_vecs"] for m in ms])
+        ref, fit = mk(refs), mk(fits)
+        raw = (refs, fits)
+    return ref, fit, raw
+
+
+def algorithmic_terms(wl, ref, fit):
+    """Pair-terms of one step: starts x steps x sum over pairs of N*M (real, unpadded)."""
+    per = (ref.counts.astype(np.int64) * fit.counts.astype(np.int64)).sum()
+    if wl["mode"] == "vol_pharm":
+        per += (ref.ph_counts.astype(np.int64) * fit.ph_counts.astype(np.int64)).sum()
+    return int(per) * wl["starts"] * wl["steps"]
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling in the background during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace('.', '').isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace('.', '').isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) >= 9
+                          for i, v in enumerate(r[5:9]) if v.strip().lower() == "active"})
+        load = sorted(sm)[len(sm) // 4:] if sm else []   # drop idle-ish samples at the edges
+        return {"sm_mhz": statistics.median(load) if load else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(sm)}
+
+
+def measure_peak(dev):
+    """MUFU ex2 and FP32 FMA throughput of this GPU (ops/s) from the probe kernel."""
+    import ctypes
+    import torch
+    from fast_shepherd_score_b200 import _lib
+    L = _lib.load()
+    out = torch.zeros(1 << 16, device=dev)
+    res = {}
+    for which, name in ((0, "ex2"), (1, "ffma")):
+        ops = ctypes.c_longlong(0)
+        iters = 4096 if which == 0 else 16384
+        st = _lib.stream_ptr(dev)
+        _lib.check(L.fss_probe_peak(which, 256, 8, _lib.ptr(out), ctypes.byref(ops), st))
+        torch.cuda.synchronize(dev)
+        best = 0.0
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            _lib.check(L.fss_probe_peak(which, iters, 8, _lib.ptr(out), ctypes.byref(ops), st))
+            e1.record()
+            torch.cuda.synchronize(dev)
+            best = max(best, ops.value / (e0.elapsed_time(e1) * 1e-3))
+        res[name] = best
+    return res
+
+
+def flush_l2(buf):
+    buf.add_(1.0)   # 256 MB read+write: evicts the 126 MB L2
+
+
+def run_cuda(args, wl):
+    import torch
+    import torch.distributed as dist
+    from fast_shepherd_score_b200 import _lib, api, kernels as K
+    from fast_shepherd_score_b200 import align as al
+    from fast_shepherd_score_b200.layout import cost_order
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    n_pairs = args.pairs or wl["pairs"]
+    ref_h, fit_h, raw = make_inputs(wl, n_pairs, seed=1 + rank)
+    mode = wl["mode"]
+    terms = algorithmic_terms(wl, ref_h, fit_h)
+
+    # ---- device-resident step ---------------------------------------------------------
+    rc, rp = ref_h.to_device(dev)
+    fc, fp = fit_h.to_device(dev)
+    idx = torch.arange(n_pairs, dtype=torch.int32, device=dev)
+    order = cost_order(ref_h.counts, fit_h.counts, dev)
+    esp = mode == "surf_esp"
+    kl = api._kernel_lam(mode, wl["lam"]) if esp else None
+    P, S = n_pairs, wl["starts"]
+    rows = (torch.empty(P * S, device=dev), torch.empty(P * S, 4, device=dev),
+            torch.empty(P * S, 3, device=dev))
+    outb = (torch.empty(P, device=dev), torch.empty(P, 4, device=dev), torch.empty(P, 3, device=dev))
+    align_ms = []
+
+    def step(record_kernel=False):
+        if mode == "vol_pharm":
+            rs = K.self_overlap(rc, wl["alpha"]); fs = K.self_overlap(fc, wl["alpha"])
+            rsp = K.pharm_self_overlap(rp, True); fsp = K.pharm_self_overlap(fp, True)
+        else:
+            rs = K.self_overlap(rc, wl["alpha"], esp, kl); fs = K.self_overlap(fc, wl["alpha"], esp, kl)
+            rsp = fsp = None
+        sq, st = K.seeds(rc, fc, idx, idx, S)
+        if record_kernel:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+        amode = {"surf_esp": "esp", "vol": "shape", "vol_pharm": "shape_pharm"}[mode]
+        al.align_packed(amode, ref=rc, fit=fc, ref_ph=rp, fit_ph=fp, pair_ref=idx, pair_fit=idx,
+                        seed_q=sq, seed_t=st, steps=wl["steps"], lr=wl["lr"], alpha=wl["alpha"],
+                        lam=kl, ref_self=rs, fit_self=fs, ref_self_ph=rsp, fit_self_ph=fsp,
+                        order=order, rows=rows, out=outb, check_status=False)
+        if record_kernel:
+            e1.record()
+            align_ms.append((e0, e1))
+        return outb
+
+    launches_per_step = 5 if mode != "vol_pharm" else 7
+    l2 = torch.empty(64 << 20, device=dev)   # 256 MB
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local).start()
+    times = []
+    for _ in range(args.steps):
+        flush_l2(l2)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step(record_kernel=True)
+        e1.record()
+        times.append((e0, e1))
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    total_ms = sum(a.elapsed_time(b) for a, b in times)
+    kern_ms = [a.elapsed_time(b) for a, b in align_ms]
+    t_max = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    ms_per_step = float(t_max.item()) / args.steps
+    value = n_pairs * world / (ms_per_step * 1e-3)
+    status = int(al._scratch(dev)[1].item())
+    if status:
+        raise RuntimeError(f"kernel status flags {status}")
+
+    # ---- end to end through the host-array API ----------------------------------------
+    e2e_ms = []
+    h2d = ref_h.nbytes + fit_h.nbytes + 2 * 4 * n_pairs
+    d2h = n_pairs * 8 * 4
+    for i in range(max(1, min(args.steps, 3)) + 1):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        out = api.align_host(mode, ref_h, fit_h, alpha=wl["alpha"], lam=wl["lam"],
+                             num_seeds=S, steps=wl["steps"], lr=wl["lr"], device=dev)
+        t1 = time.perf_counter()
+        if i:   # first call is a warm-up
+            e2e_ms.append((t1 - t0) * 1e3)
+    e2e_t = torch.tensor([statistics.median(e2e_ms)], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = n_pairs * world / (float(e2e_t.item()) * 1e-3)
+    assert np.all(np.isfinite(out.scores))
+
+    if rank != 0:
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return None
+
+    # ---- roofline ---------------------------------------------------------------------
+    peak = measure_peak(dev)
+    kavg = statistics.mean(kern_ms)
+    achieved = terms / (kavg * 1e-3)
+    per_term_fp32 = {"surf_esp": 9, "vol": 8, "vol_pharm": 8}[mode]
+    roof = min(peak["ex2"], peak["ffma"] / per_term_fp32)
+
+    line = {
+        "metric": "aligned pairs/s (50 starts x 200 Adam steps), batched fused kernel",
+        "value": round(value, 2), "unit": "aligned pairs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": wl["desc"], "mode": mode, "pairs_per_gpu": n_pairs,
+                   "starts": S, "adam_steps": wl["steps"], "lr": wl["lr"],
+                   "alpha": wl["alpha"], "lam": wl["lam"],
+                   "l2": "flushed between timed steps (256 MB write outside timed windows)",
+                   "parallelism": f"dp{world} (independent pair shards, no collective)"},
+        "e2e": {"value": round(e2e_value, 2), "unit": "aligned pairs/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "api": "fast_shepherd_score_b200.api.align_host (pinned host arrays)"},
+        "gpu_launches": launches_per_step * args.steps,
+        "roofline": {"bound": "mufu", "achieved": round(achieved / 1e9, 1),
+                     "peak": round(roof / 1e9, 1), "unit": "Gterm/s",
+                     "frac": round(achieved / roof, 4), "traffic": None,
+                     "peak_source": "measured by fss_probe_peak on this GPU: "
+                                    f"ex2 {peak['ex2'] / 1e9:.0f} G/s, ffma "
+                                    f"{peak['ffma'] / 1e9:.0f} G/s /{per_term_fp32} per term",
+                     "terms_per_launch": terms, "kernel_ms": round(kavg, 3)},
+        "clocks": clk,
+    }
+    if args.cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(wl, raw, budget_s=args.cpu_seconds)
+    if args.comparators and world == 1:
+        line["comparators"] = comparators(wl, raw, dev)
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return line
+
+
+def _pad(clouds, fill=0.0, dtype=np.float32):
+    n = np.array([len(c) for c in clouds])
+    out = np.full((len(clouds), max(int(n.max()), 1)) + np.asarray(clouds[0]).shape[1:], fill,
+                  dtype)
+    for i, c in enumerate(clouds):
+        out[i, :len(c)] = c
+    return out, n
+
+
+def cpu_align_sample(wl, raw, k, nthreads=None):
+    """Run the oracle on the first k pairs; returns (seconds, pairs)."""
+    from oracle import align as oa
+    refs, fits = raw
+    t0 = time.perf_counter()
+    if wl["mode"] == "surf_esp":
+        A, N = _pad([p for p, _ in refs[:k]]); B, M = _pad([p for p, _ in fits[:k]])
+        CA, _ = _pad([c for _, c in refs[:k]]); CB, _ = _pad([c for _, c in fits[:k]])
+        oa.align_esp(A, B, CA, CB, N, M, alpha=wl["alpha"], lam=oa.LAM_SCALING * wl["lam"],
+                     num_seeds=wl["starts"], steps=wl["steps"], lr=wl["lr"], nthreads=nthreads)
+    elif wl["mode"] == "vol":
+        A, N = _pad(refs[:k]); B, M = _pad(fits[:k])
+        oa.align_shape(A, B, N, M, alpha=wl["alpha"], num_seeds=wl["starts"], steps=wl["steps"],
+                       lr=wl["lr"], nthreads=nthreads)
+    else:
+        g = lambda ms, key: [m[key] for m in ms[:k]]
+        A, N = _pad(g(refs, "atom_pos")); B, M = _pad(g(fits, "atom_pos"))
+        PA, PN = _pad(g(refs, "pharm_ancs")); PB, PM = _pad(g(fits, "pharm_ancs"))
+        RV, _ = _pad(g(refs, "pharm_vecs")); FV, _ = _pad(g(fits, "pharm_vecs"))
+        At, _ = _pad(g(refs, "pharm_types"), 8, np.int64); Bt, _ = _pad(g(fits, "pharm_types"), 8, np.int64)
+        oa.align_combo(A, B, N, M, PA, PB, RV, FV, At, Bt, PN, PM, alpha=wl["alpha"], w=0.5,
+                       num_seeds=wl["starts"], steps=wl["steps"], lr=wl["lr"], nthreads=nthreads)
+    return time.perf_counter() - t0, k
+
+
+def cpu_baseline(wl, raw, budget_s=15.0):
+    """The CPU oracle on a bounded sample of the workload, all host threads."""
+    from oracle import _lib as ol
+    ol.build()
+    cores = ol.max_threads()
+    dt, k = cpu_align_sample(wl, raw, max(1, min(cores, 8)))
+    per_pair = dt / k
+    k2 = int(max(k, min(len(raw[0]), budget_s / max(per_pair, 1e-6))))
+    k2 = max(cores, (k2 // cores) * cores) if k2 >= cores else k2
+    k2 = min(k2, len(raw[0]))
+    dt, k2 = cpu_align_sample(wl, raw, k2)
+    return {"value": round(k2 / dt, 3), "unit": "aligned pairs/s", "cores": cores,
+            "kind": "port",
+            "sample": f"first {k2} pairs of the same workload ({dt:.1f} s, all {cores} host "
+                      "threads, C oracle restating the reference numba fine loop)"}
+
+
+def comparators(wl, raw, dev, n_plain=16, n_graph=256):
+    """Plain one-pair-per-launch and per-step CUDA-graph forms on subsets (pairs/s)."""
+    import torch
+    from fast_shepherd_score_b200 import align as al, kernels as K
+    from fast_shepherd_score_b200.api import _kernel_lam
+    if wl["mode"] not in ("surf_esp", "vol"):
+        return None
+    refs, fits = raw
+    esp = wl["mode"] == "surf_esp"
+    S, steps = wl["starts"], wl["steps"]
+    kl = _kernel_lam(wl["mode"], wl["lam"]) if esp else None
+    def padded(k):
+        if esp:
+            A, N = _pad([p for p, _ in refs[:k]]); B, M = _pad([p for p, _ in fits[:k]])
+            CA, _ = _pad([c for _, c in refs[:k]]); CB, _ = _pad([c for _, c in fits[:k]])
+        else:
+            A, N = _pad(refs[:k]); B, M = _pad(fits[:k]); CA = CB = None
+        t = lambda a: None if a is None else torch.as_tensor(a, device=dev)
+        return t(A), t(B), t(CA), t(CB), t(N), t(M)
+    out = {}
+    # plain: one pair at a time, two launches per Adam step
+    A, B, CA, CB, N, M = padded(n_plain)
+    VAA = (K._batch_self_overlap_esp(A, CA, N, wl["alpha"], kl) if esp
+           else K._batch_self_overlap(A, N, wl["alpha"]))
+    VBB = (K._batch_self_overlap_esp(B, CB, M, wl["alpha"], kl) if esp
+           else K._batch_self_overlap(B, M, wl["alpha"]))
+    from fast_shepherd_score_b200.layout import CloudSet
+    idx = torch.arange(n_plain, dtype=torch.int32, device=dev)
+    sq, st = K.seeds(CloudSet.from_padded(A, N, CA), CloudSet.from_padded(B, M, CB), idx, idx, S)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for i in range(n_plain):
+        n, m = int(N[i]), int(M[i])
+        al.align_one_pair_per_launch(A[i, :n], B[i, :m], n, m, float(VAA[i] + VBB[i]), sq[i],
+                                     st[i], steps=steps, alpha=wl["alpha"], lr=wl["lr"],
+                                     CA=None if CA is None else CA[i, :n],
+                                     CB=None if CB is None else CB[i, :m], lam=kl)
+    torch.cuda.synchronize(dev)
+    dt = time.perf_counter() - t0
+    out["plain_one_pair_per_launch"] = {"value": round(n_plain / dt, 3), "unit": "aligned pairs/s",
+                                        "pairs": n_plain, "launches_per_pair": 2 * steps}
+    # per-step CUDA graph over a batch (reference _graphed.py structure)
+    A, B, CA, CB, N, M = padded(n_graph)
+    idx = torch.arange(n_graph, dtype=torch.int32, device=dev)
+    sq, st = K.seeds(CloudSet.from_padded(A, N, CA), CloudSet.from_padded(B, M, CB), idx, idx, S)
+    VAA = (K._batch_self_overlap_esp(A, CA, N, wl["alpha"], kl) if esp
+           else K._batch_self_overlap(A, N, wl["alpha"]))
+    VBB = (K._batch_self_overlap_esp(B, CB, M, wl["alpha"], kl) if esp
+           else K._batch_self_overlap(B, M, wl["alpha"]))
+    rep = lambda x: None if x is None else x.repeat_interleave(S, 0)
+    loop = al.GraphedFineLoop(rep(A), rep(B), rep(N), rep(M), rep(VAA + VBB), sq.reshape(-1, 4),
+                              st.reshape(-1, 3), alpha=wl["alpha"], lr=wl["lr"], CA_k=rep(CA),
+                              CB_k=rep(CB), lam=kl).capture()
+    loop.run(2)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    loop.run(steps)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    dt = e0.elapsed_time(e1) * 1e-3
+    out["graph_per_step"] = {"value": round(n_graph / dt, 2), "unit": "aligned pairs/s",
+                             "pairs": n_graph, "launches_per_step": 2}
+    return out
+
+
+def run_reference(args, wl):
+    """The CPU implementation of the path (oracle port of the reference numba path)."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    from oracle import _lib as ol
+    ol.build()
+    cores = ol.max_threads()
+    n_pairs = args.pairs or wl["pairs"]
+    _, _, raw = make_inputs(wl, n_pairs, seed=1)
+    # calibrate a sample so that warm-up + steps stay within a few minutes
+    dt, k = cpu_align_sample(wl, raw, max(1, min(cores, 8)))
+    per_pair = dt / k
+    k = int(max(1, min(n_pairs, args.cpu_seconds / max(per_pair, 1e-6))))
+    for _ in range(args.warmup if per_pair * k * args.warmup < 60 else 0):
+        cpu_align_sample(wl, raw, max(1, min(k, cores)))
+    times = []
+    for _ in range(args.steps):
+        dt, kk = cpu_align_sample(wl, raw, k)
+        times.append(dt)
+    ms = statistics.median(times) * 1e3
+    value = k / (ms * 1e-3)
+    line = {"impl": "reference", "metric": "aligned pairs/s (50 starts x 200 Adam steps)",
+            "value": round(value, 3), "unit": "aligned pairs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)",
+            "config": {"workload": wl["desc"], "mode": wl["mode"], "sample_pairs_per_step": k},
+            "cpu_baseline": {"value": round(value, 3), "unit": "aligned pairs/s", "cores": cores,
+                             "kind": "port",
+                             "sample": f"{k} pairs of the workload per step on all {cores} "
+                                       "host threads (C oracle restating the reference numba "
+                                       "fine loop; the reference itself is Python and is not "
+                                       "present on the GPU box)"},
+            "e2e": {"value": round(value, 3), "unit": "aligned pairs/s",
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return line
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    ap.add_argument("--workload", default="surf_esp", choices=list(WORKLOADS))
+    ap.add_argument("--pairs", type=int, default=0, help="override pairs per GPU")
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-comparators", dest="comparators", action="store_false")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args(argv)
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference(args, wl)
+    return run_cuda(args, wl)
+
+
+if __name__ == "__main__":
+    main()

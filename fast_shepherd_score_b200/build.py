@@ -16,7 +16,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libfss_cuda.so")
-SOURCES = ["fss_capi.cu", "fss_align.cu", "fss_eval.cu", "fss_seeds.cu", "fss_score.cu"]
+SOURCES = ["fss_capi.cu", "fss_align.cu", "fss_eval.cu", "fss_seeds.cu", "fss_score.cu",
+           "fss_probe.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

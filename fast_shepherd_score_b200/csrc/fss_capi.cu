@@ -64,6 +64,9 @@ int score_bwd_launch(const float* ref_pts, const int32_t* ref_off, const float* 
                      const float* overlaps, const float* grad_score, float* grad_ref,
                      float* grad_fit, cudaStream_t st);
 
+int probe_launch(int which, int iters, int blocks_per_sm, float* out, long long* ops,
+                 cudaStream_t st);
+
 }  // namespace fss
 
 #define FSS_GUARD(expr)                                                   \
@@ -160,6 +163,11 @@ int fss_score_bwd(const float* ref_pts, const int32_t* ref_off, const float* fit
   FSS_GUARD(fss::score_bwd_launch(ref_pts, ref_off, fit_pts, fit_off, pair_ref, pair_fit,
                                   n_pairs, max_ref_points, max_fit_points, alpha, esp, inv_lam,
                                   overlaps, grad_score, grad_ref, grad_fit, S(stream)));
+}
+
+int fss_probe_peak(int32_t which, int32_t iters, int32_t blocks_per_sm, float* out,
+                   long long* ops, void* stream) {
+  FSS_GUARD(fss::probe_launch(which, iters, blocks_per_sm, out, ops, S(stream)));
 }
 
 }  // extern "C"

@@ -188,6 +188,16 @@ int fss_score_bwd(const float *ref_pts, const int32_t *ref_off, const float *fit
                   int32_t esp, float inv_lam, const float *overlaps, const float *grad_score,
                   float *grad_ref, float *grad_fit, void *stream);
 
+/* ---------------------------------------------------------------------------------------
+ * Roof probe (measurement support, no reference counterpart): launches a throughput kernel
+ * of `which` = 0 (ex2 on the MUFU pipe) or 1 (FP32 FMA) with `blocks_per_sm` CTAs of 256
+ * threads per SM, each thread running `iters` x 8 independent operations; *ops receives the
+ * operation count so ops / elapsed time is the device's measured rate.  `out` (grid floats)
+ * is never written in practice; it keeps the work observable to the compiler.
+ * ------------------------------------------------------------------------------------- */
+int fss_probe_peak(int32_t which, int32_t iters, int32_t blocks_per_sm, float *out,
+                   long long *ops, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
