@@ -32,23 +32,23 @@ struct AlignParams {
   int* counter;
 };
 
-constexpr int kMaxThreads = 512;
+constexpr int kMaxThreads = 320;  // 10 warps; with 2 CTAs per SM the kernel gets <= 96 registers
 
 template <int LPP, int MODE>
-__global__ void __launch_bounds__(kMaxThreads) align_kernel(const AlignParams p) {
+__global__ void __launch_bounds__(kMaxThreads, 2) align_kernel(const AlignParams p) {
   constexpr bool kShape = MODE == FSS_MODE_SHAPE || MODE == FSS_MODE_ESP ||
                           MODE == FSS_MODE_SHAPE_PHARM || MODE == FSS_MODE_SHAPE_COLOR;
   constexpr bool kEsp = MODE == FSS_MODE_ESP;
   constexpr bool kPharm = MODE == FSS_MODE_PHARM || MODE == FSS_MODE_SHAPE_PHARM ||
                           MODE == FSS_MODE_SHAPE_COLOR;
   extern __shared__ __align__(16) float4 smem[];
-  float4* sP = smem;
-  float4* sB = sP + p.maxN;
+  float4* sP = smem;                 // 2 * maxN (duplicated expanded reference)
+  float4* sB = sP + 2 * p.maxN;
   float4* sRA = sB + p.maxM;
   float4* sRV = sRA + p.maxNp;
   float4* sFA = sRV + p.maxNp;
   float4* sFV = sFA + p.maxMp;
-  float* sQc = reinterpret_cast<float*>(sFV + p.maxMp);
+  float2* sQc = reinterpret_cast<float2*>(sFV + p.maxMp);
   __shared__ float red[96];
   __shared__ int s_item;
 
@@ -187,8 +187,8 @@ __global__ void self_overlap_kernel(const float4* __restrict__ pts, const int* _
     return;
   }
   float4* sP = smem;
-  float4* sB = sP + n;
-  float* sQc = reinterpret_cast<float*>(sB + n);
+  float4* sB = sP + 2 * n;
+  float2* sQc = reinterpret_cast<float2*>(sB + n);
   const float3 c = block_centroid(pts + o0, n, red);
   stage_ref<ESP>(pts + o0, n, c, k, e, sP, sQc);
   stage_copy(pts + o0, n, sB);
@@ -376,8 +376,8 @@ int align_launch(const fss_align_desc* d, cudaStream_t st) {
   p.row_score = d->row_score; p.row_q = d->row_q; p.row_t = d->row_t;
   p.counter = d->scratch;
 
-  const size_t smem = sizeof(float4) * ((size_t)maxN + maxM + 2 * (size_t)maxNp + 2 * (size_t)maxMp) +
-                      sizeof(float) * (d->mode == FSS_MODE_ESP ? (size_t)maxN : 0) + 16;
+  const size_t smem = sizeof(float4) * (2 * (size_t)maxN + maxM + 2 * (size_t)maxNp + 2 * (size_t)maxMp) +
+                      sizeof(float2) * (d->mode == FSS_MODE_ESP ? (size_t)maxN : 0) + 16;
   int rc;
   switch (d->mode) {
     case FSS_MODE_SHAPE: rc = dispatch_lpp<FSS_MODE_SHAPE>(lpp, p, threads, d->cta_per_sm, smem, st); break;
@@ -413,7 +413,7 @@ int self_overlap_launch(const float* pts, const int32_t* off, int n_mol, int max
   const float e = (float)((double)inv_lam * 1.4426950408889634);
   const float inv2k = (float)(1.0 / (a * 1.4426950408889634));
   const float Kc = (float)(std::pow(M_PI, 1.5) / std::pow(2.0 * a, 1.5));
-  const size_t smem = sizeof(float4) * 2 * (size_t)max_n + sizeof(float) * (size_t)max_n + 16;
+  const size_t smem = sizeof(float4) * 3 * (size_t)max_n + sizeof(float2) * (size_t)max_n + 16;
   cudaError_t ce;
   if (esp) {
     ce = cudaFuncSetAttribute(self_overlap_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -213,27 +213,42 @@ __device__ __forceinline__ void step_combo(PoseState& s, const Moments& ms, floa
 // ---------------------------------------------------------------------------------------
 // Shape / ESP pairwise sum for one pose.
 //
+// Shared-memory layout of the staged reference cloud (point i):
+//   sPd[2i]   = (Px, Px, Py, Py)      sPd[2i+1] = (Pz, Pz, Pw, Pw)      sQd[i] = (Qc, Qc)
+// i.e. every component duplicated so that one 16-byte load yields the float2 operands of
+// the packed f32x2 instructions (__ffma2_rn / __fadd2_rn), which process two fit points
+// per instruction and halve the FP32 issue cost of the hot loop.
+//
 // The lanes of one pose group (LPP consecutive lanes) split the fit points j = lane + LPP*u;
-// every lane loops over all N staged reference points.  JB fit points are held in registers
-// per pass so one shared-memory load of P_i feeds JB terms.  Returns the lane's partial
-// moments in "raw" units: v = sum g, f_j = sum_i g (a_i - b'_j) (multiply by K and alpha K).
+// every lane loops over all N staged reference points.  Returns the lane's partial moments
+// in "raw" units: v = sum g, f_j = sum_i g (a_i - b'_j) (multiply by K and alpha K).
+//
+// Factored exponent: the per-fit-point part F_j.w of the exponent is constant over i, so
+//   sum_i 2^(P_i.w + P_i.b' + F_j.w) = 2^(F_j.w) * sum_i 2^(P_i.w + P_i.b')
+// and the hot loop costs 3 FMA (+1 for ESP) for the exponent instead of 4 (+1).  The
+// unscaled exponent P_i.w + P_i.b' = -k|a_i-b'|^2 + k|b'|^2 (+ESP terms) is bounded by
+// -F_j.w; when that exceeds kFactorMax for any point of the warp the chunk falls back to
+// the unfactored form so 2^x can never overflow.
 // ---------------------------------------------------------------------------------------
+constexpr float kFactorMax = 96.f;
+
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
 template <int JB, bool ESP>
-__device__ __forceinline__ void shape_chunk(const float4* __restrict__ sP,
-                                            const float* __restrict__ sQc,
-                                            const float4* __restrict__ sB, int N, int M,
-                                            int j0, int stride, const Rot& R, float tx, float ty,
-                                            float tz, float k, float e, float inv2k,
-                                            Moments& acc) {
+__device__ __forceinline__ void shape_chunk_plain(const float4* __restrict__ sPd,
+                                                  const float2* __restrict__ sQd,
+                                                  const float4* __restrict__ sB, int N, int M,
+                                                  int j0, int stride, const Rot& R, float tx,
+                                                  float ty, float tz, float k, float e,
+                                                  float inv2k, Moments& acc) {
   float bx[JB], by[JB], bz[JB], fw[JB], cj[JB];
-  float bx0[JB], by0[JB], bz0[JB];
   float sg[JB], sx[JB], sy[JB], sz[JB];
 #pragma unroll
   for (int u = 0; u < JB; ++u) {
     const int j = j0 + u * stride;
     const bool ok = j < M;
     const float4 b = ok ? sB[j] : make_float4(0.f, 0.f, 0.f, 0.f);
-    bx0[u] = b.x; by0[u] = b.y; bz0[u] = b.z; cj[u] = b.w;
+    cj[u] = b.w;
     const float3 p = rot_apply(R, b.x, b.y, b.z);
     bx[u] = p.x + tx; by[u] = p.y + ty; bz[u] = p.z + tz;
     float w = -k * (bx[u] * bx[u] + by[u] * by[u] + bz[u] * bz[u]);
@@ -241,53 +256,136 @@ __device__ __forceinline__ void shape_chunk(const float4* __restrict__ sP,
     fw[u] = ok ? w : -INFINITY;
     sg[u] = 0.f; sx[u] = 0.f; sy[u] = 0.f; sz[u] = 0.f;
   }
-#pragma unroll 2
   for (int i = 0; i < N; ++i) {
-    const float4 P = sP[i];
+    const float4 a = sPd[2 * i], c = sPd[2 * i + 1];
+    const float px = a.x, py = a.z, pz = c.x, pw = c.z;
     float qc = 0.f;
-    if (ESP) qc = sQc[i];
+    if (ESP) qc = sQd[i].x;
 #pragma unroll
     for (int u = 0; u < JB; ++u) {
-      float E = fmaf(P.x, bx[u], fmaf(P.y, by[u], fmaf(P.z, bz[u], P.w + fw[u])));
+      float E = fmaf(px, bx[u], fmaf(py, by[u], fmaf(pz, bz[u], pw + fw[u])));
       if (ESP) E = fmaf(qc, cj[u], E);
       const float g = ex2(E);
       sg[u] += g;
-      sx[u] = fmaf(g, P.x, sx[u]);
-      sy[u] = fmaf(g, P.y, sy[u]);
-      sz[u] = fmaf(g, P.z, sz[u]);
+      sx[u] = fmaf(g, px, sx[u]);
+      sy[u] = fmaf(g, py, sy[u]);
+      sz[u] = fmaf(g, pz, sz[u]);
     }
   }
 #pragma unroll
   for (int u = 0; u < JB; ++u) {
-    const float fx = fmaf(sx[u], inv2k, -bx[u] * sg[u]);
-    const float fy = fmaf(sy[u], inv2k, -by[u] * sg[u]);
-    const float fz = fmaf(sz[u], inv2k, -bz[u] * sg[u]);
-    acc.v += sg[u];
-    acc.add_force(fx, fy, fz, bx0[u], by0[u], bz0[u]);
+    const int j = j0 + u * stride;
+    if (j < M) {
+      const float4 b = sB[j];
+      acc.v += sg[u];
+      acc.add_force(fmaf(sx[u], inv2k, -bx[u] * sg[u]), fmaf(sy[u], inv2k, -by[u] * sg[u]),
+                    fmaf(sz[u], inv2k, -bz[u] * sg[u]), b.x, b.y, b.z);
+    }
   }
 }
 
+// Packed chunk: JB2 float2 pairs = 2*JB2 fit points per lane, f32x2 arithmetic, factored
+// exponent.  Returns false (and does nothing) when the factored form could overflow.
+template <int JB2, bool ESP>
+__device__ __forceinline__ bool shape_chunk_packed(const float4* __restrict__ sPd,
+                                                   const float2* __restrict__ sQd,
+                                                   const float4* __restrict__ sB, int N, int M,
+                                                   int j0, int stride, const Rot& R, float tx,
+                                                   float ty, float tz, float k, float e,
+                                                   float inv2k, Moments& acc) {
+  float2 bx[JB2], by[JB2], bz[JB2], cj[JB2];
+  float2 sg[JB2], sx[JB2], sy[JB2], sz[JB2];
+  bool big = false;
+#pragma unroll
+  for (int v = 0; v < JB2; ++v) {
+    float xs[2], ys[2], zs[2], cs[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int j = j0 + (2 * v + h) * stride;
+      const float4 b = j < M ? sB[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float3 p = rot_apply(R, b.x, b.y, b.z);
+      xs[h] = p.x + tx; ys[h] = p.y + ty; zs[h] = p.z + tz; cs[h] = b.w;
+      float w = k * (xs[h] * xs[h] + ys[h] * ys[h] + zs[h] * zs[h]);
+      if (ESP) w = fmaf(e * b.w, b.w, w);
+      big = big || (j < M && w > kFactorMax);
+    }
+    bx[v] = f2(xs[0], xs[1]); by[v] = f2(ys[0], ys[1]); bz[v] = f2(zs[0], zs[1]);
+    cj[v] = f2(cs[0], cs[1]);
+    sg[v] = f2(0.f, 0.f); sx[v] = f2(0.f, 0.f); sy[v] = f2(0.f, 0.f); sz[v] = f2(0.f, 0.f);
+  }
+  if (__any_sync(0xffffffffu, big)) return false;
+#pragma unroll 2
+  for (int i = 0; i < N; ++i) {
+    const float4 a = sPd[2 * i], c = sPd[2 * i + 1];
+    const float2 PX = f2(a.x, a.y), PY = f2(a.z, a.w), PZ = f2(c.x, c.y), PW = f2(c.z, c.w);
+    float2 QC;
+    if (ESP) QC = sQd[i];
+#pragma unroll
+    for (int v = 0; v < JB2; ++v) {
+      float2 E = __ffma2_rn(PX, bx[v], __ffma2_rn(PY, by[v], __ffma2_rn(PZ, bz[v], PW)));
+      if (ESP) E = __ffma2_rn(QC, cj[v], E);
+      const float2 g = f2(ex2(E.x), ex2(E.y));
+      sg[v] = __fadd2_rn(sg[v], g);
+      sx[v] = __ffma2_rn(g, PX, sx[v]);
+      sy[v] = __ffma2_rn(g, PY, sy[v]);
+      sz[v] = __ffma2_rn(g, PZ, sz[v]);
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < JB2; ++v) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int j = j0 + (2 * v + h) * stride;
+      if (j < M) {
+        const float4 b = sB[j];
+        const float x = h ? bx[v].y : bx[v].x, y = h ? by[v].y : by[v].x,
+                    z = h ? bz[v].y : bz[v].x;
+        float w = -k * (x * x + y * y + z * z);
+        if (ESP) w = fmaf(-e * b.w, b.w, w);
+        const float scale = ex2(w);
+        const float g = (h ? sg[v].y : sg[v].x) * scale;
+        const float gx = (h ? sx[v].y : sx[v].x) * scale;
+        const float gy = (h ? sy[v].y : sy[v].x) * scale;
+        const float gz = (h ? sz[v].y : sz[v].x) * scale;
+        acc.v += g;
+        acc.add_force(fmaf(gx, inv2k, -x * g), fmaf(gy, inv2k, -y * g),
+                      fmaf(gz, inv2k, -z * g), b.x, b.y, b.z);
+      }
+    }
+  }
+  return true;
+}
+
+template <int JB2, bool ESP>
+__device__ __forceinline__ void shape_chunk(const float4* __restrict__ sPd,
+                                            const float2* __restrict__ sQd,
+                                            const float4* __restrict__ sB, int N, int M, int j0,
+                                            int stride, const Rot& R, float tx, float ty,
+                                            float tz, float k, float e, float inv2k,
+                                            Moments& acc) {
+  if (!shape_chunk_packed<JB2, ESP>(sPd, sQd, sB, N, M, j0, stride, R, tx, ty, tz, k, e, inv2k,
+                                    acc))
+    shape_chunk_plain<2 * JB2, ESP>(sPd, sQd, sB, N, M, j0, stride, R, tx, ty, tz, k, e, inv2k,
+                                    acc);
+}
+
 template <int LPP, bool ESP>
-__device__ __forceinline__ void shape_pose(const float4* __restrict__ sP,
-                                           const float* __restrict__ sQc,
+__device__ __forceinline__ void shape_pose(const float4* __restrict__ sPd,
+                                           const float2* __restrict__ sQd,
                                            const float4* __restrict__ sB, int N, int M, int lane,
                                            const Rot& R, float tx, float ty, float tz, float k,
                                            float e, float inv2k, Moments& acc) {
-  constexpr int JB = 4;
+  constexpr int JB2 = 2;  // 4 fit points per lane per pass
   // Trip counts depend only on M and LPP, so every lane of the group (and every group of
   // the warp, which share one pair) runs the same loop; points past M are masked.
   int base = 0;
-  for (; base + JB * LPP <= M; base += JB * LPP)
-    shape_chunk<JB, ESP>(sP, sQc, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k, acc);
-  const int rem = (M - base + LPP - 1) / LPP;  // 0..JB points left for the group's lane 0
-  if (rem == 4) {
-    shape_chunk<4, ESP>(sP, sQc, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k, acc);
-  } else if (rem == 3) {
-    shape_chunk<3, ESP>(sP, sQc, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k, acc);
-  } else if (rem == 2) {
-    shape_chunk<2, ESP>(sP, sQc, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k, acc);
-  } else if (rem == 1) {
-    shape_chunk<1, ESP>(sP, sQc, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k, acc);
+  for (; base + 2 * JB2 * LPP <= M; base += 2 * JB2 * LPP)
+    shape_chunk<JB2, ESP>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k, acc);
+  const int rem = (M - base + LPP - 1) / LPP;  // 0..4 points left for the group's lane 0
+  if (rem > 2) {
+    shape_chunk<2, ESP>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k, acc);
+  } else if (rem > 0) {
+    shape_chunk<1, ESP>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k, acc);
   }
 }
 

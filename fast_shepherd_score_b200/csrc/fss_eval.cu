@@ -21,9 +21,9 @@ __global__ void __launch_bounds__(32) overlap_eval_kernel(
   const int row = blockIdx.x;
   const int N = Nr ? min(max(Nr[row], 0), Npad) : Npad;
   const int M = Mr ? min(max(Mr[row], 0), Mpad) : Mpad;
-  float4* sP = smem;
-  float4* sB = sP + Npad;
-  float* sQc = reinterpret_cast<float*>(sB + Mpad);
+  float4* sP = smem;  // 2 * Npad (duplicated expanded reference)
+  float4* sB = sP + 2 * Npad;
+  float2* sQc = reinterpret_cast<float2*>(sB + Mpad);
   const float* a = A + (size_t)row * Npad * 3;
   const float* b = B + (size_t)row * Mpad * 3;
   // centroid of the real reference points
@@ -40,9 +40,11 @@ __global__ void __launch_bounds__(32) overlap_eval_kernel(
     if (ESP) {
       const float ci = CA[(size_t)row * Npad + i];
       w = fmaf(-e * ci, ci, w);
-      sQc[i] = 2.f * e * ci;
+      sQc[i] = make_float2(2.f * e * ci, 2.f * e * ci);
     }
-    sP[i] = make_float4(2.f * k * ax, 2.f * k * ay, 2.f * k * az, w);
+    const float px = 2.f * k * ax, py = 2.f * k * ay, pz = 2.f * k * az;
+    sP[2 * i] = make_float4(px, px, py, py);
+    sP[2 * i + 1] = make_float4(pz, pz, w, w);
   }
   for (int j = threadIdx.x; j < M; j += blockDim.x)
     sB[j] = make_float4(b[3 * j], b[3 * j + 1], b[3 * j + 2],
@@ -186,7 +188,7 @@ int overlap_eval_launch(const float* A, const float* B, const float* CA, const f
   const float e = esp ? (float)((double)inv_lam * 1.4426950408889634) : 0.f;
   const float inv2k = (float)(1.0 / (a * 1.4426950408889634));
   const double Kd = std::pow(M_PI, 1.5) / std::pow(2.0 * a, 1.5);
-  const size_t smem = sizeof(float4) * ((size_t)Npad + Mpad) + sizeof(float) * (size_t)Npad + 16;
+  const size_t smem = sizeof(float4) * (2 * (size_t)Npad + Mpad) + sizeof(float2) * (size_t)Npad + 16;
   cudaError_t ce;
   if (esp) {
     ce = cudaFuncSetAttribute(overlap_eval_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -47,20 +47,23 @@ __device__ __forceinline__ float3 block_centroid(const float4* __restrict__ g, i
   return make_float3(s.x * inv, s.y * inv, s.z * inv);
 }
 
-// Stage a reference cloud (centred on c) in the expanded form P_i = (2k a, -k|a|^2 - e c^2)
-// and, for ESP, Qc_i = 2 e c_i.
+// Stage a reference cloud (centred on c) in the expanded, duplicated form
+//   sPd[2i] = (2k a.x, 2k a.x, 2k a.y, 2k a.y), sPd[2i+1] = (2k a.z, 2k a.z, P.w, P.w)
+// with P.w = -k|a|^2 - e c^2, and for ESP sQd[i] = (2 e c_i, 2 e c_i).
 template <bool ESP>
 __device__ __forceinline__ void stage_ref(const float4* __restrict__ g, int n, float3 c, float k,
-                                          float e, float4* sP, float* sQc) {
+                                          float e, float4* sPd, float2* sQd) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     const float4 p = g[i];
     const float ax = p.x - c.x, ay = p.y - c.y, az = p.z - c.z;
     float w = -k * (ax * ax + ay * ay + az * az);
     if (ESP) {
       w = fmaf(-e * p.w, p.w, w);
-      sQc[i] = 2.f * e * p.w;
+      sQd[i] = make_float2(2.f * e * p.w, 2.f * e * p.w);
     }
-    sP[i] = make_float4(2.f * k * ax, 2.f * k * ay, 2.f * k * az, w);
+    const float px = 2.f * k * ax, py = 2.f * k * ay, pz = 2.f * k * az;
+    sPd[2 * i] = make_float4(px, px, py, py);
+    sPd[2 * i + 1] = make_float4(pz, pz, w, w);
   }
 }
 

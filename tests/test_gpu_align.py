@@ -69,7 +69,7 @@ def test_shape_rows_track_oracle_stepwise(golden, cuda):
         rows = res.rows[0].cpu().numpy()
         _, _, _, (best, _, _) = oa.align_shape(A, B, N, M, alpha=0.81, steps=steps, lr=0.1,
                                                seeds=(qs, ts), return_rows=True)
-        tol = dict(rtol=2e-5, atol=1e-6) if steps == 1 else dict(rtol=0, atol=1e-4)
+        tol = dict(rtol=2e-5, atol=1e-6) if steps == 1 else dict(rtol=0, atol=5e-5)
         np.testing.assert_allclose(rows, best, **tol)
         assert rows.shape == (len(N) * S,)
 
@@ -158,7 +158,8 @@ def test_directional_combo_matches_oracle(cuda):
 
 @pytest.mark.parametrize("lpp", [4, 8, 16, 32])
 def test_tiling_does_not_change_results(golden, cuda, lpp):
-    """Every lanes-per-pose tiling agrees (to fp32 reordering) after a few steps."""
+    """Every lanes-per-pose tiling agrees after a few steps (to fp32 reordering, which
+    Adam's normalised step amplifies to a few 1e-5)."""
     g = golden["align"]
     ref = CloudSet.from_padded(_t(g["shape_A"], cuda), _t(g["shape_N"], cuda))
     fit = CloudSet.from_padded(_t(g["shape_B"], cuda), _t(g["shape_M"], cuda))
@@ -168,7 +169,7 @@ def test_tiling_does_not_change_results(golden, cuda, lpp):
               steps=3, lr=0.1)
     base = al.align_packed("shape", lanes_per_pose=32, **kw).rows[0].cpu().numpy()
     got = al.align_packed("shape", lanes_per_pose=lpp, **kw).rows[0].cpu().numpy()
-    np.testing.assert_allclose(got, base, rtol=2e-5)
+    np.testing.assert_allclose(got, base, rtol=0, atol=5e-5)
 
 
 def test_edge_sizes_and_degenerate_pairs(cuda):
@@ -219,9 +220,9 @@ def test_graphed_and_plain_loops_agree_with_fused(golden, cuda):
     loop = al.GraphedFineLoop(rep(A), rep(B), rep(N), rep(M), rep(VAA + VBB), qs.reshape(-1, 4),
                               ts.reshape(-1, 3), alpha=0.81, lr=0.1)
     best, _, _ = loop.run(3)
-    torch.testing.assert_close(best, fused, rtol=2e-5, atol=1e-6)
+    torch.testing.assert_close(best, fused, rtol=0, atol=5e-5)
     i = 2
     best1, _, _ = al.align_one_pair_per_launch(A[i], B[i], int(N[i]), int(M[i]),
                                                float(VAA[i] + VBB[i]), qs[i], ts[i], steps=3,
                                                alpha=0.81, lr=0.1)
-    torch.testing.assert_close(best1, fused[i * S:(i + 1) * S], rtol=2e-5, atol=1e-6)
+    torch.testing.assert_close(best1, fused[i * S:(i + 1) * S], rtol=0, atol=5e-5)

@@ -175,4 +175,4 @@ def test_tanimoto_adam_step_matches_reference_tail(cuda):
         np.testing.assert_allclose(qd.cpu().numpy(), st[0], atol=2e-5)
         np.testing.assert_allclose(td.cpu().numpy(), st[1], atol=2e-5)
         np.testing.assert_allclose(bs.cpu().numpy(), st[6], rtol=1e-6)
-        np.testing.assert_allclose(bqd.cpu().numpy(), st[7], atol=1e-7)
+        np.testing.assert_allclose(bqd.cpu().numpy(), st[7], atol=2e-5)
