@@ -287,7 +287,8 @@ def run_cuda(args, wl):
                    "starts": S, "adam_steps": wl["steps"], "lr": wl["lr"],
                    "alpha": wl["alpha"], "lam": wl["lam"],
                    "l2": "flushed between timed steps (256 MB write outside timed windows)",
-                   "parallelism": f"dp{world} (independent pair shards, no collective)"},
+                   "parallelism": f"dp{world} (independent pair shards, no collective)",
+                   "tile": dict(al.LAST_TILE)},
         "e2e": {"value": round(e2e_value, 2), "unit": "aligned pairs/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "api": "fast_shepherd_score_b200.api.align_host (pinned host arrays)"},

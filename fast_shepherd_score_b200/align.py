@@ -30,7 +30,7 @@ from typing import Optional
 import numpy as np
 import torch
 
-from . import _lib, kernels
+from . import _lib, autotune, kernels
 from ._lib import AlignDesc, check, ptr, stream_ptr
 from .layout import CloudSet, PharmSet, cost_order
 
@@ -41,6 +41,7 @@ MODE_IDS = {"shape": _lib.MODE_SHAPE, "esp": _lib.MODE_ESP, "pharm": _lib.MODE_P
             "shape_pharm": _lib.MODE_SHAPE_PHARM, "shape_color": _lib.MODE_SHAPE_COLOR}
 
 _SCRATCH: dict = {}
+LAST_TILE: dict = {}   # tiling of the most recent fused launch (for reports)
 
 
 def _scratch(device) -> torch.Tensor:
@@ -122,6 +123,13 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
             order = cost_order(ref.counts[pr], fit.counts[pf], dev)
         else:
             order = cost_order(ref_ph.counts[pr], fit_ph.counts[pf], dev)
+    if (lanes_per_pose == 0 and chunks == 0 and cta_per_sm == 0 and autotune.enabled()
+            and P >= 64 and steps > 0):
+        tile = _tuned_tile(mode, shape, ref, fit, ref_ph, fit_ph, pair_ref, pair_fit, seed_q,
+                           seed_t, steps, lr, alpha, lam, color_weight, ref_self, fit_self,
+                           ref_self_ph, fit_self_ph)
+        lanes_per_pose, chunks, cta_per_sm = (tile["lanes_per_pose"], tile["chunks"],
+                                              tile["cta_per_sm"])
     if rows is None:
         rows = (torch.empty(P * S, dtype=_f32, device=dev),
                 torch.empty(P * S, 4, dtype=_f32, device=dev),
@@ -130,6 +138,9 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
         out = (torch.empty(P, dtype=_f32, device=dev), torch.empty(P, 4, dtype=_f32, device=dev),
                torch.empty(P, 3, dtype=_f32, device=dev))
     scratch = _scratch(dev) if scratch is None else scratch
+    LAST_TILE.clear()
+    LAST_TILE.update(lanes_per_pose=int(lanes_per_pose), chunks=int(chunks),
+                     cta_per_sm=int(cta_per_sm), autotuned=autotune.enabled() and P >= 64)
     d = AlignDesc()
     d.mode, d.n_pairs, d.n_starts, d.steps = m, P, S, int(steps)
     d.pair_ref, d.pair_fit = ptr(pair_ref, _i32), ptr(pair_fit, _i32)
@@ -164,6 +175,37 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
     res = AlignResult(out)
     res.rows = rows
     return res
+
+
+def _tuned_tile(mode, shape, ref, fit, ref_ph, fit_ph, pair_ref, pair_fit, seed_q, seed_t,
+                steps, lr, alpha, lam, color_weight, ref_self, fit_self, ref_self_ph,
+                fit_self_ph):
+    """The autotuned tile for this launch's shape bucket (tuned on first sight)."""
+    cs_r, cs_f = (ref, fit) if shape else (ref_ph, fit_ph)
+    S = int(seed_q.shape[1])
+    P = int(seed_q.shape[0])
+    key = autotune.shape_key(seed_q.device, mode, cs_r.max_points, cs_f.max_points,
+                             float(np.mean(cs_f.counts)) if len(cs_f.counts) else 0.0, S, P)
+    rec = autotune.lookup(key)
+    if rec is not None:
+        return rec
+    pr = pair_ref.cpu().numpy()
+    pf = pair_fit.cpu().numpy()
+    cost = cs_r.counts[pr].astype(np.int64) * cs_f.counts[pf].astype(np.int64)
+    # enough pairs for several waves of CTAs, so the sample is throughput- not latency-bound
+    k = min(P, 8 * torch.cuda.get_device_properties(seed_q.device).multi_processor_count)
+    sel = torch.from_numpy(autotune.sample_pairs(cost, k)).to(seed_q.device)
+    sub = dict(ref=ref, fit=fit, ref_ph=ref_ph, fit_ph=fit_ph, pair_ref=pair_ref[sel],
+               pair_fit=pair_fit[sel], seed_q=seed_q[sel], seed_t=seed_t[sel],
+               steps=min(int(steps), 10), lr=lr, alpha=alpha, lam=lam,
+               color_weight=color_weight, ref_self=ref_self, fit_self=fit_self,
+               ref_self_ph=ref_self_ph, fit_self_ph=fit_self_ph, check_status=False,
+               scratch=torch.zeros(2, dtype=_i32, device=seed_q.device))
+
+    def run(**tile):
+        align_packed(mode, **sub, **tile)
+
+    return autotune.tune(run, key, autotune.candidates(mode, cs_f.max_points, S))
 
 
 # ------------------------------------------------------------------------------------------

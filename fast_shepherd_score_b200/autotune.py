@@ -1,0 +1,138 @@
+"""Autotuner for the fused alignment kernel's tiling.
+
+Tunables of one launch (``fss_align_desc``):
+  lanes_per_pose  4, 8, 16 or 32 lanes cooperate on one pose (so 32/lanes starts per warp)
+  chunks          start blocks per pair (a CTA owns one pair and n_starts/chunks starts)
+  cta_per_sm      persistent CTAs per SM (1 or 2; 2 hides latency, 1 leaves more L1)
+
+For a new problem shape the tuner times each candidate on a sample of the batch's pairs
+(the costliest and a spread of the rest) for a few Adam steps, with CUDA events, and keeps
+the fastest.  Results are cached per (device, mode, size buckets, starts) in memory and in a
+JSON file (``$FSS_AUTOTUNE_CACHE`` or ``~/.cache/fast_shepherd_score_b200/autotune.json``).
+Set ``FSS_AUTOTUNE=0`` to disable tuning (the library's built-in default is then used).
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import threading
+from typing import Optional
+
+import numpy as np
+import torch
+
+_LOCK = threading.Lock()
+_MEM: dict = {}
+_LOADED = False
+LANES = (4, 8, 16, 32)
+
+
+def _cache_path() -> str:
+    p = os.environ.get("FSS_AUTOTUNE_CACHE")
+    if p:
+        return p
+    return os.path.join(os.path.expanduser("~"), ".cache", "fast_shepherd_score_b200",
+                        "autotune.json")
+
+
+def _load():
+    global _LOADED
+    if _LOADED:
+        return
+    _LOADED = True
+    try:
+        with open(_cache_path()) as f:
+            _MEM.update(json.load(f))
+    except Exception:
+        pass
+
+
+def _save():
+    try:
+        path = _cache_path()
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        tmp = path + f".{os.getpid()}.tmp"
+        with open(tmp, "w") as f:
+            json.dump(_MEM, f, indent=1, sort_keys=True)
+        os.replace(tmp, path)
+    except Exception:
+        pass
+
+
+def enabled() -> bool:
+    return os.environ.get("FSS_AUTOTUNE", "1") != "0"
+
+
+def _bucket(x: int) -> int:
+    return 0 if x <= 0 else 1 << int(math.ceil(math.log2(max(int(x), 1))))
+
+
+def shape_key(device, mode: str, max_ref: int, max_fit: int, mean_fit: float, n_starts: int,
+              n_pairs: int) -> str:
+    name = torch.cuda.get_device_name(device).replace(" ", "_")
+    return (f"{name}|{mode}|r{_bucket(max_ref)}|f{_bucket(max_fit)}|m{_bucket(int(mean_fit))}"
+            f"|s{n_starts}|p{_bucket(n_pairs)}")
+
+
+def candidates(mode: str, max_fit: int, n_starts: int):
+    out = []
+    for lpp in LANES:
+        if mode != "pharm" and lpp > 4 and lpp // 2 >= max(max_fit, 1):
+            continue  # more lanes than fit points: idle lanes
+        if mode == "pharm" and lpp > 8:
+            continue
+        for cps in (0, 2, 1):   # 0 = as many CTAs per SM as fit
+            out.append({"lanes_per_pose": lpp, "chunks": 0, "cta_per_sm": cps})
+    return out
+
+
+def lookup(key: str) -> Optional[dict]:
+    with _LOCK:
+        _load()
+        return _MEM.get(key)
+
+
+def tune(run, key: str, cands, repeats: int = 2) -> dict:
+    """Time ``run(**tile)`` for each candidate tile; cache and return the fastest."""
+    best, best_ms = None, float("inf")
+    timings = {}
+    for c in cands:
+        try:
+            run(**c)  # warm (shared-memory attribute, first-launch costs)
+            ms = []
+            for _ in range(repeats):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                run(**c)
+                e1.record()
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            t = min(ms)
+        except (ValueError, RuntimeError):
+            continue
+        timings[f"{c['lanes_per_pose']}x{c['cta_per_sm']}"] = round(t, 4)
+        if t < best_ms:
+            best, best_ms = c, t
+    if best is None:
+        best = {"lanes_per_pose": 0, "chunks": 0, "cta_per_sm": 0}
+    rec = dict(best)
+    rec["ms"] = round(best_ms, 4) if best_ms < float("inf") else None
+    rec["timings"] = timings
+    with _LOCK:
+        _load()
+        _MEM[key] = rec
+        _save()
+    return rec
+
+
+def sample_pairs(cost: np.ndarray, k: int) -> np.ndarray:
+    """Indices of a representative sample: the costliest pairs and an even spread."""
+    order = np.argsort(-cost, kind="stable")
+    if len(order) <= k:
+        return order
+    head = order[: k // 4]
+    rest = order[k // 4:]
+    spread = rest[np.linspace(0, len(rest) - 1, k - len(head)).astype(np.int64)]
+    return np.concatenate([head, spread])

@@ -117,24 +117,28 @@ __global__ void __launch_bounds__(kMaxThreads, 2) align_kernel(const AlignParams
       }
       for (int step = 0; step < p.steps; ++step) {
         const Rot R = quat_to_rot(s.q);
-        Moments ms;
-        ms.zero();
+        Reduced rs;
         if (kShape) {
+          Moments ms;
+          ms.zero();
           shape_pose<LPP, kEsp>(sP, sQc, sB, N, M, lane, R, s.t[0], s.t[1], s.t[2], p.k, p.e,
                                 p.inv2k, ms);
-          ms.template group_sum<LPP>();
-          ms.scale(p.Kc, p.aKc);
+          rs.from(ms, s.q);
+          rs.template group_sum<LPP>();
+          rs.scale(p.Kc, p.aKc);
         }
         if (kPharm) {
           Moments mc;
           mc.zero();
           pharm_pose<LPP>(sRA, sRV, sFA, sFV, Np, Mp, lane, R, s.t[0], s.t[1], s.t[2], p.tab,
                           mc);
-          mc.template group_sum<LPP>();
-          if (kShape) step_combo(s, ms, Us, mc, Uc, p.w, p.lr);
-          else step_single(s, mc, Us, p.lr);
+          Reduced rc;
+          rc.from(mc, s.q);
+          rc.template group_sum<LPP>();
+          if (kShape) step_combo(s, rs, Us, rc, Uc, p.w, p.lr);
+          else step_single(s, rc, Us, p.lr);
         } else {
-          step_single(s, ms, Us, p.lr);
+          step_single(s, rs, Us, p.lr);
         }
       }
       if (active && lane == 0) {
@@ -279,13 +283,15 @@ int dispatch_lpp(int lpp, const AlignParams& prm, int threads, int cps, size_t s
   }
 }
 
-// Default tiling: lanes per pose from the fit size (about 4 fit points per lane for the
-// register tile), start blocks chosen to waste the fewest pose slots.
+// Default tiling (the Python autotuner overrides it with measured choices): lanes per pose
+// so that each lane owns about 8 fit points -- enough pairwise work per lane to amortise
+// the per-step group reduction and Adam tail -- and start blocks that waste the fewest pose
+// slots.  Pharmacophore-only poses are tiny, so they get the narrowest groups.
 void auto_tile(int mode, int max_fit, int n_starts, int* lpp, int* chunks) {
   int l = *lpp;
   if (l <= 0) {
-    const int m = mode == FSS_MODE_PHARM ? max_fit * 2 : max_fit;
-    l = m <= 16 ? 4 : (m <= 32 ? 8 : (m <= 64 ? 16 : 32));
+    const int m = mode == FSS_MODE_PHARM ? 0 : max_fit;
+    l = m < 64 ? 4 : (m < 128 ? 8 : (m < 256 ? 16 : 32));
   }
   *lpp = l;
   if (*chunks > 0) return;

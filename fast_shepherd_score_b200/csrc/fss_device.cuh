@@ -122,6 +122,37 @@ __device__ __forceinline__ void quat_grad_from_moment(const float q[4], const fl
   dq[3] = 2.f * (qi * (xz + zx) + qj * (yz + zy) + qr * (yx - xy) - 2.f * qk * (xx + yy));
 }
 
+// What a pose group reduces per step: value, dV/dt and dV/dq.  dV/dq is linear in the
+// moment G, so every lane turns its partial G into a partial dq first and the butterfly
+// moves 8 floats instead of 13.
+struct Reduced {
+  float v, f[3], dq[4];
+  __device__ __forceinline__ void from(const Moments& m, const float q[4]) {
+    v = m.v;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) f[i] = m.f[i];
+    quat_grad_from_moment(q, m.g, dq);
+  }
+  template <int WIDTH>
+  __device__ __forceinline__ void group_sum() {
+#pragma unroll
+    for (int o = WIDTH / 2; o > 0; o >>= 1) {
+      v += __shfl_xor_sync(0xffffffffu, v, o);
+#pragma unroll
+      for (int i = 0; i < 3; ++i) f[i] += __shfl_xor_sync(0xffffffffu, f[i], o);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) dq[i] += __shfl_xor_sync(0xffffffffu, dq[i], o);
+    }
+  }
+  __device__ __forceinline__ void scale(float sv, float sf) {
+    v *= sv;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) f[i] *= sf;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) dq[i] *= sf;
+  }
+};
+
 // Loop-carried optimiser state of one pose.
 struct PoseState {
   float q[4], t[3];
@@ -177,34 +208,29 @@ __device__ __forceinline__ void tanimoto(float V, float U, float& score, float& 
   scale = U / (denom * denom);
 }
 
-// Single-channel step: score, best tracking and Adam from the channel's moments.
-__device__ __forceinline__ void step_single(PoseState& s, const Moments& m, float U, float lr) {
+// Single-channel step: score, best tracking and Adam from the channel's reduced sums.
+__device__ __forceinline__ void step_single(PoseState& s, const Reduced& m, float U, float lr) {
   float score, scale;
   tanimoto(m.v, U, score, scale);
-  float dq[4];
-  quat_grad_from_moment(s.q, m.g, dq);
   float gq[4], gt[3];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) gq[i] = -scale * dq[i];
+  for (int i = 0; i < 4; ++i) gq[i] = -scale * m.dq[i];
 #pragma unroll
   for (int i = 0; i < 3; ++i) gt[i] = -scale * m.f[i];
   adam_tail(s, score, gq, gt, lr);
 }
 
 // Two-channel step (1-w) * shape + w * pharm, the joint gradient of cpu_fused.py:111-167.
-__device__ __forceinline__ void step_combo(PoseState& s, const Moments& ms, float Us,
-                                           const Moments& mc, float Uc, float w, float lr) {
+__device__ __forceinline__ void step_combo(PoseState& s, const Reduced& ms, float Us,
+                                           const Reduced& mc, float Uc, float w, float lr) {
   float ss, scs, sc, scc;
   tanimoto(ms.v, Us, ss, scs);
   tanimoto(mc.v, Uc, sc, scc);
   const float score = (1.f - w) * ss + w * sc;
   const float cs = -(1.f - w) * scs, cc = -w * scc;
-  float dqs[4], dqc[4];
-  quat_grad_from_moment(s.q, ms.g, dqs);
-  quat_grad_from_moment(s.q, mc.g, dqc);
   float gq[4], gt[3];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) gq[i] = cs * dqs[i] + cc * dqc[i];
+  for (int i = 0; i < 4; ++i) gq[i] = cs * ms.dq[i] + cc * mc.dq[i];
 #pragma unroll
   for (int i = 0; i < 3; ++i) gt[i] = cs * ms.f[i] + cc * mc.f[i];
   adam_tail(s, score, gq, gt, lr);
