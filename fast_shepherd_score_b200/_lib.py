@@ -55,6 +55,7 @@ _SIGS = {
     "fss_pharm_self_overlap": ([_vp, _vp, _vp, _i32, _i32, _i32, _vp, _vp], ctypes.c_int),
     "fss_seeds": ([_vp] * 6 + [_i32, _i32, _vp, _i32, _vp, _vp, _vp], ctypes.c_int),
     "fss_align": ([ctypes.POINTER(AlignDesc), _vp], ctypes.c_int),
+    "fss_align_static": ([ctypes.POINTER(AlignDesc), _vp], ctypes.c_int),
     "fss_pick_best": ([_vp] * 3 + [_i32, _i32] + [_vp] * 4, ctypes.c_int),
     "fss_score_fwd": ([_vp] * 6 + [_i32, _i32, _i32, _f32, _i32, _f32, _vp, _vp, _vp],
                       ctypes.c_int),

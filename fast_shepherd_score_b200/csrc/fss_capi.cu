@@ -66,6 +66,7 @@ int score_bwd_launch(const float* ref_pts, const int32_t* ref_off, const float* 
 
 int probe_launch(int which, int iters, int blocks_per_sm, float* out, long long* ops,
                  cudaStream_t st);
+int align_static_launch(const fss_align_desc* d, cudaStream_t st);
 
 }  // namespace fss
 
@@ -137,6 +138,10 @@ int fss_seeds(const float* ref_pts, const int32_t* ref_off, const float* fit_pts
 
 int fss_align(const fss_align_desc* desc, void* stream) {
   FSS_GUARD(fss::align_launch(desc, S(stream)));
+}
+
+int fss_align_static(const fss_align_desc* desc, void* stream) {
+  FSS_GUARD(fss::align_static_launch(desc, S(stream)));
 }
 
 int fss_pick_best(const float* row_score, const float* row_q, const float* row_t,

@@ -162,6 +162,21 @@ typedef struct fss_align_desc {
  * (accel/drivers/vol_color.py:199-518) with early stop disabled (fixed step count). */
 int fss_align(const fss_align_desc *desc, void *stream);
 
+/* Allocation-free variant of fss_align.  It has no counterpart in the reference: it is for
+ * callers that cannot allocate device memory where they align (a host runtime that only
+ * hands over input and output buffers, code inside another framework's memory pool, or a
+ * latency-critical loop that must not call cudaMalloc).  The descriptor is read as for
+ * fss_align except that row_score/row_q/row_t and scratch are ignored (may be NULL): the
+ * per-(pair, start) rows and the work counter live in one library-owned __device__ array
+ * of FSS_STATIC_MAX_ROWS rows (about 4 MiB per device, held until the process exits), so
+ * n_pairs * n_starts above FSS_STATIC_MAX_ROWS is rejected with FSS_ERR_UNSUPPORTED.
+ * out_score/out_q/out_t are required.  The first call on a device resolves the array's
+ * address (cudaGetSymbolAddress) with that device current; make that first call before
+ * any stream capture.  All calls share the array, so calls that overlap on the GPU race;
+ * a pair larger than the declared max_* extents returns a NaN score. */
+#define FSS_STATIC_MAX_ROWS 131072
+int fss_align_static(const fss_align_desc *desc, void *stream);
+
 /* Per-pair argmax over starts of row results (shape.py:306-313). */
 int fss_pick_best(const float *row_score, const float *row_q, const float *row_t,
                   int32_t n_pairs, int32_t n_starts, float *out_score, float *out_q,
