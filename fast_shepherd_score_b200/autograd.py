@@ -1,0 +1,136 @@
+"""Differentiable Tanimoto scores with a hand-written CUDA adjoint.
+
+The reference computes d(score)/d(coordinates, charges) with torch autograd through
+``cdist``/``exp`` (score/gaussian_overlap.py:62-117 ``get_overlap``,
+score/electrostatic_scoring.py:55-120 ``get_overlap_esp``), materialising N x M distance
+matrices.  Here the forward pass (``fss_score_fwd``) and its adjoint (``fss_score_bwd``) are
+single kernels over packed clouds; :class:`PackedTanimoto` wraps them as a
+``torch.autograd.Function`` whose inputs are the packed float4 point tensors (x, y, z,
+charge), so gradients reach the caller's coordinate and charge tensors through the ordinary
+torch ops that pack them.
+
+* :func:`tanimoto_packed` -- P pairs of molecules in two packed sets (the general form; a
+  fixed target shared by many queries is one molecule of the ref set).
+* :func:`get_overlap`, :func:`get_overlap_esp` -- the reference's signatures for one pair
+  ((N,3) vs (M,3)) or a matched batch ((B,N,3) vs (B,M,3)).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, ptr, stream_ptr
+
+LAM_SCALING = (1e4 / (4 * 55.263 * math.pi)) ** 2
+_f32, _i32 = torch.float32, torch.int32
+
+
+class PackedTanimoto(torch.autograd.Function):
+    """score_p = V_AB / (V_AA + V_BB - V_AB) for P pairs of packed clouds."""
+
+    @staticmethod
+    def forward(ctx, ref_pts, fit_pts, ref_off, fit_off, pair_ref, pair_fit, max_ref, max_fit,
+                alpha, esp, inv_lam):
+        dev = ref_pts.device
+        P = int(pair_ref.shape[0])
+        ref_pts, fit_pts = ref_pts.contiguous(), fit_pts.contiguous()
+        score = torch.empty(P, dtype=_f32, device=dev)
+        ov = torch.empty(P, 3, dtype=_f32, device=dev)
+        check(_lib.load().fss_score_fwd(ptr(ref_pts, _f32), ptr(ref_off, _i32), ptr(fit_pts, _f32),
+                                        ptr(fit_off, _i32), ptr(pair_ref, _i32),
+                                        ptr(pair_fit, _i32), P, int(max_ref), int(max_fit),
+                                        float(alpha), int(esp), float(inv_lam), ptr(score),
+                                        ptr(ov), stream_ptr(dev)), "score_fwd")
+        ctx.save_for_backward(ref_pts, fit_pts, ref_off, fit_off, pair_ref, pair_fit, ov)
+        ctx.cfg = (int(max_ref), int(max_fit), float(alpha), int(esp), float(inv_lam))
+        ctx.mark_non_differentiable(ov)
+        return score, ov
+
+    @staticmethod
+    def backward(ctx, g_score, g_ov):
+        ref_pts, fit_pts, ref_off, fit_off, pair_ref, pair_fit, ov = ctx.saved_tensors
+        max_ref, max_fit, alpha, esp, inv_lam = ctx.cfg
+        gr = torch.zeros_like(ref_pts)
+        gf = torch.zeros_like(fit_pts)
+        g = g_score.to(_f32).contiguous()
+        check(_lib.load().fss_score_bwd(ptr(ref_pts, _f32), ptr(ref_off, _i32), ptr(fit_pts, _f32),
+                                        ptr(fit_off, _i32), ptr(pair_ref, _i32),
+                                        ptr(pair_fit, _i32), int(pair_ref.shape[0]), max_ref,
+                                        max_fit, alpha, esp, inv_lam, ptr(ov), ptr(g), ptr(gr),
+                                        ptr(gf), stream_ptr(ref_pts.device)), "score_bwd")
+        return gr, gf, None, None, None, None, None, None, None, None, None
+
+
+def tanimoto_packed(ref_pts, ref_off, fit_pts, fit_off, pair_ref, pair_fit, *, alpha=0.81,
+                    lam=None, max_ref=None, max_fit=None, return_overlaps=False):
+    """Differentiable Tanimoto for pairs of packed clouds.
+
+    ``ref_pts``/``fit_pts`` (n, 4) float32 CUDA tensors (x, y, z, charge), ``*_off`` int32
+    prefix offsets, ``pair_*`` int32 molecule indices.  ``lam`` (kernel lambda) switches the
+    ESP weighting on.  Gradients flow to ``ref_pts`` and ``fit_pts`` (w = d/d charge).
+    """
+    if max_ref is None:
+        max_ref = int((ref_off[1:] - ref_off[:-1]).max()) if ref_off.numel() > 1 else 0
+    if max_fit is None:
+        max_fit = int((fit_off[1:] - fit_off[:-1]).max()) if fit_off.numel() > 1 else 0
+    esp = lam is not None
+    score, ov = PackedTanimoto.apply(ref_pts, fit_pts, ref_off.to(_i32).contiguous(),
+                                     fit_off.to(_i32).contiguous(),
+                                     pair_ref.to(_i32).contiguous(), pair_fit.to(_i32).contiguous(),
+                                     max_ref, max_fit, alpha, esp,
+                                     1.0 / float(lam) if esp else 0.0)
+    return (score, ov) if return_overlaps else score
+
+
+def _pack(x, c=None):
+    """(B, N, 3) [+ (B, N)] -> differentiable (B*N, 4) float4 rows and offsets."""
+    B, N, _ = x.shape
+    w = c.reshape(B, N, 1) if c is not None else torch.zeros(B, N, 1, dtype=x.dtype, device=x.device)
+    pts = torch.cat([x, w.to(x.dtype)], -1).reshape(B * N, 4).to(_f32)
+    off = torch.arange(0, (B + 1) * N, N, dtype=_i32, device=x.device)
+    return pts, off
+
+
+def _batched(c1, c2, q1=None, q2=None):
+    single = c1.dim() == 2 and c2.dim() == 2
+    if c1.dim() == 2:
+        c1 = c1.unsqueeze(0)
+        q1 = None if q1 is None else q1.reshape(1, -1)
+    if c2.dim() == 2:
+        c2 = c2.unsqueeze(0)
+        q2 = None if q2 is None else q2.reshape(1, -1)
+    B = max(c1.shape[0], c2.shape[0])
+    return c1, c2, q1, q2, B, single
+
+
+def _score(c1, c2, q1, q2, alpha, lam):
+    c1, c2, q1, q2, B, single = _batched(c1, c2, q1, q2)
+    if not (c1.is_cuda and c2.is_cuda):
+        raise ValueError("fast_shepherd_score_b200 scores CUDA tensors only")
+    r, roff = _pack(c1, q1)
+    f, foff = _pack(c2, q2)
+    idx = torch.arange(B, dtype=_i32, device=c1.device)
+    pr = idx if c1.shape[0] == B else torch.zeros(B, dtype=_i32, device=c1.device)
+    pf = idx if c2.shape[0] == B else torch.zeros(B, dtype=_i32, device=c1.device)
+    s = tanimoto_packed(r, roff, f, foff, pr, pf, alpha=alpha, lam=lam,
+                        max_ref=c1.shape[1], max_fit=c2.shape[1])
+    s = s.to(c1.dtype) if c1.dtype != _f32 else s
+    return s[0] if single else s
+
+
+def get_overlap(centers_1, centers_2, alpha: float = 0.81):
+    """Shape Tanimoto (gaussian_overlap.py:73), differentiable in both clouds.
+
+    (N,3) vs (M,3) -> scalar; (B,N,3) vs (B,M,3), or a single cloud against a batch -> (B,).
+    """
+    return _score(centers_1, centers_2, None, None, alpha, None)
+
+
+def get_overlap_esp(centers_1, centers_2, charges_1, charges_2, alpha: float = 0.81,
+                    lam: float = 0.3 * LAM_SCALING):
+    """ESP-weighted Tanimoto (electrostatic_scoring.py:69), differentiable in coordinates and
+    charges; ``lam`` as the reference's (surface default 0.3 * LAM_SCALING)."""
+    return _score(centers_1, centers_2, charges_1, charges_2, alpha, lam)
