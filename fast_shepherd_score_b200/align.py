@@ -65,13 +65,17 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
                  alpha: float = 0.81, lam: Optional[float] = None, color_weight: float = 0.5,
                  ref_self=None, fit_self=None, ref_self_ph=None, fit_self_ph=None,
                  order=None, lanes_per_pose: int = 0, chunks: int = 0, cta_per_sm: int = 0,
-                 rows=None, out=None, scratch=None, check_status: bool = True):
+                 rows=None, out=None, scratch=None, check_status: bool = True,
+                 validate: bool = True):
     """Run the fused alignment kernel over packed clouds.
 
     ``mode`` in {"shape", "esp", "pharm", "shape_pharm", "shape_color"}.  ``seed_q``/``seed_t``
     are (P,S,4)/(P,S,3).  Returns (score, q, t) per pair; ``rows`` (if given, a tuple of
     (P*S,), (P*S,4), (P*S,3) tensors) receives every start's best score and pose.
     Self overlaps default to the kernels' own (:func:`kernels.self_overlap`).
+    ``validate=False`` skips the pair-index range check (a device read-back) for callers that
+    validated their indices on the host; ``check_status=False`` skips reading the kernel's
+    status word (both keep the launch free of host synchronisation).
     """
     m = MODE_IDS[mode]
     shape = m != _lib.MODE_PHARM
@@ -96,7 +100,7 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
     n_fit = fit.n_mol if shape else fit_ph.n_mol
     if shape and pharm and (ref_ph.n_mol != n_ref or fit_ph.n_mol != n_fit):
         raise ValueError("shape and pharmacophore sets must describe the same molecules")
-    if P:
+    if P and validate:
         lo = int(torch.minimum(pair_ref.min(), pair_fit.min()))
         if lo < 0 or int(pair_ref.max()) >= n_ref or int(pair_fit.max()) >= n_fit:
             raise ValueError("pair index outside the molecule tables")

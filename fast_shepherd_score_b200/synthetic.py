@@ -125,3 +125,72 @@ def random_rotation(rng):
     return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
                      [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
                      [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
+
+
+def library_on_device(n_mol, seed=5, device="cuda", atom_lo=15, atom_hi=60, ph_lo=3, ph_hi=20,
+                      radius=6.0, min_dist=1.2, max_tries=64):
+    """A large shape+pharmacophore library generated directly on the device.
+
+    Same distributions as :func:`shape_pharm_molecules` (atoms uniform in a 6 A ball with
+    >= 1.2 A spacing, 3-20 pharmacophores of 8 uniform types near the atoms, unit vectors
+    for the directional types), drawn with a seeded ``torch.Generator`` on ``device`` so a
+    million molecules take seconds.  Returns (CloudSet atoms, PharmSet pharmacophores).
+    """
+    import torch
+    from .layout import CloudSet, PharmSet, _offsets
+    dev = torch.device(device)
+    g = torch.Generator(device=dev)
+    g.manual_seed(int(seed))
+    na = torch.randint(atom_lo, atom_hi + 1, (n_mol,), generator=g, device=dev)
+    nmax = int(atom_hi)
+    X = torch.zeros(n_mol, nmax, 3, device=dev)
+
+    def propose(k):
+        v = torch.randn(k, 3, generator=g, device=dev)
+        v = v / v.norm(dim=1, keepdim=True)
+        r = radius * torch.rand(k, generator=g, device=dev) ** (1.0 / 3.0)
+        return v * r[:, None]
+
+    md2 = min_dist * min_dist
+    for s in range(nmax):
+        need = torch.nonzero(na > s).flatten()
+        for _ in range(max_tries):
+            if need.numel() == 0:
+                break
+            cand = propose(need.numel())
+            if s == 0:
+                X[need, 0] = cand
+                need = need[:0]
+                break
+            d2 = ((X[need, :s] - cand[:, None, :]) ** 2).sum(-1).min(1).values
+            ok = d2 >= md2
+            X[need[ok], s] = cand[ok]
+            need = need[~ok]
+        if need.numel():
+            X[need, s] = propose(need.numel())
+    mask = torch.arange(nmax, device=dev)[None, :] < na[:, None]
+    pts = torch.zeros(int(na.sum()), 4, device=dev)
+    pts[:, :3] = X[mask]
+    counts = na.cpu().numpy().astype(np.int64)
+    atoms = CloudSet(pts, torch.from_numpy(_offsets(counts)).to(dev), counts, int(counts.max()))
+
+    npf = torch.randint(ph_lo, ph_hi + 1, (n_mol,), generator=g, device=dev)
+    tot = int(npf.sum())
+    mol = torch.repeat_interleave(torch.arange(n_mol, device=dev), npf)
+    pick = (torch.rand(tot, generator=g, device=dev) * na[mol]).long().clamp(max=nmax - 1)
+    anc_xyz = X[mol, pick] + 0.5 * torch.randn(tot, 3, generator=g, device=dev)
+    types = torch.randint(0, N_PHARM_TYPES, (tot,), generator=g, device=dev, dtype=torch.int32)
+    v = torch.randn(tot, 3, generator=g, device=dev)
+    v = v / v.norm(dim=1, keepdim=True)
+    directional = torch.zeros_like(types, dtype=torch.bool)
+    for t in DIRECTIONAL_TYPES:
+        directional |= types == t
+    v = torch.where(directional[:, None], v, torch.zeros_like(v))
+    anc = torch.zeros(tot, 4, device=dev)
+    anc[:, :3] = anc_xyz
+    anc[:, 3] = types.view(torch.float32)
+    vec = torch.zeros(tot, 4, device=dev)
+    vec[:, :3] = v
+    pc = npf.cpu().numpy().astype(np.int64)
+    pharm = PharmSet(anc, vec, torch.from_numpy(_offsets(pc)).to(dev), pc, int(pc.max()))
+    return atoms, pharm
