@@ -192,6 +192,10 @@ def run_cuda(args, wl):
             torch.empty(P * S, 3, device=dev))
     outb = (torch.empty(P, device=dev), torch.empty(P, 4, device=dev), torch.empty(P, 3, device=dev))
     align_ms = []
+    tile = {}
+    if args.tile:   # fixed tiling (no autotuning): lanes_per_pose,chunks,cta_per_sm,accumulate
+        v = [int(x) for x in args.tile.split(",")]
+        tile = dict(zip(("lanes_per_pose", "chunks", "cta_per_sm", "accumulate"), v))
 
     def step(record_kernel=False):
         if mode == "vol_pharm":
@@ -208,7 +212,7 @@ def run_cuda(args, wl):
         al.align_packed(amode, ref=rc, fit=fc, ref_ph=rp, fit_ph=fp, pair_ref=idx, pair_fit=idx,
                         seed_q=sq, seed_t=st, steps=wl["steps"], lr=wl["lr"], alpha=wl["alpha"],
                         lam=kl, ref_self=rs, fit_self=fs, ref_self_ph=rsp, fit_self_ph=fsp,
-                        order=order, rows=rows, out=outb, check_status=False)
+                        order=order, rows=rows, out=outb, check_status=False, **tile)
         if record_kernel:
             e1.record()
             align_ms.append((e0, e1))
@@ -563,6 +567,8 @@ def main(argv=None):
     ap.add_argument("--no-server", dest="server", action="store_false",
                     help="skip the screening-server leg (Poisson stream, p50/p99)")
     ap.add_argument("--server-seconds", type=float, default=20.0)
+    ap.add_argument("--tile", default="", help="fixed tiling instead of the autotuner: "
+                    "lanes_per_pose,chunks,cta_per_sm,accumulate (e.g. 32,0,0,2)")
     args = ap.parse_args(argv)
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":

@@ -13,7 +13,8 @@ import threading
 import torch
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libfss_cuda.so")
+# FSS_LIB selects another build of the same ABI (e.g. one compiled with other tuning macros)
+LIB_PATH = os.environ.get("FSS_LIB") or os.path.join(_HERE, "libfss_cuda.so")
 
 FSS_OK, FSS_ERR_INVALID, FSS_ERR_CUDA, FSS_ERR_NOMEM, FSS_ERR_UNSUPPORTED, FSS_ERR_TIMEOUT = range(6)
 MODE_SHAPE, MODE_ESP, MODE_PHARM, MODE_SHAPE_PHARM, MODE_SHAPE_COLOR = range(5)
@@ -40,6 +41,7 @@ class AlignDesc(ctypes.Structure):
         ("max_ref_points", _i32), ("max_fit_points", _i32),
         ("max_ref_features", _i32), ("max_fit_features", _i32),
         ("lanes_per_pose", _i32), ("chunks", _i32), ("cta_per_sm", _i32),
+        ("accumulate", _i32),
         ("scratch", _vp),
     ]
 
@@ -77,7 +79,7 @@ def load(build_if_missing: bool = True):
     with _LOCK:
         if _LIB is not None:
             return _LIB
-        if build_if_missing:
+        if build_if_missing and not os.environ.get("FSS_LIB"):
             from . import build as _build
             if _build.needs_build():
                 try:
@@ -94,7 +96,7 @@ def load(build_if_missing: bool = True):
             fn = getattr(lib, name)
             fn.argtypes = argt
             fn.restype = rest
-        if lib.fss_abi_version() != 1:
+        if lib.fss_abi_version() != 2:
             raise RuntimeError("libfss_cuda.so ABI version mismatch; rebuild the library")
         _LIB = lib
         return lib

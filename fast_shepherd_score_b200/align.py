@@ -65,14 +65,16 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
                  alpha: float = 0.81, lam: Optional[float] = None, color_weight: float = 0.5,
                  ref_self=None, fit_self=None, ref_self_ph=None, fit_self_ph=None,
                  order=None, lanes_per_pose: int = 0, chunks: int = 0, cta_per_sm: int = 0,
-                 rows=None, out=None, scratch=None, check_status: bool = True,
-                 validate: bool = True):
+                 accumulate: int = 0, rows=None, out=None, scratch=None,
+                 check_status: bool = True, validate: bool = True):
     """Run the fused alignment kernel over packed clouds.
 
     ``mode`` in {"shape", "esp", "pharm", "shape_pharm", "shape_color"}.  ``seed_q``/``seed_t``
     are (P,S,4)/(P,S,3).  Returns (score, q, t) per pair; ``rows`` (if given, a tuple of
     (P*S,), (P*S,4), (P*S,3) tensors) receives every start's best score and pose.
     Self overlaps default to the kernels' own (:func:`kernels.self_overlap`).
+    ``accumulate`` picks where the shape/ESP sums run: 0 automatic (autotuned), 1 FP32 lanes,
+    2 tensor cores (modes "shape" and "esp", 32 lanes per pose).
     ``validate=False`` skips the pair-index range check (a device read-back) for callers that
     validated their indices on the host; ``check_status=False`` skips reading the kernel's
     status word (both keep the launch free of host synchronisation).
@@ -127,13 +129,14 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
             order = cost_order(ref.counts[pr], fit.counts[pf], dev)
         else:
             order = cost_order(ref_ph.counts[pr], fit_ph.counts[pf], dev)
-    if (lanes_per_pose == 0 and chunks == 0 and cta_per_sm == 0 and autotune.enabled()
-            and P >= 64 and steps > 0):
+    if (lanes_per_pose == 0 and chunks == 0 and cta_per_sm == 0 and accumulate == 0
+            and autotune.enabled() and P >= 64 and steps > 0):
         tile = _tuned_tile(mode, shape, ref, fit, ref_ph, fit_ph, pair_ref, pair_fit, seed_q,
                            seed_t, steps, lr, alpha, lam, color_weight, ref_self, fit_self,
                            ref_self_ph, fit_self_ph)
         lanes_per_pose, chunks, cta_per_sm = (tile["lanes_per_pose"], tile["chunks"],
                                               tile["cta_per_sm"])
+        accumulate = tile.get("accumulate", 0)
     if rows is None:
         rows = (torch.empty(P * S, dtype=_f32, device=dev),
                 torch.empty(P * S, 4, dtype=_f32, device=dev),
@@ -144,7 +147,8 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
     scratch = _scratch(dev) if scratch is None else scratch
     LAST_TILE.clear()
     LAST_TILE.update(lanes_per_pose=int(lanes_per_pose), chunks=int(chunks),
-                     cta_per_sm=int(cta_per_sm), autotuned=autotune.enabled() and P >= 64)
+                     cta_per_sm=int(cta_per_sm), accumulate=int(accumulate),
+                     autotuned=autotune.enabled() and P >= 64)
     d = AlignDesc()
     d.mode, d.n_pairs, d.n_starts, d.steps = m, P, S, int(steps)
     d.pair_ref, d.pair_fit = ptr(pair_ref, _i32), ptr(pair_fit, _i32)
@@ -170,6 +174,7 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
     d.row_score, d.row_q, d.row_t = (ptr(rows[0], _f32), ptr(rows[1], _f32), ptr(rows[2], _f32))
     d.out_score, d.out_q, d.out_t = (ptr(out[0], _f32), ptr(out[1], _f32), ptr(out[2], _f32))
     d.lanes_per_pose, d.chunks, d.cta_per_sm = int(lanes_per_pose), int(chunks), int(cta_per_sm)
+    d.accumulate = int(accumulate)
     d.scratch = ptr(scratch, _i32)
     check(_lib.load().fss_align(d, stream_ptr(dev)), f"align[{mode}]")
     if check_status:

@@ -4,6 +4,8 @@ Tunables of one launch (``fss_align_desc``):
   lanes_per_pose  4, 8, 16 or 32 lanes cooperate on one pose (so 32/lanes starts per warp)
   chunks          start blocks per pair (a CTA owns one pair and n_starts/chunks starts)
   cta_per_sm      persistent CTAs per SM (1 or 2; 2 hides latency, 1 leaves more L1)
+  accumulate      1 = value/gradient sums on the FP32 lanes, 2 = on the tensor cores
+                  (shape/ESP modes; 32 lanes per pose)
 
 For a new problem shape the tuner times each candidate on a sample of the batch's pairs
 (the costliest and a spread of the rest) for a few Adam steps, with CUDA events, and keeps
@@ -84,7 +86,34 @@ def candidates(mode: str, max_fit: int, n_starts: int):
             continue
         for cps in (0, 2, 1):   # 0 = as many CTAs per SM as fit
             out.append({"lanes_per_pose": lpp, "chunks": 0, "cta_per_sm": cps})
+        # smaller CTAs (twice the default start blocks): less waiting at the per-item barrier
+        base = _auto_chunks(lpp, n_starts)
+        if 2 * base <= n_starts:
+            out.append({"lanes_per_pose": lpp, "chunks": 2 * base, "cta_per_sm": 0})
+    if mode in ("shape", "esp") and max_fit >= 16:
+        base = _auto_chunks(32, n_starts)
+        for ch, cps in ((0, 0), (0, 1), (2 * base, 0)):
+            if ch <= n_starts:
+                out.append({"lanes_per_pose": 32, "chunks": ch, "cta_per_sm": cps,
+                            "accumulate": 2})
     return out
+
+
+def _auto_chunks(lpp: int, n_starts: int, max_threads: int = 320) -> int:
+    """The library's default start-block count for a lanes-per-pose choice: the fewest idle
+    pose slots with CTAs of at most max_threads threads (fss_align.cu auto_tile)."""
+    best_c, best_w = 1, 1 << 30
+    for c in range(1, n_starts + 1):
+        ppc = -(-n_starts // c)
+        if ppc > max_threads // lpp:
+            continue
+        warps = -(-ppc * lpp // 32)
+        waste = warps * 32 // lpp * c - n_starts
+        if waste < best_w:
+            best_c, best_w = c, waste
+        if waste == 0:
+            break
+    return best_c
 
 
 def lookup(key: str) -> Optional[dict]:
@@ -112,7 +141,8 @@ def tune(run, key: str, cands, repeats: int = 2) -> dict:
             t = min(ms)
         except (ValueError, RuntimeError):
             continue
-        timings[f"{c['lanes_per_pose']}x{c['cta_per_sm']}"] = round(t, 4)
+        tag = "tc" if c.get("accumulate") == 2 else ""
+        timings[f"{tag}{c['lanes_per_pose']}x{c['cta_per_sm']}c{c['chunks']}"] = round(t, 4)
         if t < best_ms:
             best, best_ms = c, t
     if best is None:

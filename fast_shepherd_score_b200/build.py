@@ -41,25 +41,30 @@ def needs_build() -> bool:
     return any(os.path.getmtime(p) > t for p in sources())
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and not needs_build():
+def build(force: bool = False, verbose: bool = False, out: str = None, defines=()) -> str:
+    """Compile every source and link ``out`` (default: the package's libfss_cuda.so).
+    ``defines`` (e.g. ``["FSS_JB2=3"]``) set the kernels' compile-time tuning macros."""
+    target = os.path.abspath(out) if out else LIB
+    if not force and target == LIB and not needs_build():
         return LIB
-    objdir = os.path.join(HERE, "_build")
+    objdir = (os.path.join(HERE, "_build") if target == LIB else
+              os.path.join(os.path.dirname(target), "_build_" + os.path.basename(target)))
     os.makedirs(objdir, exist_ok=True)
     flags = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-cudart", "static",
                     "-I", os.path.join(ROOT, "include"), "-I", CSRC]
     if verbose:
         flags += ["-Xptxas", "-v"]
+    flags += [f"-D{d}" for d in defines]
     objs = []
     for src in SOURCES:
         obj = os.path.join(objdir, src.replace(".cu", ".o"))
         cmd = [nvcc(), "-c", os.path.join(CSRC, src), "-o", obj] + flags
         subprocess.run(cmd, check=True)
         objs.append(obj)
-    tmp = LIB + ".tmp"
+    tmp = target + ".tmp"
     subprocess.run([nvcc(), "-shared", "-o", tmp] + objs + ARCH + ["-cudart", "static"], check=True)
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, target)
+    return target
 
 
 if __name__ == "__main__":

@@ -10,6 +10,7 @@
 #include <cmath>
 
 #include "fss_internal.cuh"
+#include "fss_mma.cuh"
 
 namespace fss {
 
@@ -32,23 +33,38 @@ struct AlignParams {
   int* counter;
 };
 
-constexpr int kMaxThreads = 320;  // 10 warps; with 2 CTAs per SM the kernel gets <= 96 registers
+#ifndef FSS_MAX_THREADS
+#define FSS_MAX_THREADS 320
+#endif
+#ifndef FSS_MIN_CTAS
+#define FSS_MIN_CTAS 2
+#endif
+// 320 threads = 10 warps; with 2 CTAs per SM the kernel gets <= 96 registers
+constexpr int kMaxThreads = FSS_MAX_THREADS;
 
-template <int LPP, int MODE>
-__global__ void __launch_bounds__(kMaxThreads, 2) align_kernel(const AlignParams p) {
+// TC: shape/ESP sums on the tensor cores (fss_mma.cuh); requires LPP == 32 and a mode
+// without a pharmacophore channel.
+template <int LPP, int MODE, bool TC>
+__global__ void __launch_bounds__(kMaxThreads, FSS_MIN_CTAS) align_kernel(const AlignParams p) {
   constexpr bool kShape = MODE == FSS_MODE_SHAPE || MODE == FSS_MODE_ESP ||
                           MODE == FSS_MODE_SHAPE_PHARM || MODE == FSS_MODE_SHAPE_COLOR;
   constexpr bool kEsp = MODE == FSS_MODE_ESP;
   constexpr bool kPharm = MODE == FSS_MODE_PHARM || MODE == FSS_MODE_SHAPE_PHARM ||
                           MODE == FSS_MODE_SHAPE_COLOR;
+  static_assert(!TC || (LPP == 32 && !kPharm), "tensor-core sums: whole-warp shape/ESP poses");
   extern __shared__ __align__(16) float4 smem[];
-  float4* sP = smem;                 // 2 * maxN (duplicated expanded reference)
-  float4* sB = sP + 2 * p.maxN;
+  // FP32 path: sP = 2 * maxN duplicated expanded reference (+ sQc).  Tensor-core path:
+  // sP = 8 * nbMax block-interleaved reference, sCm/sQm after the fit cloud.
+  const int nbMax = (p.maxN + 7) >> 3;
+  float4* sP = smem;
+  float4* sB = sP + (TC ? kMmaP4PerBlock * nbMax : 2 * p.maxN);
   float4* sRA = sB + p.maxM;
   float4* sRV = sRA + p.maxNp;
   float4* sFA = sRV + p.maxNp;
   float4* sFV = sFA + p.maxMp;
   float2* sQc = reinterpret_cast<float2*>(sFV + p.maxMp);
+  float2* sCm = reinterpret_cast<float2*>(sB + p.maxM);
+  float2* sQm = sCm + kMmaC2PerBlock * nbMax;
   __shared__ float red[96];
   __shared__ int s_item;
 
@@ -88,7 +104,8 @@ __global__ void __launch_bounds__(kMaxThreads, 2) align_kernel(const AlignParams
     float3 c = make_float3(0.f, 0.f, 0.f);
     if (kShape) {
       c = block_centroid(p.ref_pts + r0, N, red);
-      stage_ref<kEsp>(p.ref_pts + r0, N, c, p.k, p.e, sP, sQc);
+      if constexpr (TC) stage_ref_mma<kEsp>(p.ref_pts + r0, N, c, p.k, p.e, sP, sQm, sCm);
+      else stage_ref<kEsp>(p.ref_pts + r0, N, c, p.k, p.e, sP, sQc);
       stage_copy(p.fit_pts + f0, M, sB);
     }
     if (kPharm) {
@@ -121,8 +138,12 @@ __global__ void __launch_bounds__(kMaxThreads, 2) align_kernel(const AlignParams
         if (kShape) {
           Moments ms;
           ms.zero();
-          shape_pose<LPP, kEsp>(sP, sQc, sB, N, M, lane, R, s.t[0], s.t[1], s.t[2], p.k, p.e,
-                                p.inv2k, ms);
+          if constexpr (TC)
+            shape_pose_mma<kEsp>(sP, sQm, sCm, sB, N, M, lane, R, s.t[0], s.t[1], s.t[2], p.k,
+                                 p.e, ms);
+          else
+            shape_pose<LPP, kEsp>(sP, sQc, sB, N, M, lane, R, s.t[0], s.t[1], s.t[2], p.k,
+                                  p.e, p.inv2k, ms);
           rs.from(ms, s.q);
           rs.template group_sum<LPP>();
           rs.scale(p.Kc, p.aKc);
@@ -252,10 +273,10 @@ PharmTables make_pharm_tables(bool directional) {
 
 namespace {
 
-template <int LPP, int MODE>
+template <int LPP, int MODE, bool TC = false>
 int launch_align(const AlignParams& prm, int threads, int cta_per_sm, size_t smem,
                  cudaStream_t st) {
-  auto kern = align_kernel<LPP, MODE>;
+  auto kern = align_kernel<LPP, MODE, TC>;
   cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)smem);
   if (ce != cudaSuccess)
@@ -272,8 +293,11 @@ int launch_align(const AlignParams& prm, int threads, int cta_per_sm, size_t sme
 }
 
 template <int MODE>
-int dispatch_lpp(int lpp, const AlignParams& prm, int threads, int cps, size_t smem,
+int dispatch_lpp(int lpp, bool tc, const AlignParams& prm, int threads, int cps, size_t smem,
                  cudaStream_t st) {
+  if constexpr (MODE == FSS_MODE_SHAPE || MODE == FSS_MODE_ESP) {
+    if (tc) return launch_align<32, MODE, true>(prm, threads, cps, smem, st);
+  }
   switch (lpp) {
     case 4: return launch_align<4, MODE>(prm, threads, cps, smem, st);
     case 8: return launch_align<8, MODE>(prm, threads, cps, smem, st);
@@ -345,7 +369,15 @@ int align_launch(const fss_align_desc* d, cudaStream_t st) {
     return set_error(FSS_ERR_CUDA, std::string("fss_align: scratch reset: ") + cudaGetErrorString(ce));
   if (d->n_pairs == 0) return FSS_OK;
 
-  int lpp = d->lanes_per_pose, chunks = d->chunks;
+  const bool tc_mode = d->mode == FSS_MODE_SHAPE || d->mode == FSS_MODE_ESP;
+  if (d->accumulate < 0 || d->accumulate > 2)
+    return set_error(FSS_ERR_INVALID, "fss_align: accumulate must be 0, 1 or 2");
+  if (d->accumulate == 2 && !tc_mode)
+    return set_error(FSS_ERR_INVALID, "fss_align: tensor-core sums need mode SHAPE or ESP");
+  const bool tc = d->accumulate == 2;
+  if (tc && d->lanes_per_pose != 0 && d->lanes_per_pose != 32)
+    return set_error(FSS_ERR_INVALID, "fss_align: tensor-core sums use 32 lanes per pose");
+  int lpp = tc ? 32 : d->lanes_per_pose, chunks = d->chunks;
   auto_tile(d->mode, shape ? maxM : maxMp, d->n_starts, &lpp, &chunks);
   if (chunks < 1 || chunks > d->n_starts)
     return set_error(FSS_ERR_INVALID, "fss_align: chunks must be in [1, n_starts]");
@@ -382,15 +414,19 @@ int align_launch(const fss_align_desc* d, cudaStream_t st) {
   p.row_score = d->row_score; p.row_q = d->row_q; p.row_t = d->row_t;
   p.counter = d->scratch;
 
-  const size_t smem = sizeof(float4) * (2 * (size_t)maxN + maxM + 2 * (size_t)maxNp + 2 * (size_t)maxMp) +
-                      sizeof(float2) * (d->mode == FSS_MODE_ESP ? (size_t)maxN : 0) + 16;
+  const size_t nb = ((size_t)maxN + 7) / 8;
+  const size_t smem =
+      tc ? sizeof(float4) * (kMmaP4PerBlock * nb + maxM) +
+               sizeof(float2) * (kMmaC2PerBlock + kMmaQ2PerBlock) * nb + 16
+         : sizeof(float4) * (2 * (size_t)maxN + maxM + 2 * (size_t)maxNp + 2 * (size_t)maxMp) +
+               sizeof(float2) * (d->mode == FSS_MODE_ESP ? (size_t)maxN : 0) + 16;
   int rc;
   switch (d->mode) {
-    case FSS_MODE_SHAPE: rc = dispatch_lpp<FSS_MODE_SHAPE>(lpp, p, threads, d->cta_per_sm, smem, st); break;
-    case FSS_MODE_ESP: rc = dispatch_lpp<FSS_MODE_ESP>(lpp, p, threads, d->cta_per_sm, smem, st); break;
-    case FSS_MODE_PHARM: rc = dispatch_lpp<FSS_MODE_PHARM>(lpp, p, threads, d->cta_per_sm, smem, st); break;
-    case FSS_MODE_SHAPE_PHARM: rc = dispatch_lpp<FSS_MODE_SHAPE_PHARM>(lpp, p, threads, d->cta_per_sm, smem, st); break;
-    default: rc = dispatch_lpp<FSS_MODE_SHAPE_COLOR>(lpp, p, threads, d->cta_per_sm, smem, st); break;
+    case FSS_MODE_SHAPE: rc = dispatch_lpp<FSS_MODE_SHAPE>(lpp, tc, p, threads, d->cta_per_sm, smem, st); break;
+    case FSS_MODE_ESP: rc = dispatch_lpp<FSS_MODE_ESP>(lpp, tc, p, threads, d->cta_per_sm, smem, st); break;
+    case FSS_MODE_PHARM: rc = dispatch_lpp<FSS_MODE_PHARM>(lpp, tc, p, threads, d->cta_per_sm, smem, st); break;
+    case FSS_MODE_SHAPE_PHARM: rc = dispatch_lpp<FSS_MODE_SHAPE_PHARM>(lpp, tc, p, threads, d->cta_per_sm, smem, st); break;
+    default: rc = dispatch_lpp<FSS_MODE_SHAPE_COLOR>(lpp, tc, p, threads, d->cta_per_sm, smem, st); break;
   }
   if (rc != FSS_OK) return rc;
   if (d->out_score && d->out_q && d->out_t)

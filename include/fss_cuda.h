@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define FSS_ABI_VERSION 1
+#define FSS_ABI_VERSION 2
 
 enum fss_status {
   FSS_OK = 0,
@@ -149,6 +149,9 @@ typedef struct fss_align_desc {
   int32_t lanes_per_pose;    /* 4, 8, 16 or 32 lanes cooperate on one pose */
   int32_t chunks;            /* start blocks per pair (CTA covers n_starts/chunks starts) */
   int32_t cta_per_sm;        /* persistent CTAs per SM */
+  int32_t accumulate;        /* where the value/gradient sums of the shape and ESP channels
+                              * run: 0 automatic, 1 FP32 lanes, 2 tensor cores (tf32 hi/lo
+                              * split MMA, one warp per pose; modes SHAPE and ESP) */
   /* scratch: two device int32 -- [0] work counter, [1] status flags (bit 0: a pair was
    * larger than the max_* extents).  The launch zeroes both on `stream`. */
   int32_t *scratch;

@@ -26,7 +26,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_limits():
     lib = _lib.load()
-    assert lib.fss_abi_version() == 1
+    assert lib.fss_abi_version() == 2
     assert lib.fss_max_points() >= 1024
 
 
