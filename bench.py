@@ -212,7 +212,8 @@ def run_cuda(args, wl):
         al.align_packed(amode, ref=rc, fit=fc, ref_ph=rp, fit_ph=fp, pair_ref=idx, pair_fit=idx,
                         seed_q=sq, seed_t=st, steps=wl["steps"], lr=wl["lr"], alpha=wl["alpha"],
                         lam=kl, ref_self=rs, fit_self=fs, ref_self_ph=rsp, fit_self_ph=fsp,
-                        order=order, rows=rows, out=outb, check_status=False, **tile)
+                        order=order, rows=rows, out=outb, check_status=False, validate=False,
+                        **tile)
         if record_kernel:
             e1.record()
             align_ms.append((e0, e1))

@@ -127,11 +127,13 @@ __device__ __forceinline__ void mma_pass(const float4* __restrict__ sPm,
       if (!FACT) E = __fadd2_rn(E, NW[r]);
       G[r] = f2(ex2(E.x), ex2(E.y));
     }
+    const float2 neg1 = f2(-1.f, -1.f);
 #pragma unroll
     for (int m = 0; m < 2; ++m) {
       const float2 u = G[2 * m], v = G[2 * m + 1];  // rows g / g+8 of tile m; k = t, t+4
       const float2 uh = f2(tf32_hi(u.x), tf32_hi(u.y)), vh = f2(tf32_hi(v.x), tf32_hi(v.y));
-      const float2 ul = __fadd2_rn(u, f2(-uh.x, -uh.y)), vl = __fadd2_rn(v, f2(-vh.x, -vh.y));
+      // lo = g - hi, exact (hi is a truncation of g)
+      const float2 ul = __ffma2_rn(uh, neg1, u), vl = __ffma2_rn(vh, neg1, v);
       mma_tf32(D[m], uh.x, vh.x, uh.y, vh.y, cb);
       mma_tf32(D[m], ul.x, vl.x, ul.y, vl.y, cb);
     }
