@@ -41,7 +41,7 @@ class AlignDesc(ctypes.Structure):
         ("max_ref_points", _i32), ("max_fit_points", _i32),
         ("max_ref_features", _i32), ("max_fit_features", _i32),
         ("lanes_per_pose", _i32), ("chunks", _i32), ("cta_per_sm", _i32),
-        ("accumulate", _i32),
+        ("accumulate", _i32), ("kernel_variant", _i32),
         ("scratch", _vp),
     ]
 

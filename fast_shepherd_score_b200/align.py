@@ -65,7 +65,8 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
                  alpha: float = 0.81, lam: Optional[float] = None, color_weight: float = 0.5,
                  ref_self=None, fit_self=None, ref_self_ph=None, fit_self_ph=None,
                  order=None, lanes_per_pose: int = 0, chunks: int = 0, cta_per_sm: int = 0,
-                 accumulate: int = 0, rows=None, out=None, scratch=None,
+                 accumulate: int = 0, kernel_variant: int = 0, rows=None, out=None,
+                 scratch=None,
                  check_status: bool = True, validate: bool = True):
     """Run the fused alignment kernel over packed clouds.
 
@@ -74,7 +75,9 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
     (P*S,), (P*S,4), (P*S,3) tensors) receives every start's best score and pose.
     Self overlaps default to the kernels' own (:func:`kernels.self_overlap`).
     ``accumulate`` picks where the shape/ESP sums run: 0 automatic (autotuned), 1 FP32 lanes,
-    2 tensor cores (modes "shape" and "esp", 32 lanes per pose).
+    2 tensor cores (modes "shape" and "esp", 32 lanes per pose).  ``kernel_variant`` picks the
+    FP32-lane loop's code variant: 0 automatic, 1 base, 2 wide register tile, 3 one-CTA/SM
+    register budget (2 and 3 for "shape" and "esp").
     ``validate=False`` skips the pair-index range check (a device read-back) for callers that
     validated their indices on the host; ``check_status=False`` skips reading the kernel's
     status word (both keep the launch free of host synchronisation).
@@ -130,13 +133,14 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
         else:
             order = cost_order(ref_ph.counts[pr], fit_ph.counts[pf], dev)
     if (lanes_per_pose == 0 and chunks == 0 and cta_per_sm == 0 and accumulate == 0
-            and autotune.enabled() and P >= 64 and steps > 0):
+            and kernel_variant == 0 and autotune.enabled() and P >= 64 and steps > 0):
         tile = _tuned_tile(mode, shape, ref, fit, ref_ph, fit_ph, pair_ref, pair_fit, seed_q,
                            seed_t, steps, lr, alpha, lam, color_weight, ref_self, fit_self,
                            ref_self_ph, fit_self_ph)
         lanes_per_pose, chunks, cta_per_sm = (tile["lanes_per_pose"], tile["chunks"],
                                               tile["cta_per_sm"])
         accumulate = tile.get("accumulate", 0)
+        kernel_variant = tile.get("kernel_variant", 0)
     if rows is None:
         rows = (torch.empty(P * S, dtype=_f32, device=dev),
                 torch.empty(P * S, 4, dtype=_f32, device=dev),
@@ -148,6 +152,7 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
     LAST_TILE.clear()
     LAST_TILE.update(lanes_per_pose=int(lanes_per_pose), chunks=int(chunks),
                      cta_per_sm=int(cta_per_sm), accumulate=int(accumulate),
+                     kernel_variant=int(kernel_variant),
                      autotuned=autotune.enabled() and P >= 64)
     d = AlignDesc()
     d.mode, d.n_pairs, d.n_starts, d.steps = m, P, S, int(steps)
@@ -175,6 +180,7 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
     d.out_score, d.out_q, d.out_t = (ptr(out[0], _f32), ptr(out[1], _f32), ptr(out[2], _f32))
     d.lanes_per_pose, d.chunks, d.cta_per_sm = int(lanes_per_pose), int(chunks), int(cta_per_sm)
     d.accumulate = int(accumulate)
+    d.kernel_variant = int(kernel_variant)
     d.scratch = ptr(scratch, _i32)
     check(_lib.load().fss_align(d, stream_ptr(dev)), f"align[{mode}]")
     if check_status:

@@ -6,6 +6,8 @@ Tunables of one launch (``fss_align_desc``):
   cta_per_sm      persistent CTAs per SM (1 or 2; 2 hides latency, 1 leaves more L1)
   accumulate      1 = value/gradient sums on the FP32 lanes, 2 = on the tensor cores
                   (shape/ESP modes; 32 lanes per pose)
+  kernel_variant  code variant of the FP32-lane loop (shape/ESP modes): 1 base, 2 wide
+                  register tile, 3 one-CTA/SM register budget
 
 For a new problem shape the tuner times each candidate on a sample of the batch's pairs
 (the costliest and a spread of the rest) for a few Adam steps, with CUDA events, and keeps
@@ -79,17 +81,21 @@ def shape_key(device, mode: str, max_ref: int, max_fit: int, mean_fit: float, n_
 
 def candidates(mode: str, max_fit: int, n_starts: int):
     out = []
+    variants = (1, 2, 3) if mode in ("shape", "esp") else (0,)
     for lpp in LANES:
         if mode != "pharm" and lpp > 4 and lpp // 2 >= max(max_fit, 1):
             continue  # more lanes than fit points: idle lanes
         if mode == "pharm" and lpp > 8:
             continue
-        for cps in (0, 2, 1):   # 0 = as many CTAs per SM as fit
-            out.append({"lanes_per_pose": lpp, "chunks": 0, "cta_per_sm": cps})
-        # smaller CTAs (twice the default start blocks): less waiting at the per-item barrier
-        base = _auto_chunks(lpp, n_starts)
-        if 2 * base <= n_starts:
-            out.append({"lanes_per_pose": lpp, "chunks": 2 * base, "cta_per_sm": 0})
+        for var in variants:
+            for cps in (0, 2, 1):   # 0 = as many CTAs per SM as fit
+                out.append({"lanes_per_pose": lpp, "chunks": 0, "cta_per_sm": cps,
+                            "kernel_variant": var})
+            # smaller CTAs (twice the default start blocks): less waiting at the per-item barrier
+            base = _auto_chunks(lpp, n_starts)
+            if 2 * base <= n_starts:
+                out.append({"lanes_per_pose": lpp, "chunks": 2 * base, "cta_per_sm": 0,
+                            "kernel_variant": var})
     if mode in ("shape", "esp") and max_fit >= 16:
         base = _auto_chunks(32, n_starts)
         for ch, cps in ((0, 0), (0, 1), (2 * base, 0)):
@@ -141,7 +147,7 @@ def tune(run, key: str, cands, repeats: int = 2) -> dict:
             t = min(ms)
         except (ValueError, RuntimeError):
             continue
-        tag = "tc" if c.get("accumulate") == 2 else ""
+        tag = "tc" if c.get("accumulate") == 2 else f"v{c.get('kernel_variant', 0)}:"
         timings[f"{tag}{c['lanes_per_pose']}x{c['cta_per_sm']}c{c['chunks']}"] = round(t, 4)
         if t < best_ms:
             best, best_ms = c, t

@@ -7,6 +7,7 @@ time; the host language binding (``fast_shepherd_score_b200._lib``) loads it wit
 """
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -16,8 +17,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libfss_cuda.so")
-SOURCES = ["fss_capi.cu", "fss_align.cu", "fss_eval.cu", "fss_seeds.cu", "fss_score.cu",
-           "fss_probe.cu", "fss_static.cu"]
+SOURCES = ["fss_capi.cu", "fss_align.cu", "fss_align_shape.cu", "fss_align_esp.cu",
+           "fss_align_pharm.cu", "fss_eval.cu", "fss_seeds.cu", "fss_score.cu", "fss_probe.cu",
+           "fss_static.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -55,12 +57,15 @@ def build(force: bool = False, verbose: bool = False, out: str = None, defines=(
     if verbose:
         flags += ["-Xptxas", "-v"]
     flags += [f"-D{d}" for d in defines]
-    objs = []
-    for src in SOURCES:
-        obj = os.path.join(objdir, src.replace(".cu", ".o"))
-        cmd = [nvcc(), "-c", os.path.join(CSRC, src), "-o", obj] + flags
-        subprocess.run(cmd, check=True)
-        objs.append(obj)
+    objs = [os.path.join(objdir, src.replace(".cu", ".o")) for src in SOURCES]
+
+    def compile_one(src_obj):
+        src, obj = src_obj
+        subprocess.run([nvcc(), "-c", os.path.join(CSRC, src), "-o", obj] + flags, check=True)
+
+    # translation units are independent: compile them in parallel
+    with concurrent.futures.ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 1)) as ex:
+        list(ex.map(compile_one, zip(SOURCES, objs)))
     tmp = target + ".tmp"
     subprocess.run([nvcc(), "-shared", "-o", tmp] + objs + ARCH + ["-cudart", "static"], check=True)
     os.replace(tmp, target)

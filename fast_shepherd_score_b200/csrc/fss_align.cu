@@ -1,180 +1,12 @@
-// fss_align.cu -- the fused persistent alignment kernel and its helpers.
-//
-// One launch runs every (pair, start) pose for all Adam steps.  Work item = (pair, block
-// of starts); a persistent grid pulls items from a device counter in cost order (costliest
-// pairs first), stages the pair's clouds in shared memory once and keeps every pose's
-// optimiser state in registers for the whole loop.  LPP lanes cooperate on one pose; the
-// poses of one CTA all belong to the same pair so the shared-memory reads of the reference
-// cloud are warp-wide broadcasts and every loop bound is uniform.
+// fss_align.cu -- host side of the fused alignment (validation, tiling, dispatch) and the
+// small helper kernels (per-pair argmax, self overlaps).  The fused kernel itself lives in
+// fss_align_kernel.cuh and is instantiated per mode in fss_align_<mode>.cu.
 #include <algorithm>
 #include <cmath>
 
-#include "fss_internal.cuh"
-#include "fss_mma.cuh"
+#include "fss_align_kernel.cuh"
 
 namespace fss {
-
-struct AlignParams {
-  int mode, n_pairs, n_starts, steps, chunks, n_items;
-  int maxN, maxM, maxNp, maxMp;
-  const int* pair_ref;
-  const int* pair_fit;
-  const int* order;
-  const float4* ref_pts; const int* ref_off;
-  const float4* fit_pts; const int* fit_off;
-  const float* ref_self; const float* fit_self;
-  const float4* ref_anc; const float4* ref_vec; const int* ref_ph_off;
-  const float4* fit_anc; const float4* fit_vec; const int* fit_ph_off;
-  const float* ref_self_ph; const float* fit_self_ph;
-  const float* seed_q; const float* seed_t;
-  float alpha, k, e, inv2k, Kc, aKc, w, lr;
-  PharmTables tab;
-  float* row_score; float* row_q; float* row_t;
-  int* counter;
-};
-
-#ifndef FSS_MAX_THREADS
-#define FSS_MAX_THREADS 320
-#endif
-#ifndef FSS_MIN_CTAS
-#define FSS_MIN_CTAS 2
-#endif
-// 320 threads = 10 warps; with 2 CTAs per SM the kernel gets <= 96 registers
-constexpr int kMaxThreads = FSS_MAX_THREADS;
-
-// TC: shape/ESP sums on the tensor cores (fss_mma.cuh); requires LPP == 32 and a mode
-// without a pharmacophore channel.
-template <int LPP, int MODE, bool TC>
-__global__ void __launch_bounds__(kMaxThreads, FSS_MIN_CTAS) align_kernel(const AlignParams p) {
-  constexpr bool kShape = MODE == FSS_MODE_SHAPE || MODE == FSS_MODE_ESP ||
-                          MODE == FSS_MODE_SHAPE_PHARM || MODE == FSS_MODE_SHAPE_COLOR;
-  constexpr bool kEsp = MODE == FSS_MODE_ESP;
-  constexpr bool kPharm = MODE == FSS_MODE_PHARM || MODE == FSS_MODE_SHAPE_PHARM ||
-                          MODE == FSS_MODE_SHAPE_COLOR;
-  static_assert(!TC || (LPP == 32 && !kPharm), "tensor-core sums: whole-warp shape/ESP poses");
-  extern __shared__ __align__(16) float4 smem[];
-  // FP32 path: sP = 2 * maxN duplicated expanded reference (+ sQc).  Tensor-core path:
-  // sP = 8 * nbMax block-interleaved reference, sCm/sQm after the fit cloud.
-  const int nbMax = (p.maxN + 7) >> 3;
-  float4* sP = smem;
-  float4* sB = sP + (TC ? kMmaP4PerBlock * nbMax : 2 * p.maxN);
-  float4* sRA = sB + p.maxM;
-  float4* sRV = sRA + p.maxNp;
-  float4* sFA = sRV + p.maxNp;
-  float4* sFV = sFA + p.maxMp;
-  float2* sQc = reinterpret_cast<float2*>(sFV + p.maxMp);
-  float2* sCm = reinterpret_cast<float2*>(sB + p.maxM);
-  float2* sQm = sCm + kMmaC2PerBlock * nbMax;
-  __shared__ float red[96];
-  __shared__ int s_item;
-
-  const int tid = threadIdx.x;
-  const int grp = tid / LPP, lane = tid % LPP;
-  const int ppc = blockDim.x / LPP;  // poses per CTA
-  constexpr int kGroupsPerWarp = 32 / LPP;
-
-  for (;;) {
-    if (tid == 0) s_item = atomicAdd(p.counter, 1);
-    __syncthreads();
-    const int item = s_item;
-    if (item >= p.n_items) break;
-    const int pidx = p.order ? p.order[item / p.chunks] : item / p.chunks;
-    const int chunk = item % p.chunks;
-    const int ri = p.pair_ref[pidx], fi = p.pair_fit[pidx];
-
-    // ---- stage the pair's clouds -------------------------------------------------------
-    int N = 0, M = 0, Np = 0, Mp = 0, r0 = 0, f0 = 0, rp0 = 0, fp0 = 0;
-    if (kShape) {
-      r0 = p.ref_off[ri]; f0 = p.fit_off[fi];
-      N = p.ref_off[ri + 1] - r0;
-      M = p.fit_off[fi + 1] - f0;
-    }
-    if (kPharm) {
-      rp0 = p.ref_ph_off[ri]; fp0 = p.fit_ph_off[fi];
-      Np = p.ref_ph_off[ri + 1] - rp0;
-      Mp = p.fit_ph_off[fi + 1] - fp0;
-    }
-    if (N < 0 || M < 0 || Np < 0 || Mp < 0 || N > p.maxN || M > p.maxM || Np > p.maxNp ||
-        Mp > p.maxMp) {
-      // larger than the tiles this launch was sized for: flag it, leave its rows untouched
-      if (tid == 0) atomicOr(p.counter + 1, 1);
-      __syncthreads();
-      continue;
-    }
-    float3 c = make_float3(0.f, 0.f, 0.f);
-    if (kShape) {
-      c = block_centroid(p.ref_pts + r0, N, red);
-      if constexpr (TC) stage_ref_mma<kEsp>(p.ref_pts + r0, N, c, p.k, p.e, sP, sQm, sCm);
-      else stage_ref<kEsp>(p.ref_pts + r0, N, c, p.k, p.e, sP, sQc);
-      stage_copy(p.fit_pts + f0, M, sB);
-    }
-    if (kPharm) {
-      if (!kShape) c = block_centroid(p.ref_anc + rp0, Np, red);
-      stage_ref_pharm(p.ref_anc + rp0, p.ref_vec ? p.ref_vec + rp0 : nullptr, Np, c, sRA, sRV);
-      stage_fit_pharm(p.fit_anc + fp0, p.fit_vec ? p.fit_vec + fp0 : nullptr, Mp, sFA, sFV);
-    }
-    __syncthreads();
-
-    const float Us = p.ref_self[ri] + p.fit_self[fi];
-    const float Uc = kShape && kPharm ? p.ref_self_ph[ri] + p.fit_self_ph[fi] : 0.f;
-    const int start = chunk * ppc + grp;
-    const int warp_first = chunk * ppc + (tid >> 5) * kGroupsPerWarp;
-    if (warp_first < p.n_starts) {  // whole idle warps skip the loop; idle groups shadow one
-      const bool active = start < p.n_starts;
-      const size_t row = (size_t)pidx * p.n_starts + (active ? start : p.n_starts - 1);
-      PoseState s;
-      {
-        float q0[4], t0[3];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) q0[i] = p.seed_q[row * 4 + i];
-        t0[0] = p.seed_t[row * 3 + 0] - c.x;
-        t0[1] = p.seed_t[row * 3 + 1] - c.y;
-        t0[2] = p.seed_t[row * 3 + 2] - c.z;
-        pose_init(s, q0, t0);
-      }
-      for (int step = 0; step < p.steps; ++step) {
-        const Rot R = quat_to_rot(s.q);
-        Reduced rs;
-        if (kShape) {
-          Moments ms;
-          ms.zero();
-          if constexpr (TC)
-            shape_pose_mma<kEsp>(sP, sQm, sCm, sB, N, M, lane, R, s.t[0], s.t[1], s.t[2], p.k,
-                                 p.e, ms);
-          else
-            shape_pose<LPP, kEsp>(sP, sQc, sB, N, M, lane, R, s.t[0], s.t[1], s.t[2], p.k,
-                                  p.e, p.inv2k, ms);
-          rs.from(ms, s.q);
-          rs.template group_sum<LPP>();
-          rs.scale(p.Kc, p.aKc);
-        }
-        if (kPharm) {
-          Moments mc;
-          mc.zero();
-          pharm_pose<LPP>(sRA, sRV, sFA, sFV, Np, Mp, lane, R, s.t[0], s.t[1], s.t[2], p.tab,
-                          mc);
-          Reduced rc;
-          rc.from(mc, s.q);
-          rc.template group_sum<LPP>();
-          if (kShape) step_combo(s, rs, Us, rc, Uc, p.w, p.lr);
-          else step_single(s, rc, Us, p.lr);
-        } else {
-          step_single(s, rs, Us, p.lr);
-        }
-      }
-      if (active && lane == 0) {
-        const size_t r = (size_t)pidx * p.n_starts + start;
-        p.row_score[r] = s.best;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) p.row_q[r * 4 + i] = s.bq[i];
-        p.row_t[r * 3 + 0] = s.bt[0] + c.x;
-        p.row_t[r * 3 + 1] = s.bt[1] + c.y;
-        p.row_t[r * 3 + 2] = s.bt[2] + c.z;
-      }
-    }
-    __syncthreads();  // shared memory is restaged for the next item
-  }
-}
 
 // Per-pair argmax over starts (first index wins ties, as torch.argmax).
 __global__ void pick_best_kernel(const float* __restrict__ rs, const float* __restrict__ rq,
@@ -273,40 +105,6 @@ PharmTables make_pharm_tables(bool directional) {
 
 namespace {
 
-template <int LPP, int MODE, bool TC = false>
-int launch_align(const AlignParams& prm, int threads, int cta_per_sm, size_t smem,
-                 cudaStream_t st) {
-  auto kern = align_kernel<LPP, MODE, TC>;
-  cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)smem);
-  if (ce != cudaSuccess)
-    return set_error(FSS_ERR_CUDA, std::string("fss_align: shared-memory attribute: ") +
-                                       cudaGetErrorString(ce));
-  int occ = 0;
-  ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem);
-  if (ce != cudaSuccess || occ <= 0)
-    return set_error(FSS_ERR_UNSUPPORTED, "fss_align: the tile does not fit on an SM");
-  if (cta_per_sm > 0) occ = std::min(occ, cta_per_sm);
-  const int grid = std::max(1, std::min(prm.n_items, occ * num_sms()));
-  kern<<<grid, threads, smem, st>>>(prm);
-  return check_launch("fss_align");
-}
-
-template <int MODE>
-int dispatch_lpp(int lpp, bool tc, const AlignParams& prm, int threads, int cps, size_t smem,
-                 cudaStream_t st) {
-  if constexpr (MODE == FSS_MODE_SHAPE || MODE == FSS_MODE_ESP) {
-    if (tc) return launch_align<32, MODE, true>(prm, threads, cps, smem, st);
-  }
-  switch (lpp) {
-    case 4: return launch_align<4, MODE>(prm, threads, cps, smem, st);
-    case 8: return launch_align<8, MODE>(prm, threads, cps, smem, st);
-    case 16: return launch_align<16, MODE>(prm, threads, cps, smem, st);
-    case 32: return launch_align<32, MODE>(prm, threads, cps, smem, st);
-    default: return set_error(FSS_ERR_INVALID, "fss_align: lanes_per_pose must be 4, 8, 16 or 32");
-  }
-}
-
 // Default tiling (the Python autotuner overrides it with measured choices): lanes per pose
 // so that each lane owns about 8 fit points -- enough pairwise work per lane to amortise
 // the per-step group reduction and Adam tail -- and start blocks that waste the fewest pose
@@ -377,6 +175,12 @@ int align_launch(const fss_align_desc* d, cudaStream_t st) {
   const bool tc = d->accumulate == 2;
   if (tc && d->lanes_per_pose != 0 && d->lanes_per_pose != 32)
     return set_error(FSS_ERR_INVALID, "fss_align: tensor-core sums use 32 lanes per pose");
+  if (d->kernel_variant < 0 || d->kernel_variant > 3 || (!tc_mode && d->kernel_variant > 1))
+    return set_error(FSS_ERR_INVALID, "fss_align: kernel_variant must be 0..3 (0 or 1 for "
+                                      "modes with a pharmacophore channel)");
+  // automatic code variant: wide register tile for large clouds, roomy registers for small
+  const int var = d->kernel_variant > 0 ? d->kernel_variant - 1
+                  : !tc_mode ? 0 : (maxM >= 64 ? 1 : 2);
   int lpp = tc ? 32 : d->lanes_per_pose, chunks = d->chunks;
   auto_tile(d->mode, shape ? maxM : maxMp, d->n_starts, &lpp, &chunks);
   if (chunks < 1 || chunks > d->n_starts)
@@ -422,11 +226,9 @@ int align_launch(const fss_align_desc* d, cudaStream_t st) {
                sizeof(float2) * (d->mode == FSS_MODE_ESP ? (size_t)maxN : 0) + 16;
   int rc;
   switch (d->mode) {
-    case FSS_MODE_SHAPE: rc = dispatch_lpp<FSS_MODE_SHAPE>(lpp, tc, p, threads, d->cta_per_sm, smem, st); break;
-    case FSS_MODE_ESP: rc = dispatch_lpp<FSS_MODE_ESP>(lpp, tc, p, threads, d->cta_per_sm, smem, st); break;
-    case FSS_MODE_PHARM: rc = dispatch_lpp<FSS_MODE_PHARM>(lpp, tc, p, threads, d->cta_per_sm, smem, st); break;
-    case FSS_MODE_SHAPE_PHARM: rc = dispatch_lpp<FSS_MODE_SHAPE_PHARM>(lpp, tc, p, threads, d->cta_per_sm, smem, st); break;
-    default: rc = dispatch_lpp<FSS_MODE_SHAPE_COLOR>(lpp, tc, p, threads, d->cta_per_sm, smem, st); break;
+    case FSS_MODE_SHAPE: rc = launch_align_shape(lpp, tc, var, p, threads, d->cta_per_sm, smem, st); break;
+    case FSS_MODE_ESP: rc = launch_align_esp(lpp, tc, var, p, threads, d->cta_per_sm, smem, st); break;
+    default: rc = launch_align_pharm(d->mode, lpp, p, threads, d->cta_per_sm, smem, st); break;
   }
   if (rc != FSS_OK) return rc;
   if (d->out_score && d->out_q && d->out_t)

@@ -258,17 +258,6 @@ __device__ __forceinline__ void step_combo(PoseState& s, const Reduced& ms, floa
 // ---------------------------------------------------------------------------------------
 constexpr float kFactorMax = 96.f;
 
-// Register tile of the hot loop: FSS_JB2 float2 pairs (2*FSS_JB2 fit points) per lane per
-// pass, and the unroll depth of the loop over reference points.
-#ifndef FSS_JB2
-#define FSS_JB2 2
-#endif
-#ifndef FSS_UNROLL
-#define FSS_UNROLL 2
-#endif
-constexpr int kFitTile2 = FSS_JB2;
-constexpr int kRefUnroll = FSS_UNROLL;
-
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
 template <int JB, bool ESP>
@@ -323,7 +312,7 @@ __device__ __forceinline__ void shape_chunk_plain(const float4* __restrict__ sPd
 
 // Packed chunk: JB2 float2 pairs = 2*JB2 fit points per lane, f32x2 arithmetic, factored
 // exponent.  Returns false (and does nothing) when the factored form could overflow.
-template <int JB2, bool ESP>
+template <int JB2, bool ESP, int UNR>
 __device__ __forceinline__ bool shape_chunk_packed(const float4* __restrict__ sPd,
                                                    const float2* __restrict__ sQd,
                                                    const float4* __restrict__ sB, int N, int M,
@@ -351,7 +340,7 @@ __device__ __forceinline__ bool shape_chunk_packed(const float4* __restrict__ sP
     sg[v] = f2(0.f, 0.f); sx[v] = f2(0.f, 0.f); sy[v] = f2(0.f, 0.f); sz[v] = f2(0.f, 0.f);
   }
   if (__any_sync(0xffffffffu, big)) return false;
-#pragma unroll kRefUnroll
+#pragma unroll UNR
   for (int i = 0; i < N; ++i) {
     const float4 a = sPd[2 * i], c = sPd[2 * i + 1];
     const float2 PX = f2(a.x, a.y), PY = f2(a.z, a.w), PZ = f2(c.x, c.y), PW = f2(c.z, c.w);
@@ -393,43 +382,48 @@ __device__ __forceinline__ bool shape_chunk_packed(const float4* __restrict__ sP
   return true;
 }
 
-template <int JB2, bool ESP>
+template <int JB2, bool ESP, int UNR>
 __device__ __forceinline__ void shape_chunk(const float4* __restrict__ sPd,
                                             const float2* __restrict__ sQd,
                                             const float4* __restrict__ sB, int N, int M, int j0,
                                             int stride, const Rot& R, float tx, float ty,
                                             float tz, float k, float e, float inv2k,
                                             Moments& acc) {
-  if (!shape_chunk_packed<JB2, ESP>(sPd, sQd, sB, N, M, j0, stride, R, tx, ty, tz, k, e, inv2k,
+  if (!shape_chunk_packed<JB2, ESP, UNR>(sPd, sQd, sB, N, M, j0, stride, R, tx, ty, tz, k, e, inv2k,
                                     acc))
     shape_chunk_plain<2 * JB2, ESP>(sPd, sQd, sB, N, M, j0, stride, R, tx, ty, tz, k, e, inv2k,
                                     acc);
 }
 
-template <int LPP, bool ESP>
+// JB2: float2 pairs of fit points per lane per pass (register tile, 2*JB2 points);
+// UNR: unroll depth of the loop over reference points.
+template <int LPP, bool ESP, int JB2 = 2, int UNR = 2>
 __device__ __forceinline__ void shape_pose(const float4* __restrict__ sPd,
                                            const float2* __restrict__ sQd,
                                            const float4* __restrict__ sB, int N, int M, int lane,
                                            const Rot& R, float tx, float ty, float tz, float k,
                                            float e, float inv2k, Moments& acc) {
-  constexpr int JB2 = kFitTile2;
+  static_assert(JB2 >= 1 && JB2 <= 4, "register tile of 2..8 fit points");
   // Trip counts depend only on M and LPP, so every lane of the group (and every group of
   // the warp, which share one pair) runs the same loop; points past M are masked.
   int base = 0;
   for (; base + 2 * JB2 * LPP <= M; base += 2 * JB2 * LPP)
-    shape_chunk<JB2, ESP>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k, acc);
+    shape_chunk<JB2, ESP, UNR>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k,
+                               acc);
   // 0..2*JB2 points are left for the group's lane 0: finish with the smallest tile
   const int pairs = ((M - base + LPP - 1) / LPP + 1) / 2;
   if (JB2 >= 4 && pairs == 4) {
-    shape_chunk<(JB2 >= 4 ? 4 : 1), ESP>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty, tz, k,
-                                         e, inv2k, acc);
+    shape_chunk<(JB2 >= 4 ? 4 : 1), ESP, UNR>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty,
+                                              tz, k, e, inv2k, acc);
   } else if (JB2 >= 3 && pairs == 3) {
-    shape_chunk<(JB2 >= 3 ? 3 : 1), ESP>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty, tz, k,
-                                         e, inv2k, acc);
+    shape_chunk<(JB2 >= 3 ? 3 : 1), ESP, UNR>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty,
+                                              tz, k, e, inv2k, acc);
   } else if (pairs == 2) {
-    shape_chunk<2, ESP>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k, acc);
+    shape_chunk<2, ESP, UNR>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k,
+                             acc);
   } else if (pairs == 1) {
-    shape_chunk<1, ESP>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k, acc);
+    shape_chunk<1, ESP, UNR>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k,
+                             acc);
   }
 }
 

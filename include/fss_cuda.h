@@ -152,6 +152,10 @@ typedef struct fss_align_desc {
   int32_t accumulate;        /* where the value/gradient sums of the shape and ESP channels
                               * run: 0 automatic, 1 FP32 lanes, 2 tensor cores (tf32 hi/lo
                               * split MMA, one warp per pose; modes SHAPE and ESP) */
+  int32_t kernel_variant;    /* code variant of the FP32-lane loop: 0 automatic, 1 base (4 fit
+                              * points per lane, 2 CTAs/SM register budget), 2 wide (6 fit
+                              * points per lane, deeper unroll), 3 roomy (4 fit points, one
+                              * CTA/SM register budget); 2 and 3 for modes SHAPE and ESP */
   /* scratch: two device int32 -- [0] work counter, [1] status flags (bit 0: a pair was
    * larger than the max_* extents).  The launch zeroes both on `stream`. */
   int32_t *scratch;

@@ -172,6 +172,41 @@ def test_tiling_does_not_change_results(golden, cuda, lpp):
     np.testing.assert_allclose(got, base, rtol=0, atol=5e-5)
 
 
+@pytest.mark.parametrize("mode", ["shape", "esp"])
+@pytest.mark.parametrize("variant", [2, 3])
+def test_code_variants_agree(golden, cuda, mode, variant):
+    """The wide-tile and one-CTA/SM code variants give the base variant's rows after a few
+    steps (to fp32 summation order) on every lanes-per-pose tiling."""
+    g = golden["align"]
+    tag = "shape" if mode == "shape" else "esp"
+    C = (lambda k: _t(g[k], cuda)) if mode == "esp" else (lambda k: None)
+    ref = CloudSet.from_padded(_t(g[f"{tag}_A"], cuda), _t(g[f"{tag}_N"], cuda), C(f"{tag}_CA"))
+    fit = CloudSet.from_padded(_t(g[f"{tag}_B"], cuda), _t(g[f"{tag}_M"], cuda), C(f"{tag}_CB"))
+    idx = torch.arange(len(g[f"{tag}_N"]), dtype=torch.int32, device=cuda)
+    kw = dict(ref=ref, fit=fit, pair_ref=idx, pair_fit=idx,
+              seed_q=_t(g[f"{tag}_seeds_q"], cuda), seed_t=_t(g[f"{tag}_seeds_t"], cuda),
+              steps=3, lr=0.1, lam=float(g["esp_lam"]) if mode == "esp" else None)
+    for lpp in (4, 16, 32):
+        base = al.align_packed(mode, lanes_per_pose=lpp, kernel_variant=1, **kw).rows[0]
+        got = al.align_packed(mode, lanes_per_pose=lpp, kernel_variant=variant, **kw).rows[0]
+        np.testing.assert_allclose(got.cpu().numpy(), base.cpu().numpy(), rtol=0, atol=5e-5)
+
+
+def test_variant_rejected_for_pharm_modes(cuda):
+    refs, fits = syn.shape_pharm_pairs(2, seed=3)
+    ref_ph = PharmSet.from_arrays([m["pharm_types"] for m in refs], [m["pharm_ancs"] for m in refs],
+                                  [m["pharm_vecs"] for m in refs], device=cuda)
+    fit_ph = PharmSet.from_arrays([m["pharm_types"] for m in fits], [m["pharm_ancs"] for m in fits],
+                                  [m["pharm_vecs"] for m in fits], device=cuda)
+    idx = torch.arange(2, dtype=torch.int32, device=cuda)
+    sq = torch.zeros(2, 4, 4, device=cuda)
+    sq[..., 0] = 1
+    st = torch.zeros(2, 4, 3, device=cuda)
+    with pytest.raises((ValueError, RuntimeError)):
+        al.align_packed("pharm", ref_ph=ref_ph, fit_ph=fit_ph, pair_ref=idx, pair_fit=idx,
+                        seed_q=sq, seed_t=st, steps=1, lr=0.1, kernel_variant=2)
+
+
 def test_edge_sizes_and_degenerate_pairs(cuda):
     """Tiny and empty clouds, tile remainders (M = 1..33), and pairs below 3 points."""
     rng = np.random.default_rng(5)
