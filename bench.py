@@ -160,6 +160,12 @@ def flush_l2(buf):
     buf.add_(1.0)   # 256 MB read+write: evicts the 126 MB L2
 
 
+# DRAM bytes (read + write) per pair of one fused-kernel launch, from an ncu capture of the
+# same workload at 256 pairs (dram__bytes_read.sum + dram__bytes_write.sum = 4.14 MB +
+# 0.23 MB), scaled by pairs; the kernel's traffic grows with the pairs it processes.
+DRAM_BYTES_PER_PAIR = {"surf_esp": (4.14336e6 + 2.3424e5) / 256}
+
+
 def run_cuda(args, wl):
     import torch
     import torch.distributed as dist
@@ -301,7 +307,11 @@ def run_cuda(args, wl):
         "gpu_launches": launches_per_step * args.steps,
         "roofline": {"bound": "mufu", "achieved": round(achieved / 1e9, 1),
                      "peak": round(roof / 1e9, 1), "unit": "Gterm/s",
-                     "frac": round(achieved / roof, 4), "traffic": None,
+                     "frac": round(achieved / roof, 4),
+                     "traffic": (round(DRAM_BYTES_PER_PAIR[mode] * n_pairs)
+                                 if mode in DRAM_BYTES_PER_PAIR else None),
+                     "traffic_source": "bytes per launch: ncu dram__bytes_read+write of the "
+                                       "256-pair case, scaled by pairs",
                      "peak_source": "measured by fss_probe_peak on this GPU: "
                                     f"ex2 {peak['ex2'] / 1e9:.0f} G/s, ffma "
                                     f"{peak['ffma'] / 1e9:.0f} G/s /{per_term_fp32} per term",

@@ -41,7 +41,8 @@ class AlignDesc(ctypes.Structure):
         ("max_ref_points", _i32), ("max_fit_points", _i32),
         ("max_ref_features", _i32), ("max_fit_features", _i32),
         ("lanes_per_pose", _i32), ("chunks", _i32), ("cta_per_sm", _i32),
-        ("accumulate", _i32), ("kernel_variant", _i32),
+        ("accumulate", _i32), ("kernel_variant", _i32), ("pharm_extended", _i32),
+        ("similarity", _i32), ("tversky_sigma", _f32),
         ("scratch", _vp),
     ]
 
@@ -54,7 +55,7 @@ _SIGS = {
     "fss_pharm_grad": ([_vp] * 10 + [_i32] * 5 + [_vp] * 4, ctypes.c_int),
     "fss_tanimoto_adam_step": ([_vp] * 13 + [_i32, _f32, _vp], ctypes.c_int),
     "fss_self_overlap": ([_vp, _vp, _i32, _i32, _f32, _i32, _f32, _vp, _vp], ctypes.c_int),
-    "fss_pharm_self_overlap": ([_vp, _vp, _vp, _i32, _i32, _i32, _vp, _vp], ctypes.c_int),
+    "fss_pharm_self_overlap": ([_vp, _vp, _vp, _i32, _i32, _i32, _i32, _vp, _vp], ctypes.c_int),
     "fss_seeds": ([_vp] * 6 + [_i32, _i32, _vp, _i32, _vp, _vp, _vp], ctypes.c_int),
     "fss_align": ([ctypes.POINTER(AlignDesc), _vp], ctypes.c_int),
     "fss_align_static": ([ctypes.POINTER(AlignDesc), _vp], ctypes.c_int),

@@ -35,6 +35,8 @@ from ._lib import AlignDesc, check, ptr, stream_ptr
 from .layout import CloudSet, PharmSet, cost_order
 
 _f32, _i32 = torch.float32, torch.int32
+# Tversky weights of the reference (accel/drivers/pharm.py:40)
+TVERSKY_SIGMA = {"tversky": 0.95, "tversky_ref": 1.0, "tversky_fit": 0.05}
 LAM_SCALING = (1e4 / (4 * 55.263 * math.pi)) ** 2   # score/constants.py:16-17
 
 MODE_IDS = {"shape": _lib.MODE_SHAPE, "esp": _lib.MODE_ESP, "pharm": _lib.MODE_PHARM,
@@ -65,8 +67,8 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
                  alpha: float = 0.81, lam: Optional[float] = None, color_weight: float = 0.5,
                  ref_self=None, fit_self=None, ref_self_ph=None, fit_self_ph=None,
                  order=None, lanes_per_pose: int = 0, chunks: int = 0, cta_per_sm: int = 0,
-                 accumulate: int = 0, kernel_variant: int = 0, rows=None, out=None,
-                 scratch=None,
+                 accumulate: int = 0, kernel_variant: int = 0, similarity: str = "tanimoto",
+                 pharm_extended: int = 0, rows=None, out=None, scratch=None,
                  check_status: bool = True, validate: bool = True):
     """Run the fused alignment kernel over packed clouds.
 
@@ -77,7 +79,9 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
     ``accumulate`` picks where the shape/ESP sums run: 0 automatic (autotuned), 1 FP32 lanes,
     2 tensor cores (modes "shape" and "esp", 32 lanes per pose).  ``kernel_variant`` picks the
     FP32-lane loop's code variant: 0 automatic, 1 base, 2 wide register tile, 3 one-CTA/SM
-    register budget (2 and 3 for "shape" and "esp").
+    register budget (2 and 3 for "shape" and "esp").  Mode "pharm" only: ``similarity`` in
+    ("tanimoto", "tversky", "tversky_ref", "tversky_fit") and ``pharm_extended`` 0 (cosine
+    weights), 1 (extended points and anchors), 2 (extended points only).
     ``validate=False`` skips the pair-index range check (a device read-back) for callers that
     validated their indices on the host; ``check_status=False`` skips reading the kernel's
     status word (both keep the launch free of host synchronisation).
@@ -94,6 +98,14 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
         raise ValueError(f"mode {mode!r} needs ref and fit pharmacophores")
     if m == _lib.MODE_ESP and lam is None:
         raise ValueError("esp mode needs lam")
+    similarity = similarity.lower()
+    if similarity != "tanimoto" and similarity not in TVERSKY_SIGMA:
+        raise ValueError("similarity must be one of ('tanimoto','tversky','tversky_ref',"
+                         "'tversky_fit')")
+    if (similarity != "tanimoto" or pharm_extended) and m != _lib.MODE_PHARM:
+        raise ValueError("Tversky similarity and extended points apply to mode 'pharm' only")
+    if pharm_extended not in (0, 1, 2):
+        raise ValueError("pharm_extended must be 0, 1 or 2")
     pair_ref = torch.as_tensor(pair_ref, device=dev).to(_i32).contiguous()
     pair_fit = torch.as_tensor(pair_fit, device=dev).to(_i32).contiguous()
     seed_q = seed_q.to(_f32).contiguous()
@@ -117,9 +129,9 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
     if pharm:
         if m == _lib.MODE_PHARM:
             if ref_self is None:
-                ref_self = kernels.pharm_self_overlap(ref_ph, directional)
+                ref_self = kernels.pharm_self_overlap(ref_ph, directional, pharm_extended)
             if fit_self is None:
-                fit_self = kernels.pharm_self_overlap(fit_ph, directional)
+                fit_self = kernels.pharm_self_overlap(fit_ph, directional, pharm_extended)
         else:
             if ref_self_ph is None:
                 ref_self_ph = kernels.pharm_self_overlap(ref_ph, directional)
@@ -181,6 +193,9 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
     d.lanes_per_pose, d.chunks, d.cta_per_sm = int(lanes_per_pose), int(chunks), int(cta_per_sm)
     d.accumulate = int(accumulate)
     d.kernel_variant = int(kernel_variant)
+    d.pharm_extended = int(pharm_extended)
+    if similarity != "tanimoto":
+        d.similarity, d.tversky_sigma = 1, TVERSKY_SIGMA[similarity]
     d.scratch = ptr(scratch, _i32)
     check(_lib.load().fss_align(d, stream_ptr(dev)), f"align[{mode}]")
     if check_status:
@@ -300,6 +315,12 @@ def _quat_rot(q):
                        -1).reshape(q.shape[:-1] + (3, 3))
 
 
+def extended_code(extended_points: bool, only_extended: bool) -> int:
+    """fss_align_desc.pharm_extended for the reference's flags (only_extended matters only
+    with extended_points, analytical_gradients/_torch.py:288-297)."""
+    return 0 if not extended_points else (2 if only_extended else 1)
+
+
 def coarse_fine_pharm_align_many(anchors_1, anchors_2, vectors_1, vectors_2, types_1, types_2,
                                  VAA=None, VBB=None, *, similarity: str = "tanimoto",
                                  extended_points: bool = False, only_extended: bool = False,
@@ -309,15 +330,14 @@ def coarse_fine_pharm_align_many(anchors_1, anchors_2, vectors_1, vectors_2, typ
                                  N_real=None, M_real=None, early_stop_patience: int = 5,
                                  early_stop_tol: float = 1e-5, seeds: Optional[tuple] = None,
                                  **tile):
-    """Batched directional pharmacophore alignment (Tanimoto).
+    """Batched directional pharmacophore alignment (Tanimoto or Tversky, optionally with
+    extended points).
 
     Clouds are centred on their own centroids first and the translation folded back at the
     end, as the reference does (pharm.py:205-225, :509-517).  ``seeds`` (if given) are for
-    the centred clouds.  VAA/VBB are recomputed by the kernel, as in the reference kernel path.
+    the centred clouds.  VAA/VBB are recomputed by the kernel with the same extended-point
+    convention as the cross overlap, as in the reference (pharm.py:732-748).
     """
-    if similarity != "tanimoto" or extended_points or only_extended:
-        raise NotImplementedError("the CUDA pharm path implements similarity='tanimoto' "
-                                  "without extended points")
     if trans_centers is not None:
         raise NotImplementedError("trans_init is not part of the CUDA backend")
     K, npad, _ = anchors_1.shape
@@ -337,7 +357,9 @@ def coarse_fine_pharm_align_many(anchors_1, anchors_2, vectors_1, vectors_2, typ
         seeds = kernels.seeds(CloudSet.from_padded(a1c, N_real),
                               CloudSet.from_padded(a2c, M_real), pr, pf, num_seeds)
     sc, q, t = align_packed("pharm", ref_ph=ref_ph, fit_ph=fit_ph, pair_ref=pr, pair_fit=pf,
-                            seed_q=seeds[0], seed_t=seeds[1], steps=steps_fine, lr=lr, **tile)
+                            seed_q=seeds[0], seed_t=seeds[1], steps=steps_fine, lr=lr,
+                            similarity=similarity,
+                            pharm_extended=extended_code(extended_points, only_extended), **tile)
     R = _quat_rot(q)
     t = t - torch.einsum('bij,bj->bi', R, c_fit) + c_ref
     return sc, q, t

@@ -226,15 +226,13 @@ def _align_batch_pharm(pairs, *, similarity: str = "tanimoto", extended_points: 
     """Directional pharmacophore alignment; writes transform_pharm / sim_aligned_pharm."""
     if not pairs:
         return
-    if similarity != "tanimoto" or extended_points or only_extended:
-        raise NotImplementedError("the CUDA pharm path implements similarity='tanimoto' "
-                                  "without extended points")
     if trans_init:
         raise NotImplementedError("trans_init=True is not part of the CUDA backend")
     dev = _device_of(pairs)
     rp, fp, ri, fi = _pharm_inputs(pairs, dev)
     return _align(pairs, "pharm", None, None, rp, fp, ri, fi, steps=steps_fine, lr=lr,
-                  num_seeds=num_repeats or seeds_for("pharm"))
+                  num_seeds=num_repeats or seeds_for("pharm"), similarity=similarity,
+                  extended_points=extended_points, only_extended=only_extended)
 
 
 def _align_batch_vol_color(pairs, *, alpha: float = 0.81, color_weight: float = 0.5,

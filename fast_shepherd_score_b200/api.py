@@ -181,8 +181,11 @@ def align_device(mode, ref: Optional[CloudSet], fit: Optional[CloudSet],
                  ref_ph: Optional[PharmSet], fit_ph: Optional[PharmSet], pair_ref, pair_fit,
                  *, alpha=0.81, lam=0.3, color_weight=0.5, num_seeds=50, steps=200, lr=0.1,
                  seeds=None, ref_self=None, fit_self=None, ref_self_ph=None, fit_self_ph=None,
-                 **tile):
-    """Device-resident form of :func:`align_host` (all tensors already on the GPU)."""
+                 similarity="tanimoto", extended_points=False, only_extended=False, **tile):
+    """Device-resident form of :func:`align_host` (all tensors already on the GPU).
+    ``similarity`` / ``extended_points`` / ``only_extended`` apply to mode "pharm"."""
+    if mode != "pharm" and (similarity != "tanimoto" or extended_points or only_extended):
+        raise ValueError("similarity and extended points apply to mode 'pharm' only")
     if mode in SHAPE_MODES:
         esp = mode in ("vol_esp", "surf_esp")
         kl = _kernel_lam(mode, lam) if esp else None
@@ -201,7 +204,10 @@ def align_device(mode, ref: Optional[CloudSet], fit: Optional[CloudSet],
             seeds = K.seeds(_as_cloud(rph), _as_cloud(fph), pair_ref, pair_fit, num_seeds)
         res = al.align_packed("pharm", ref_ph=rph, fit_ph=fph, pair_ref=pair_ref,
                               pair_fit=pair_fit, seed_q=seeds[0], seed_t=seeds[1],
-                              steps=steps, lr=lr, ref_self=ref_self, fit_self=fit_self, **tile)
+                              steps=steps, lr=lr, ref_self=ref_self, fit_self=fit_self,
+                              similarity=similarity,
+                              pharm_extended=al.extended_code(extended_points, only_extended),
+                              **tile)
         sc, q, t = res
         cr = c_ref[pair_ref.long()]
         cf = c_fit[pair_fit.long()]

@@ -60,6 +60,7 @@ __global__ void self_overlap_kernel(const float4* __restrict__ pts, const int* _
   if (threadIdx.x == 0) out[m] = acc.v * Kc;
 }
 
+template <int EXT>
 __global__ void pharm_self_kernel(const float4* __restrict__ anc, const float4* __restrict__ vec,
                                   const int* __restrict__ off, int n_mol, int max_n,
                                   PharmTables tab, float* out) {
@@ -84,7 +85,7 @@ __global__ void pharm_self_kernel(const float4* __restrict__ anc, const float4* 
   for (int i = 0; i < 9; ++i) R.r[i] = (i % 4 == 0) ? 1.f : 0.f;
   Moments acc;
   acc.zero();
-  pharm_pose<32>(sRA, sRV, sFA, sFV, n, n, threadIdx.x, R, -c.x, -c.y, -c.z, tab, acc);
+  pharm_pose<32, EXT>(sRA, sRV, sFA, sFV, n, n, threadIdx.x, R, -c.x, -c.y, -c.z, tab, acc);
   acc.group_sum<32>();
   if (threadIdx.x == 0) out[m] = acc.v;
 }
@@ -173,6 +174,13 @@ int align_launch(const fss_align_desc* d, cudaStream_t st) {
   if (d->accumulate == 2 && !tc_mode)
     return set_error(FSS_ERR_INVALID, "fss_align: tensor-core sums need mode SHAPE or ESP");
   const bool tc = d->accumulate == 2;
+  if (d->pharm_extended < 0 || d->pharm_extended > 2 ||
+      (d->pharm_extended != 0 && d->mode != FSS_MODE_PHARM))
+    return set_error(FSS_ERR_INVALID, "fss_align: pharm_extended must be 0, 1 or 2 (mode PHARM)");
+  if (d->similarity < 0 || d->similarity > 1 || (d->similarity && d->mode != FSS_MODE_PHARM) ||
+      (d->similarity && !(d->tversky_sigma >= 0.f && d->tversky_sigma <= 1.f)))
+    return set_error(FSS_ERR_INVALID, "fss_align: similarity must be 0 (Tanimoto) or 1 (Tversky, "
+                                      "mode PHARM, tversky_sigma in [0, 1])");
   if (tc && d->lanes_per_pose != 0 && d->lanes_per_pose != 32)
     return set_error(FSS_ERR_INVALID, "fss_align: tensor-core sums use 32 lanes per pose");
   if (d->kernel_variant < 0 || d->kernel_variant > 3 || (!tc_mode && d->kernel_variant > 1))
@@ -214,6 +222,7 @@ int align_launch(const fss_align_desc* d, cudaStream_t st) {
   p.Kc = (float)(std::pow(M_PI, 1.5) / std::pow(2.0 * alpha, 1.5));
   p.aKc = (float)(alpha * std::pow(M_PI, 1.5) / std::pow(2.0 * alpha, 1.5));
   p.w = d->color_weight; p.lr = d->lr;
+  p.sigma = d->similarity == 1 ? d->tversky_sigma : -1.f;
   p.tab = make_pharm_tables(d->mode != FSS_MODE_SHAPE_COLOR);
   p.row_score = d->row_score; p.row_q = d->row_q; p.row_t = d->row_t;
   p.counter = d->scratch;
@@ -228,7 +237,10 @@ int align_launch(const fss_align_desc* d, cudaStream_t st) {
   switch (d->mode) {
     case FSS_MODE_SHAPE: rc = launch_align_shape(lpp, tc, var, p, threads, d->cta_per_sm, smem, st); break;
     case FSS_MODE_ESP: rc = launch_align_esp(lpp, tc, var, p, threads, d->cta_per_sm, smem, st); break;
-    default: rc = launch_align_pharm(d->mode, lpp, p, threads, d->cta_per_sm, smem, st); break;
+    default:
+      rc = launch_align_pharm(d->mode, lpp, d->pharm_extended, p, threads, d->cta_per_sm, smem,
+                              st);
+      break;
   }
   if (rc != FSS_OK) return rc;
   if (d->out_score && d->out_q && d->out_t)
@@ -273,17 +285,22 @@ int self_overlap_launch(const float* pts, const int32_t* off, int n_mol, int max
 }
 
 int pharm_self_launch(const float* anc, const float* vec, const int32_t* off, int n_mol, int max_n,
-                      int directional, float* out, cudaStream_t st) {
+                      int directional, int extended, float* out, cudaStream_t st) {
   if (n_mol < 0 || !anc || !off || !out || (directional && !vec))
     return set_error(FSS_ERR_INVALID, "fss_pharm_self_overlap: bad arguments");
+  if (extended < 0 || extended > 2 || (extended && !directional))
+    return set_error(FSS_ERR_INVALID, "fss_pharm_self_overlap: extended must be 0, 1 or 2 "
+                                      "(directional tables)");
   if (max_n > kMaxPoints) return set_error(FSS_ERR_UNSUPPORTED, "fss_pharm_self_overlap: molecule too large");
   if (n_mol == 0) return FSS_OK;
   const size_t smem = sizeof(float4) * 4 * (size_t)max_n + 16;
-  cudaError_t ce = cudaFuncSetAttribute(pharm_self_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  auto kern = extended == 1 ? pharm_self_kernel<1>
+              : extended == 2 ? pharm_self_kernel<2> : pharm_self_kernel<0>;
+  cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (ce != cudaSuccess) return set_error(FSS_ERR_CUDA, std::string("fss_pharm_self_overlap: ") + cudaGetErrorString(ce));
-  pharm_self_kernel<<<n_mol, 32, smem, st>>>(reinterpret_cast<const float4*>(anc),
-                                             reinterpret_cast<const float4*>(vec), off, n_mol, max_n,
-                                             make_pharm_tables(directional != 0), out);
+  kern<<<n_mol, 32, smem, st>>>(reinterpret_cast<const float4*>(anc),
+                                reinterpret_cast<const float4*>(vec), off, n_mol, max_n,
+                                make_pharm_tables(directional != 0), out);
   return check_launch("fss_pharm_self_overlap");
 }
 

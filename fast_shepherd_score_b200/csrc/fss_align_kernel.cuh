@@ -34,6 +34,7 @@ struct AlignParams {
   const float* ref_self_ph; const float* fit_self_ph;
   const float* seed_q; const float* seed_t;
   float alpha, k, e, inv2k, Kc, aKc, w, lr;
+  float sigma;  // pharm mode: Tversky sigma (>= 0) or Tanimoto (< 0)
   PharmTables tab;
   float* row_score; float* row_q; float* row_t;
   int* counter;
@@ -57,8 +58,8 @@ template <>
 struct AlignVariant<2> { static constexpr int kJB2 = 2, kUnroll = 4, kMinCtas = 1; };
 
 // TC: shape/ESP sums on the tensor cores (fss_mma.cuh); requires LPP == 32 and a mode
-// without a pharmacophore channel.
-template <int LPP, int MODE, bool TC, int VAR>
+// without a pharmacophore channel.  EXT: extended pharmacophore points (pharm_pose).
+template <int LPP, int MODE, bool TC, int VAR, int EXT = 0>
 __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
     align_kernel(const AlignParams p) {
   using V = AlignVariant<VAR>;
@@ -132,6 +133,7 @@ __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
     __syncthreads();
 
     const float Us = p.ref_self[ri] + p.fit_self[fi];
+    const float Dtv = p.sigma * p.ref_self[ri] + (1.f - p.sigma) * p.fit_self[fi];
     const float Uc = kShape && kPharm ? p.ref_self_ph[ri] + p.fit_self_ph[fi] : 0.f;
     const int start = chunk * ppc + grp;
     const int warp_first = chunk * ppc + (tid >> 5) * kGroupsPerWarp;
@@ -167,12 +169,13 @@ __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
         if (kPharm) {
           Moments mc;
           mc.zero();
-          pharm_pose<LPP>(sRA, sRV, sFA, sFV, Np, Mp, lane, R, s.t[0], s.t[1], s.t[2], p.tab,
+          pharm_pose<LPP, EXT>(sRA, sRV, sFA, sFV, Np, Mp, lane, R, s.t[0], s.t[1], s.t[2], p.tab,
                           mc);
           Reduced rc;
           rc.from(mc, s.q);
           rc.template group_sum<LPP>();
           if (kShape) step_combo(s, rs, Us, rc, Uc, p.w, p.lr);
+          else if (p.sigma >= 0.f) step_tversky(s, rc, Dtv, p.lr);
           else step_single(s, rc, Us, p.lr);
         } else {
           step_single(s, rs, Us, p.lr);
@@ -192,10 +195,10 @@ __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
   }
 }
 
-template <int LPP, int MODE, bool TC, int VAR>
+template <int LPP, int MODE, bool TC, int VAR, int EXT = 0>
 int launch_align(const AlignParams& prm, int threads, int cta_per_sm, size_t smem,
                  cudaStream_t st) {
-  auto kern = align_kernel<LPP, MODE, TC, VAR>;
+  auto kern = align_kernel<LPP, MODE, TC, VAR, EXT>;
   cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)smem);
   if (ce != cudaSuccess)
@@ -211,14 +214,14 @@ int launch_align(const AlignParams& prm, int threads, int cta_per_sm, size_t sme
   return check_launch("fss_align");
 }
 
-template <int MODE, int VAR>
+template <int MODE, int VAR, int EXT = 0>
 int dispatch_lanes(int lpp, const AlignParams& prm, int threads, int cps, size_t smem,
                    cudaStream_t st) {
   switch (lpp) {
-    case 4: return launch_align<4, MODE, false, VAR>(prm, threads, cps, smem, st);
-    case 8: return launch_align<8, MODE, false, VAR>(prm, threads, cps, smem, st);
-    case 16: return launch_align<16, MODE, false, VAR>(prm, threads, cps, smem, st);
-    case 32: return launch_align<32, MODE, false, VAR>(prm, threads, cps, smem, st);
+    case 4: return launch_align<4, MODE, false, VAR, EXT>(prm, threads, cps, smem, st);
+    case 8: return launch_align<8, MODE, false, VAR, EXT>(prm, threads, cps, smem, st);
+    case 16: return launch_align<16, MODE, false, VAR, EXT>(prm, threads, cps, smem, st);
+    case 32: return launch_align<32, MODE, false, VAR, EXT>(prm, threads, cps, smem, st);
     default: return set_error(FSS_ERR_INVALID, "fss_align: lanes_per_pose must be 4, 8, 16 or 32");
   }
 }
@@ -229,7 +232,7 @@ int launch_align_shape(int lpp, bool tc, int var, const AlignParams& prm, int th
                        size_t smem, cudaStream_t st);
 int launch_align_esp(int lpp, bool tc, int var, const AlignParams& prm, int threads, int cps,
                      size_t smem, cudaStream_t st);
-int launch_align_pharm(int mode, int lpp, const AlignParams& prm, int threads, int cps,
-                       size_t smem, cudaStream_t st);
+int launch_align_pharm(int mode, int lpp, int ext, const AlignParams& prm, int threads,
+                       int cps, size_t smem, cudaStream_t st);
 
 }  // namespace fss

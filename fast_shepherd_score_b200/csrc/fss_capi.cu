@@ -122,10 +122,10 @@ int fss_self_overlap(const float* pts, const int32_t* off, int32_t n_mol, int32_
 }
 
 int fss_pharm_self_overlap(const float* anc, const float* vec, const int32_t* off,
-                           int32_t n_mol, int32_t max_features, int32_t directional, float* out,
-                           void* stream) {
-  FSS_GUARD(fss::pharm_self_launch(anc, vec, off, n_mol, max_features, directional, out,
-                                   S(stream)));
+                           int32_t n_mol, int32_t max_features, int32_t directional,
+                           int32_t extended, float* out, void* stream) {
+  FSS_GUARD(fss::pharm_self_launch(anc, vec, off, n_mol, max_features, directional, extended,
+                                   out, S(stream)));
 }
 
 int fss_seeds(const float* ref_pts, const int32_t* ref_off, const float* fit_pts,

@@ -220,6 +220,20 @@ __device__ __forceinline__ void step_single(PoseState& s, const Reduced& m, floa
   adam_tail(s, score, gq, gt, lr);
 }
 
+// Tversky step (accel/drivers/pharm_overlap.py:36-59, analytical_gradients/_torch.py:416-436):
+// score = min(V / D, 1) with D = sigma V_AA + (1 - sigma) V_BB (0 when D <= 1e-8); the
+// gradient is V'/D while V < D and 0 once the score is clamped.
+__device__ __forceinline__ void step_tversky(PoseState& s, const Reduced& m, float D, float lr) {
+  const float score = D > 1e-8f ? fminf(m.v / D, 1.f) : 0.f;
+  const float scale = m.v < D ? 1.f / D : 0.f;
+  float gq[4], gt[3];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) gq[i] = -scale * m.dq[i];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) gt[i] = -scale * m.f[i];
+  adam_tail(s, score, gq, gt, lr);
+}
+
 // Two-channel step (1-w) * shape + w * pharm, the joint gradient of cpu_fused.py:111-167.
 __device__ __forceinline__ void step_combo(PoseState& s, const Reduced& ms, float Us,
                                            const Reduced& mc, float Uc, float w, float lr) {
@@ -439,7 +453,13 @@ struct PharmTables {
   int cat[9];
 };
 
-template <int LPP>
+// EXT: 0 cosine-weighted directional types (the default); 1 extended points -- for acceptors
+// and donors the anchor term gets weight 1 and an extra Gaussian between the extended points
+// anchor + unit vector is added; 2 only the extended-point term (anchor weight 0).  The
+// extended types are the typed overlap's EXTENDED_POINT_TYPES = {acceptor, donor}
+// (accel/drivers/pharm_overlap.py:33, :185-200), which the batched fine loop differentiates;
+// halogens keep their cosine weight.
+template <int LPP, int EXT = 0>
 __device__ __forceinline__ void pharm_pose(const float4* __restrict__ sRA,
                                            const float4* __restrict__ sRV,
                                            const float4* __restrict__ sFA,
@@ -457,7 +477,9 @@ __device__ __forceinline__ void pharm_pose(const float4* __restrict__ sRA,
     const float3 pa = rot_apply(R, fa.x, fa.y, fa.z);
     const float ax = pa.x + tx, ay = pa.y + ty, az = pa.z + tz;
     const float3 pv = rot_apply(R, fv.x, fv.y, fv.z);
+    const bool ext = EXT != 0 && (ityp == 0 || ityp == 1);  // acceptor, donor
     float fx = 0.f, fy = 0.f, fz = 0.f, wx = 0.f, wy = 0.f, wz = 0.f, o = 0.f;
+    float ex = 0.f, ey = 0.f, ez = 0.f;  // force at the extended point (EXT)
     for (int i = 0; i < N; ++i) {
       const float4 ra = sRA[i];
       if (__float_as_int(ra.w) != ityp) continue;
@@ -468,14 +490,24 @@ __device__ __forceinline__ void pharm_pose(const float4* __restrict__ sRA,
       float4 rv = make_float4(0.f, 0.f, 0.f, 0.f);
       if (icat == 1 || icat == 2) {
         rv = sRV[i];
-        const float D = pv.x * rv.x + pv.y * rv.y + pv.z * rv.z;
-        if (icat == 1) {
-          const float Dc = fminf(fmaxf(D, 0.f), 1.f);
-          w = (Dc + 2.f) * (1.f / 3.f);
-          c = (D > 0.f && D < 1.f) ? 1.f : 0.f;
+        if (ext) {
+          w = EXT == 1 ? 1.f : 0.f;
+          // extended points: (a_ref + v_ref) - (R (a_fit + v_fit) + t)
+          const float gx = dx + rv.x - pv.x, gy = dy + rv.y - pv.y, gz = dz + rv.z - pv.z;
+          const float KEe = iK * ex2(nk * (gx * gx + gy * gy + gz * gz));
+          o += KEe;
+          const float ae = ialpha * KEe;
+          ex = fmaf(ae, gx, ex); ey = fmaf(ae, gy, ey); ez = fmaf(ae, gz, ez);
         } else {
-          w = (fabsf(D) + 2.f) * (1.f / 3.f);
-          c = D > 0.f ? 1.f : (D < 0.f ? -1.f : 0.f);
+          const float D = pv.x * rv.x + pv.y * rv.y + pv.z * rv.z;
+          if (icat == 1) {
+            const float Dc = fminf(fmaxf(D, 0.f), 1.f);
+            w = (Dc + 2.f) * (1.f / 3.f);
+            c = (D > 0.f && D < 1.f) ? 1.f : 0.f;
+          } else {
+            w = (fabsf(D) + 2.f) * (1.f / 3.f);
+            c = D > 0.f ? 1.f : (D < 0.f ? -1.f : 0.f);
+          }
         }
       }
       const float KE = iK * E;
@@ -488,6 +520,7 @@ __device__ __forceinline__ void pharm_pose(const float4* __restrict__ sRA,
     }
     acc.v += o;
     acc.add_force(fx, fy, fz, fa.x, fa.y, fa.z);
+    if (ext) acc.add_force(ex, ey, ez, fa.x + fv.x, fa.y + fv.y, fa.z + fv.z);
     // weight force acts through the body-frame vector; it does not move t
     acc.g[0] = fmaf(wx, fv.x, acc.g[0]); acc.g[1] = fmaf(wx, fv.y, acc.g[1]);
     acc.g[2] = fmaf(wx, fv.z, acc.g[2]); acc.g[3] = fmaf(wy, fv.x, acc.g[3]);

@@ -124,6 +124,6 @@ int pick_best_launch(const float* rs, const float* rq, const float* rt, int P, i
 int self_overlap_launch(const float* pts, const int32_t* off, int n_mol, int max_n, float alpha,
                         int esp, float inv_lam, float* out, cudaStream_t st);
 int pharm_self_launch(const float* anc, const float* vec, const int32_t* off, int n_mol, int max_n,
-                      int directional, float* out, cudaStream_t st);
+                      int directional, int extended, float* out, cudaStream_t st);
 
 }  // namespace fss

@@ -162,11 +162,14 @@ def self_overlap(cs: CloudSet, alpha: float, esp: bool = False, lam: Optional[fl
     return out
 
 
-def pharm_self_overlap(ps: PharmSet, directional: bool = True):
+def pharm_self_overlap(ps: PharmSet, directional: bool = True, extended: int = 0):
+    """Self overlap per molecule; ``extended`` 0 (cosine weights), 1 (extended points and
+    anchors) or 2 (extended points only), as batch_pharm_self_overlap
+    (accel/drivers/pharm_overlap.py:413)."""
     out = torch.empty(ps.n_mol, dtype=_f32, device=ps.anc.device)
     check(_lib.load().fss_pharm_self_overlap(ptr(ps.anc, _f32), ptr(ps.vec, _f32),
                                              ptr(ps.off, _i32), ps.n_mol, ps.max_points,
-                                             int(directional), ptr(out),
+                                             int(directional), int(extended), ptr(out),
                                              stream_ptr(ps.anc.device)), "pharm_self_overlap")
     return out
 

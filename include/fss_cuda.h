@@ -98,11 +98,13 @@ int fss_tanimoto_adam_step(const float *V, const float *dQ, const float *dT, con
 int fss_self_overlap(const float *pts, const int32_t *off, int32_t n_mol, int32_t max_points,
                      float alpha, int32_t esp, float inv_lam, float *out, void *stream);
 
-/* Pharmacophore self overlap per molecule (directional or colour tables).
- * Replaces the identity-pose self overlaps of accel/drivers/pharm.py:336-346. */
+/* Pharmacophore self overlap per molecule (directional or colour tables); `extended` 0/1/2
+ * as fss_align_desc.pharm_extended (directional tables only).
+ * Replaces the identity-pose self overlaps of accel/drivers/pharm.py:336-346 and
+ * batch_pharm_self_overlap (accel/drivers/pharm_overlap.py:413-439). */
 int fss_pharm_self_overlap(const float *anc, const float *vec, const int32_t *off,
-                           int32_t n_mol, int32_t max_features, int32_t directional, float *out,
-                           void *stream);
+                           int32_t n_mol, int32_t max_features, int32_t directional,
+                           int32_t extended, float *out, void *stream);
 
 /* Multi-start seeds for P pairs: identity, 4 PCA alignments (fp64 closed-form eigensolver),
  * up to 6 structured +-90 degree axis swaps, then the Fibonacci set `fibo_q` (n_fibo,4)
@@ -156,6 +158,14 @@ typedef struct fss_align_desc {
                               * points per lane, 2 CTAs/SM register budget), 2 wide (6 fit
                               * points per lane, deeper unroll), 3 roomy (4 fit points, one
                               * CTA/SM register budget); 2 and 3 for modes SHAPE and ESP */
+  int32_t pharm_extended;    /* mode PHARM: 0 cosine-weighted directional features, 1 extended
+                              * points (anchor + unit vector) plus anchors, 2 extended points
+                              * only (extended_points / only_extended of
+                              * analytical_gradients/_torch.py:223-355) */
+  int32_t similarity;        /* mode PHARM: 0 Tanimoto, 1 Tversky */
+  float tversky_sigma;       /* Tversky D = sigma V_AA + (1 - sigma) V_BB, sigma in [0, 1]
+                              * (accel/drivers/pharm.py:40: tversky 0.95, tversky_ref 1.0,
+                              * tversky_fit 0.05) */
   /* scratch: two device int32 -- [0] work counter, [1] status flags (bit 0: a pair was
    * larger than the max_* extents).  The launch zeroes both on `stream`. */
   int32_t *scratch;

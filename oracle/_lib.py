@@ -37,12 +37,13 @@ def lib():
             ctypes.c_double, ctypes.c_double, ctypes.c_int, _vp, _vp, _vp, ctypes.c_int]
         L.fsso_overlap_grad.restype = None
         L.fsso_pharm_grad.argtypes = [ctypes.c_int] * 3 + [_vp] * 10 + [_vp] * 3 + [
-            ctypes.c_int, _vp, _vp, _vp, ctypes.c_int]
+            ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int]
         L.fsso_pharm_grad.restype = None
         L.fsso_fine_loop_flat.argtypes = (
             [ctypes.c_int] * 4 + [_vp] * 6 + [ctypes.c_int] * 2 + [_vp] * 11 +
             [ctypes.c_double] * 3 + [_vp] * 4 + [ctypes.c_int, ctypes.c_float, ctypes.c_int,
-                                                  ctypes.c_double] + [_vp] * 3 + [ctypes.c_int])
+                                                  ctypes.c_double] + [_vp] * 3 +
+            [ctypes.c_int] * 3)
         L.fsso_fine_loop_flat.restype = ctypes.c_int
         L.fsso_max_threads.restype = ctypes.c_int
         _LIB = L

@@ -100,8 +100,9 @@ def overlap_grad(A, B, q, t, N_real=None, M_real=None, *, alpha=0.81, CA=None, C
 
 
 def pharm_grad(A, B, RV, FV, At, Bt, q, t, N_real=None, M_real=None, *, directionless=False,
-               need_grad=True, nthreads=None):
-    """Typed pharmacophore overlap and dO/dq, dO/dt per pose, float64 (cpu.py:412-612)."""
+               need_grad=True, nthreads=None, ext=0):
+    """Typed pharmacophore overlap and dO/dq, dO/dt per pose, float64 (cpu.py:412-612);
+    ``ext`` 1/2 adds the extended points of analytical_gradients/_torch.py:288-355."""
     A, B, q, t = _f32(A), _f32(B), _f32(q), _f32(t)
     RV, FV = _f32(RV), _f32(FV)
     At, Bt = _i32(At), _i32(Bt)
@@ -116,7 +117,8 @@ def pharm_grad(A, B, RV, FV, At, Bt, q, t, N_real=None, M_real=None, *, directio
     P = _lib.ptr
     _lib.lib().fsso_pharm_grad(K, Npad, Mpad, P(A), P(B), P(RV), P(FV), P(At), P(Bt), P(q),
                                P(t), P(Nr), P(Mr), P(al), P(ks), P(cats),
-                               int(bool(need_grad)), P(O), P(dQ), P(dT), _threads(nthreads))
+                               int(bool(need_grad)), P(O), P(dQ), P(dT), _threads(nthreads),
+                               int(ext))
     return O, dQ, dT
 
 
@@ -134,18 +136,18 @@ def self_overlap(X, N_real, *, alpha=0.81, C=None, lam=None, nthreads=None):
     return V.astype(np.float32)
 
 
-def pharm_self_overlap(X, V, T, N_real, *, directionless=False, nthreads=None):
+def pharm_self_overlap(X, V, T, N_real, *, directionless=False, nthreads=None, ext=0):
     """Pharmacophore self-overlap via the dq kernel at identity (pharm.py:336-346)."""
     q, t = _identity_pose(X.shape[0])
     O, _, _ = pharm_grad(X, X, V, V, T, T, q, t, N_real, N_real, directionless=directionless,
-                         need_grad=False, nthreads=nthreads)
+                         need_grad=False, nthreads=nthreads, ext=ext)
     return O.astype(np.float32)
 
 
 def fine_loop(mode, q_seed, t_seed, norm_s, *, steps, lr, es_patience=None, es_tol=1e-5,
               A=None, B=None, CA=None, CB=None, Nr=None, Mr=None, alpha=0.81, lam=None,
               PA=None, PB=None, PRV=None, PFV=None, PAt=None, PBt=None, PNr=None, PMr=None,
-              directionless=False, norm_c=None, w=0.5, nthreads=None):
+              directionless=False, norm_c=None, w=0.5, nthreads=None, ext=0, tversky=False):
     """Run the fused fine loop over K pose rows (cpu_fused.py:179-217).
 
     All per-row arrays are already expanded to K = pairs x starts rows.  Returns
@@ -174,7 +176,7 @@ def fine_loop(mode, q_seed, t_seed, norm_s, *, steps, lr, es_patience=None, es_t
         P(PB), P(PRV), P(PFV), P(PAt), P(PBt), P(PNr), P(PMr), P(al), P(ks), P(cats),
         float(alpha), inv_lam, float(w), P(norm_s), P(norm_c), P(q), P(t), int(steps),
         float(np.float32(lr)), -1 if es_patience is None else int(es_patience), float(es_tol),
-        P(best), P(bq), P(bt), _threads(nthreads))
+        P(best), P(bq), P(bt), _threads(nthreads), int(ext), int(bool(tversky)))
     if n < 0:
         raise MemoryError("oracle fine loop could not allocate its Adam state")
     return best, bq, bt, q, t, n
@@ -246,13 +248,21 @@ def center_anchors(X, N_real):
     return c.astype(np.float32), (X - c[:, None, :]).astype(np.float32)
 
 
+TVERSKY_SIGMA = {"tversky": 0.95, "tversky_ref": 1.0, "tversky_fit": 0.05}  # pharm.py:40
+
+
 def align_pharm(A, B, RV, FV, At, Bt, N_real, M_real, *, num_seeds=50, steps=100, lr=0.075,
-                seeds=None, es_patience=None, es_tol=1e-5, nthreads=None, return_rows=False):
-    """Batched directional pharmacophore alignment: pharm.py:123-517, CPU fused branch.
+                seeds=None, es_patience=None, es_tol=1e-5, nthreads=None, return_rows=False,
+                similarity="tanimoto", extended_points=False, only_extended=False):
+    """Batched directional pharmacophore alignment: pharm.py:123-517, CPU fused branch for
+    Tanimoto without extended points, and the same step arithmetic for the eager branch the
+    reference takes otherwise (Tversky tail pharm.py:417-426; extended points via
+    compute_overlap_and_grad_pharm, self overlaps with the same flags pharm.py:732-748).
 
     Anchors are centred per cloud before seeding and the optimum translation is folded back
     into the original frame at the end.  ``seeds`` (if given) are for the centred clouds.
     """
+    ext = 0 if not extended_points else (2 if only_extended else 1)
     nb = np.asarray(A).shape[0]
     c_ref, A_c = center_anchors(A, N_real)
     c_fit, B_c = center_anchors(B, M_real)
@@ -260,13 +270,19 @@ def align_pharm(A, B, RV, FV, At, Bt, N_real, M_real, *, num_seeds=50, steps=100
         seeds = batched_seeds(A_c, B_c, N_real, M_real, num_seeds)
     qs, ts = seeds
     S = qs.shape[1]
-    norm = (pharm_self_overlap(A_c, RV, At, N_real, nthreads=nthreads)
-            + pharm_self_overlap(B_c, FV, Bt, M_real, nthreads=nthreads)).astype(np.float32)
+    VAA = pharm_self_overlap(A_c, RV, At, N_real, nthreads=nthreads, ext=ext)
+    VBB = pharm_self_overlap(B_c, FV, Bt, M_real, nthreads=nthreads, ext=ext)
+    if similarity == "tanimoto":
+        norm = (VAA + VBB).astype(np.float32)
+    else:
+        sg = np.float32(TVERSKY_SIGMA[similarity])
+        norm = (sg * VAA + (np.float32(1) - sg) * VBB).astype(np.float32)
     best, bq, bt, _, _, n = fine_loop(
         2, qs.reshape(-1, 4), ts.reshape(-1, 3), _rep(norm, S), steps=steps, lr=lr,
         es_patience=es_patience, es_tol=es_tol, PA=_rep(A_c, S), PB=_rep(B_c, S),
         PRV=_rep(_f32(RV), S), PFV=_rep(_f32(FV), S), PAt=_rep(At, S), PBt=_rep(Bt, S),
-        PNr=_rep(N_real, S), PMr=_rep(M_real, S), nthreads=nthreads)
+        PNr=_rep(N_real, S), PMr=_rep(M_real, S), nthreads=nthreads, ext=ext,
+        tversky=similarity != "tanimoto")
     sc, q, t = _pick(best, bq, bt, nb, S)
     R = quat_to_rotmat(q.astype(np.float32))
     t = (t - np.einsum('bij,bj->bi', R, c_fit) + c_ref).astype(np.float32)

@@ -13,6 +13,9 @@
  *   fsso_pharm_dq       <- cpu.py:500-582 (_pharm_grad_dq_kernel, directional pharm)
  *   fsso_pharm_color    <- cpu.py:412-458 (_pharm_color_grad_kernel, directionless)
  *   tail_tanimoto       <- cpu_fused.py:54-108  (_tail_tanimoto)
+ *   pose_pharm ext!=0   <- analytical_gradients/_torch.py:223-355 (extended_points /
+ *                          only_extended of compute_overlap_and_grad_pharm)
+ *   tail_tversky        <- accel/drivers/pharm.py:417-426 + pharm_overlap.py:36-59
  *   tail_combo          <- cpu_fused.py:111-167 (_tail_vol_color)
  *   fsso_fine_loop      <- cpu_fused.py:179-217 (fine_loop_cpu) + the per-mode glue
  *                          cpu_fused.py:225-338
@@ -163,11 +166,16 @@ static inline void unit_vec(const float *v, double out[3]) {
 /* One pose of the typed pharmacophore overlap with in-register dO/dq (cpu.py:506-581).
  * A/B anchors, RV/FV vectors, At/Bt int32 types; alphas/Ks/cats are the 9-entry
  * lookup tables.  directional==0 gives the directionless colour kernel (cpu.py:418-457),
- * which is the directional one with every real type in category 0. */
+ * which is the directional one with every real type in category 0.
+ * ext: 0 cosine weights; 1 extended points -- acceptor and donor pairs get anchor weight 1
+ * plus a Gaussian between the extended points anchor + unit vector; 2 extended points only
+ * (anchor weight 0).  The extended types are EXTENDED_POINT_TYPES = {acceptor, donor} of
+ * the typed overlap the batched fine loop differentiates (accel/drivers/pharm_overlap.py:33,
+ * :185-200); halogen keeps its cosine weight. */
 static void pose_pharm(const float *A, const float *B, const float *RV, const float *FV,
                        const int32_t *At, const int32_t *Bt, const float *q, const float *t,
                        int n_real, int m_real, const double *alphas, const double *Ks,
-                       const int32_t *cats, int need_grad,
+                       const int32_t *cats, int ext, int need_grad,
                        double *O, double dQ[4], double dT[3]) {
     double R[9];
     rotmat(q, R);
@@ -191,6 +199,8 @@ static void pose_pharm(const float *A, const float *B, const float *RV, const fl
         const double fvtz = R[6] * fv[0] + R[7] * fv[1] + R[8] * fv[2];
         double f[3] = {0.0, 0.0, 0.0};   /* positional force sum_j alpha*K*w*E*(ref - rotfit) */
         double wf[3] = {0.0, 0.0, 0.0};  /* weight force sum_j coeff * ref_vn */
+        double fe[3] = {0.0, 0.0, 0.0};  /* force at the extended point (ext != 0) */
+        const int use_ext = ext != 0 && (ityp == 0 || ityp == 1);
         for (int j = 0; j < n_real; ++j) {
             if (At[j] != ityp) continue;
             const double dx = fatx - A[3 * j], dy = faty - A[3 * j + 1], dz = fatz - A[3 * j + 2];
@@ -198,7 +208,18 @@ static void pose_pharm(const float *A, const float *B, const float *RV, const fl
             const double E = exp(-ialpha * 0.5 * r2);
             double rv[3] = {0.0, 0.0, 0.0};
             double w = 1.0, c = 0.0;
-            if (icat == 1 || icat == 2) {
+            if (use_ext) {
+                unit_vec(RV + 3 * j, rv);
+                w = ext == 1 ? 1.0 : 0.0;
+                /* (rotfit + R v_fit) - (ref + v_ref), the sign convention of dx */
+                const double ex = dx + fvtx - rv[0], ey = dy + fvty - rv[1], ez = dz + fvtz - rv[2];
+                const double Ee = iK * exp(-ialpha * 0.5 * (ex * ex + ey * ey + ez * ez));
+                Oacc += Ee;
+                if (need_grad) {
+                    fe[0] += -ialpha * Ee * ex; fe[1] += -ialpha * Ee * ey;
+                    fe[2] += -ialpha * Ee * ez;
+                }
+            } else if (icat == 1 || icat == 2) {
                 unit_vec(RV + 3 * j, rv);
                 const double D = fvtx * rv[0] + fvty * rv[1] + fvtz * rv[2];
                 if (icat == 1) {
@@ -223,6 +244,10 @@ static void pose_pharm(const float *A, const float *B, const float *RV, const fl
             dT[0] += f[0]; dT[1] += f[1]; dT[2] += f[2];
             quat_tail(f, fax0, fay0, faz0, q, dQ);
             quat_tail(wf, fv[0], fv[1], fv[2], q, dQ);
+            if (use_ext) {
+                dT[0] += fe[0]; dT[1] += fe[1]; dT[2] += fe[2];
+                quat_tail(fe, fax0 + fv[0], fay0 + fv[1], faz0 + fv[2], q, dQ);
+            }
         }
     }
     *O = Oacc;
@@ -266,7 +291,7 @@ typedef struct {
     const int32_t *Nr, *Mr;
     const double *alphas, *Ks;
     const int32_t *cats;
-    int need_grad;
+    int ext, need_grad;
     double *O, *dQ, *dT;
 } pharm_args;
 
@@ -276,7 +301,7 @@ static void pharm_one(void *ctx, int k) {
                a->RV ? a->RV + (size_t)k * a->Npad * 3 : NULL,
                a->FV ? a->FV + (size_t)k * a->Mpad * 3 : NULL, a->At + (size_t)k * a->Npad,
                a->Bt + (size_t)k * a->Mpad, a->q + 4 * (size_t)k, a->t + 3 * (size_t)k,
-               a->Nr[k], a->Mr[k], a->alphas, a->Ks, a->cats, a->need_grad, a->O + k,
+               a->Nr[k], a->Mr[k], a->alphas, a->Ks, a->cats, a->ext, a->need_grad, a->O + k,
                a->dQ + 4 * (size_t)k, a->dT + 3 * (size_t)k);
 }
 
@@ -284,9 +309,9 @@ void fsso_pharm_grad(int K, int Npad, int Mpad, const float *A, const float *B,
                      const float *RV, const float *FV, const int32_t *At, const int32_t *Bt,
                      const float *q, const float *t, const int32_t *Nr, const int32_t *Mr,
                      const double *alphas, const double *Ks, const int32_t *cats,
-                     int need_grad, double *O, double *dQ, double *dT, int nthreads) {
+                     int need_grad, double *O, double *dQ, double *dT, int nthreads, int ext) {
     pharm_args a = {Npad, Mpad, A, B, RV, FV, At, Bt, q, t, Nr, Mr, alphas, Ks, cats,
-                    need_grad, O, dQ, dT};
+                    ext, need_grad, O, dQ, dT};
     parallel_for(K, nthreads, 4, pharm_one, &a);
 }
 
@@ -344,6 +369,21 @@ static void tail_tanimoto(float O, const float dQf[4], const float dTf[3], float
     adam_update(q, t, gq, gt, mq, vq, mt, vt, lr);
 }
 
+/* Tversky tail (pharm.py:417-426, pharm_overlap.py:36-59): score = min(O/D, 1) (0 when
+ * D <= 1e-8), gradient scale active/D with active = O < D. */
+static void tail_tversky(float O, const float dQf[4], const float dTf[3], float D,
+                         float *q, float *t, float *mq, float *vq, float *mt, float *vt,
+                         float *best, float *bq, float *bt, float lr) {
+    double score = D > 1e-8f ? (double)O / (double)D : 0.0;
+    if (score > 1.0) score = 1.0;
+    const double scale = O < D ? 1.0 / (double)D : 0.0;
+    track_best(score, q, t, best, bq, bt);
+    double gq[4], gt[3];
+    for (int c = 0; c < 4; ++c) gq[c] = -scale * dQf[c];
+    for (int c = 0; c < 3; ++c) gt[c] = -scale * dTf[c];
+    adam_update(q, t, gq, gt, mq, vq, mt, vt, lr);
+}
+
 /* two-channel tail: (1-w)*shape Tanimoto + w*pharm Tanimoto (cpu_fused.py:111-167) */
 static void tail_combo(float Vs, const float dQs[4], const float dTs[3], float Oc,
                        const float dQc[4], const float dTc[3], float norm_s, float norm_c,
@@ -379,7 +419,9 @@ typedef struct {
     const double *alphas, *Ks;
     const int32_t *cats;
     double alpha, inv_lam, w;
-    const float *norm_s, *norm_c; /* per pose self-overlap sums */
+    const float *norm_s, *norm_c; /* per pose self-overlap sums (Tversky: D per pose) */
+    int ext;               /* pharm: extended points 0/1/2 */
+    int tversky;           /* pharm: norm_s holds the Tversky denominator D */
 } fsso_problem;
 
 /* Evaluate the channels of one pose and apply its tail (one optimisation step). */
@@ -407,12 +449,15 @@ static void pose_step(const fsso_problem *P, int k, float *q, float *t, float *m
                P->PRV ? P->PRV + (size_t)k * P->Ppad * 3 : NULL,
                P->PFV ? P->PFV + (size_t)k * P->Qpad * 3 : NULL,
                P->PAt + (size_t)k * P->Ppad, P->PBt + (size_t)k * P->Qpad, q, t,
-               P->PNr[k], P->PMr[k], P->alphas, P->Ks, P->cats, 1, &O, dQp, dTp);
+               P->PNr[k], P->PMr[k], P->alphas, P->Ks, P->cats, P->ext, 1, &O, dQp, dTp);
     Of = (float)O;
     for (int c = 0; c < 4; ++c) dQpf[c] = (float)dQp[c];
     for (int c = 0; c < 3; ++c) dTpf[c] = (float)dTp[c];
     if (P->mode == FSSO_PHARM) {
-        tail_tanimoto(Of, dQpf, dTpf, P->norm_s[k], q, t, mq, vq, mt, vt, best, bq, bt, lr);
+        if (P->tversky)
+            tail_tversky(Of, dQpf, dTpf, P->norm_s[k], q, t, mq, vq, mt, vt, best, bq, bt, lr);
+        else
+            tail_tanimoto(Of, dQpf, dTpf, P->norm_s[k], q, t, mq, vq, mt, vt, best, bq, bt, lr);
         return;
     }
     tail_combo(Vf, dQf, dTf, Of, dQpf, dTpf, P->norm_s[k], P->norm_c[k], (float)P->w, q, t,
@@ -486,9 +531,10 @@ int fsso_fine_loop_flat(int mode, int K, int Npad, int Mpad, const float *A, con
                         const double *Ks, const int32_t *cats, double alpha, double inv_lam,
                         double w, const float *norm_s, const float *norm_c, float *q_io,
                         float *t_io, int steps, float lr, int es_patience, double es_tol,
-                        float *best, float *bq, float *bt, int nthreads) {
+                        float *best, float *bq, float *bt, int nthreads, int ext, int tversky) {
     fsso_problem P = {mode, K, Npad, Mpad, A, B, CA, CB, Nr, Mr, Ppad, Qpad, PA, PB, PRV, PFV,
-                      PAt, PBt, PNr, PMr, alphas, Ks, cats, alpha, inv_lam, w, norm_s, norm_c};
+                      PAt, PBt, PNr, PMr, alphas, Ks, cats, alpha, inv_lam, w, norm_s, norm_c,
+                      ext, tversky};
     return fsso_fine_loop(&P, q_io, t_io, steps, lr, es_patience, es_tol, best, bq, bt, nthreads);
 }
 

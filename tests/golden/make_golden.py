@@ -77,9 +77,12 @@ def rotated_copy(rng, X, shift=1.0):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("FSS_REFERENCE", "/root/reference"))
+    ap.add_argument("--only", default="", help="write only this fixture (e.g. pharm_ext)")
     args = ap.parse_args()
     _install_stub()
     sys.path.insert(0, args.reference)
+    if args.only == "pharm_ext":
+        return make_pharm_ext()
     import torch
     torch.set_num_threads(max(1, os.cpu_count() or 1))
     from shepherd_score.accel.kernels import cpu as rk
@@ -264,6 +267,76 @@ def main():
         out[f"combo_score_dl{int(dl)}"] = s.detach().numpy()
     np.savez_compressed(os.path.join(HERE, "scores.npz"), **out)
     print("scores.npz")
+    make_pharm_ext()
+
+
+def make_pharm_ext():
+    """pharm_ext.npz: extended-point pharmacophore overlaps/gradients (autograd through
+    batch_pharm_cross_overlap_with_transform, extended_points / only_extended), extended self overlaps
+    (batch_pharm_self_overlap) and Tversky / extended-point alignments
+    (coarse_fine_pharm_align_many) from the reference, on their own seeded inputs."""
+    import torch
+    from shepherd_score.accel.drivers.pharm import coarse_fine_pharm_align_many
+    from shepherd_score.accel.drivers.pharm_overlap import (
+        batch_pharm_cross_overlap_with_transform, batch_pharm_self_overlap)
+
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a))
+    rng = np.random.default_rng(2024)
+    out = {}
+    # single poses on unpadded molecules (8 features each): value, dO/dt, dO/dq
+    refs, fits = syn.shape_pharm_pairs(6, seed=21, ph_lo=8, ph_hi=8)
+    A = np.stack([m["pharm_ancs"] for m in refs]).astype(np.float64)
+    B = np.stack([m["pharm_ancs"] for m in fits]).astype(np.float64)
+    RV = np.stack([m["pharm_vecs"] for m in refs]).astype(np.float64)
+    FV = np.stack([m["pharm_vecs"] for m in fits]).astype(np.float64)
+    At = np.stack([m["pharm_types"] for m in refs]).astype(np.int64)
+    Bt = np.stack([m["pharm_types"] for m in fits]).astype(np.int64)
+    B[0], FV[0], Bt[0] = A[0] + 0.3, RV[0], At[0]          # a near-copy: many same-type pairs
+    q = rand_quat(rng, 6).astype(np.float32).astype(np.float64)
+    t = (0.5 * rng.standard_normal((6, 3))).astype(np.float32).astype(np.float64)
+    # fp32-representable inputs, evaluated in fp64 (the oracle reads fp32 arrays)
+    A, B, RV, FV = (x.astype(np.float32).astype(np.float64) for x in (A, B, RV, FV))
+    out.update(sp_A=A, sp_B=B, sp_RV=RV, sp_FV=FV, sp_At=At, sp_Bt=Bt, sp_q=q, sp_t=t)
+    for ext, only in ((1, False), (2, True)):
+        # the typed path the batched fine loop differentiates on ragged buckets
+        # (pharm.py:449-465): acceptor/donor get extended points, halogen keeps its cosine weight
+        qv = T(q).clone().requires_grad_(True)
+        tv = T(t).clone().requires_grad_(True)
+        O = batch_pharm_cross_overlap_with_transform(T(A), T(B), T(RV), T(FV), T(At), T(Bt), qv,
+                                                     tv, extended_points=True, only_extended=only)
+        dQ, dT = torch.autograd.grad(O.sum(), (qv, tv))
+        out[f"sp{ext}_O"] = O.detach().numpy()
+        out[f"sp{ext}_dT"] = dT.numpy()
+        out[f"sp{ext}_dQ"] = dQ.numpy()     # tangent to the unit sphere (q is normalised inside)
+
+    # alignments: 5 ragged pairs, pair 0 a rotated copy
+    prefs, pfits = syn.shape_pharm_pairs(5, seed=23)
+    pfits[0] = dict(prefs[0])
+    Rr = syn.random_rotation(rng)
+    sh = rng.standard_normal(3)
+    pfits[0]["pharm_ancs"] = (prefs[0]["pharm_ancs"] @ Rr.T + sh).astype(np.float32)
+    pfits[0]["pharm_vecs"] = (prefs[0]["pharm_vecs"] @ Rr.T).astype(np.float32)
+    PA, PN = pad([m["pharm_ancs"] for m in prefs]); PB, PM = pad([m["pharm_ancs"] for m in pfits])
+    PRV, _ = pad([m["pharm_vecs"] for m in prefs]); PFV, _ = pad([m["pharm_vecs"] for m in pfits])
+    PAt, _ = pad([m["pharm_types"] for m in prefs], fill=0, dtype=np.int64)
+    PBt, _ = pad([m["pharm_types"] for m in pfits], fill=0, dtype=np.int64)
+    out.update(al_A=PA, al_B=PB, al_RV=PRV, al_FV=PFV, al_At=PAt, al_Bt=PBt, al_N=PN, al_M=PM)
+    for tag, sim, ext, only in (("tv", "tversky", False, False),
+                                ("tvfit", "tversky_fit", False, False),
+                                ("ext", "tanimoto", True, False),
+                                ("onlyref", "tversky_ref", True, True)):
+        VAA = batch_pharm_self_overlap(T(PA), T(PRV), T(PAt), extended_points=ext,
+                                       only_extended=only, N_real=T(PN))
+        VBB = batch_pharm_self_overlap(T(PB), T(PFV), T(PBt), extended_points=ext,
+                                       only_extended=only, N_real=T(PM))
+        sc, bq, bt = coarse_fine_pharm_align_many(
+            T(PA), T(PB), T(PRV), T(PFV), T(PAt), T(PBt), VAA, VBB, similarity=sim,
+            extended_points=ext, only_extended=only, num_seeds=16, steps_fine=40, lr=0.1,
+            N_real=T(PN), M_real=T(PM), early_stop_patience=10 ** 9)
+        out.update({f"{tag}_VAA": VAA.numpy(), f"{tag}_VBB": VBB.numpy(),
+                    f"{tag}_score": sc.numpy(), f"{tag}_q": bq.numpy(), f"{tag}_t": bt.numpy()})
+    np.savez_compressed(os.path.join(HERE, "pharm_ext.npz"), **out)
+    print("pharm_ext.npz")
 
 
 if __name__ == "__main__":

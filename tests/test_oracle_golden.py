@@ -127,3 +127,49 @@ def test_fp64_coordinate_gradients(golden):
         np.testing.assert_allclose(gf, s[f"{tag}_grad_fit"], rtol=1e-8, atol=1e-12)
         np.testing.assert_allclose(gqr, s[f"{tag}_gradq_ref"], rtol=1e-8, atol=1e-12)
         np.testing.assert_allclose(gqf, s[f"{tag}_gradq_fit"], rtol=1e-8, atol=1e-12)
+
+
+@pytest.mark.parametrize("ext", [1, 2])
+def test_pharm_extended_points_kernel(golden, ext):
+    """Extended-point overlap (the typed overlap of the batched fine loop, extended_points /
+    only_extended): value, dO/dt and the tangential part of dO/dq (the reference normalises q
+    inside its transform, so its autograd dO/dq is tangent to the unit sphere)."""
+    g = golden["pharm_ext"]
+    O, dQ, dT = oa.pharm_grad(g["sp_A"], g["sp_B"], g["sp_RV"], g["sp_FV"], g["sp_At"],
+                              g["sp_Bt"], g["sp_q"], g["sp_t"], ext=ext)
+    q = g["sp_q"].astype(np.float64)
+    q = q / np.linalg.norm(q, axis=1, keepdims=True)
+    dQ = dQ - q * (dQ * q).sum(1, keepdims=True)
+    # q is fp32 (|q| = 1 to 1e-7) and the reference normalises it; the oracle does not
+    np.testing.assert_allclose(O, g[f"sp{ext}_O"], rtol=5e-6, atol=1e-9)
+    np.testing.assert_allclose(dT, g[f"sp{ext}_dT"], rtol=1e-5, atol=1e-7)
+    np.testing.assert_allclose(dQ, g[f"sp{ext}_dQ"], rtol=1e-5, atol=1e-6)
+    assert np.all(O > 0)
+
+
+@pytest.mark.parametrize("tag,ext", [("tv", 0), ("ext", 1), ("onlyref", 2)])
+def test_pharm_extended_self_overlaps(golden, tag, ext):
+    g = golden["pharm_ext"]
+    ca, A = oa.center_anchors(g["al_A"], g["al_N"])
+    cb, B = oa.center_anchors(g["al_B"], g["al_M"])
+    va = oa.pharm_self_overlap(A, g["al_RV"], g["al_At"], g["al_N"], ext=ext)
+    vb = oa.pharm_self_overlap(B, g["al_FV"], g["al_Bt"], g["al_M"], ext=ext)
+    np.testing.assert_allclose(va, g[f"{tag}_VAA"], rtol=1e-5)
+    np.testing.assert_allclose(vb, g[f"{tag}_VBB"], rtol=1e-5)
+
+
+@pytest.mark.parametrize("tag,sim,ext,only", [("tv", "tversky", False, False),
+                                              ("tvfit", "tversky_fit", False, False),
+                                              ("ext", "tanimoto", True, False),
+                                              ("onlyref", "tversky_ref", True, True)])
+def test_align_pharm_tversky_and_extended(golden, tag, sim, ext, only):
+    """Tversky tails and extended points in the pharmacophore fine loop: best scores match
+    the reference's eager loop (the self copy reaches 1; Adam trajectories of two fp
+    implementations separate chaotically, so the rest compare by best score)."""
+    g = golden["pharm_ext"]
+    sc, q, t = oa.align_pharm(g["al_A"], g["al_B"], g["al_RV"], g["al_FV"], g["al_At"],
+                              g["al_Bt"], g["al_N"], g["al_M"], num_seeds=16, steps=40, lr=0.1,
+                              similarity=sim, extended_points=ext, only_extended=only)
+    ref = g[f"{tag}_score"]
+    assert sc[0] > 0.99 and ref[0] > 0.99
+    np.testing.assert_allclose(sc, ref, atol=2e-3)
