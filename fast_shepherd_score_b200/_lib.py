@@ -17,7 +17,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("FSS_LIB") or os.path.join(_HERE, "libfss_cuda.so")
 
 FSS_OK, FSS_ERR_INVALID, FSS_ERR_CUDA, FSS_ERR_NOMEM, FSS_ERR_UNSUPPORTED, FSS_ERR_TIMEOUT = range(6)
-MODE_SHAPE, MODE_ESP, MODE_PHARM, MODE_SHAPE_PHARM, MODE_SHAPE_COLOR = range(5)
+MODE_SHAPE, MODE_ESP, MODE_PHARM, MODE_SHAPE_PHARM, MODE_SHAPE_COLOR, MODE_ESP_COMBO = range(6)
 
 _vp = ctypes.c_void_p
 _i32 = ctypes.c_int32
@@ -43,6 +43,12 @@ class AlignDesc(ctypes.Structure):
         ("lanes_per_pose", _i32), ("chunks", _i32), ("cta_per_sm", _i32),
         ("accumulate", _i32), ("kernel_variant", _i32), ("pharm_extended", _i32),
         ("similarity", _i32), ("tversky_sigma", _f32),
+        ("ref_atoms", _vp), ("ref_radii", _vp), ("ref_atom_off", _vp),
+        ("fit_atoms", _vp), ("fit_radii", _vp), ("fit_atom_off", _vp),
+        ("ref_surf", _vp), ("ref_surf_off", _vp), ("fit_surf", _vp), ("fit_surf_off", _vp),
+        ("max_ref_atoms", _i32), ("max_fit_atoms", _i32), ("max_ref_surf", _i32),
+        ("max_fit_surf", _i32), ("esp_inv_lam", _f32), ("coulomb", _f32),
+        ("probe_radius", _f32), ("esp_weight", _f32), ("esp_stride", _i32),
         ("scratch", _vp),
     ]
 

@@ -40,7 +40,9 @@ TVERSKY_SIGMA = {"tversky": 0.95, "tversky_ref": 1.0, "tversky_fit": 0.05}
 LAM_SCALING = (1e4 / (4 * 55.263 * math.pi)) ** 2   # score/constants.py:16-17
 
 MODE_IDS = {"shape": _lib.MODE_SHAPE, "esp": _lib.MODE_ESP, "pharm": _lib.MODE_PHARM,
-            "shape_pharm": _lib.MODE_SHAPE_PHARM, "shape_color": _lib.MODE_SHAPE_COLOR}
+            "shape_pharm": _lib.MODE_SHAPE_PHARM, "shape_color": _lib.MODE_SHAPE_COLOR,
+            "esp_combo": _lib.MODE_ESP_COMBO}
+COULOMB_SCALING = 1e4 / (4 * 55.263 * math.pi)   # score/constants.py:16
 
 _SCRATCH: dict = {}
 LAST_TILE: dict = {}   # tiling of the most recent fused launch (for reports)
@@ -68,7 +70,11 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
                  ref_self=None, fit_self=None, ref_self_ph=None, fit_self_ph=None,
                  order=None, lanes_per_pose: int = 0, chunks: int = 0, cta_per_sm: int = 0,
                  accumulate: int = 0, kernel_variant: int = 0, similarity: str = "tanimoto",
-                 pharm_extended: int = 0, rows=None, out=None, scratch=None,
+                 pharm_extended: int = 0, ref_atoms: Optional[CloudSet] = None,
+                 fit_atoms: Optional[CloudSet] = None, ref_radii=None, fit_radii=None,
+                 ref_surf: Optional[CloudSet] = None, fit_surf: Optional[CloudSet] = None,
+                 probe_radius: float = 1.0, esp_weight: float = 0.5, esp_stride: int = 1,
+                 rows=None, out=None, scratch=None,
                  check_status: bool = True, validate: bool = True):
     """Run the fused alignment kernel over packed clouds.
 
@@ -82,6 +88,10 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
     register budget (2 and 3 for "shape" and "esp").  Mode "pharm" only: ``similarity`` in
     ("tanimoto", "tversky", "tversky_ref", "tversky_fit") and ``pharm_extended`` 0 (cosine
     weights), 1 (extended points and anchors), 2 (extended points only).
+    Mode "esp_combo" (vol_and_surf_esp): ``ref``/``fit`` are the shape centres; ``ref_atoms`` /
+    ``fit_atoms`` the atoms with hydrogens (w = partial charge) with per-point ``*_radii``,
+    ``ref_surf``/``fit_surf`` the surface points (w = ESP at the point); ``lam`` is the raw
+    ShaEP weight (LAM_SCALING applied here), ``esp_stride`` the combo-score tracking stride.
     ``validate=False`` skips the pair-index range check (a device read-back) for callers that
     validated their indices on the host; ``check_status=False`` skips reading the kernel's
     status word (both keep the launch free of host synchronisation).
@@ -98,6 +108,19 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
         raise ValueError(f"mode {mode!r} needs ref and fit pharmacophores")
     if m == _lib.MODE_ESP and lam is None:
         raise ValueError("esp mode needs lam")
+    combo = m == _lib.MODE_ESP_COMBO
+    if combo:
+        if any(x is None for x in (ref_atoms, fit_atoms, ref_radii, fit_radii, ref_surf,
+                                   fit_surf)):
+            raise ValueError("esp_combo needs atoms, radii and surfaces for both sides")
+        if (ref_atoms.n_mol != ref.n_mol or ref_surf.n_mol != ref.n_mol or
+                fit_atoms.n_mol != fit.n_mol or fit_surf.n_mol != fit.n_mol):
+            raise ValueError("esp_combo sets must describe the same molecules")
+        if ref_radii.numel() != ref_atoms.pts.shape[0] or fit_radii.numel() != fit_atoms.pts.shape[0]:
+            raise ValueError("one radius per atom")
+        lam = 0.001 if lam is None else float(lam)
+        if not lam > 0:
+            raise ValueError("lam must be > 0")
     similarity = similarity.lower()
     if similarity != "tanimoto" and similarity not in TVERSKY_SIGMA:
         raise ValueError("similarity must be one of ('tanimoto','tversky','tversky_ref',"
@@ -122,10 +145,11 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
         if lo < 0 or int(pair_ref.max()) >= n_ref or int(pair_fit.max()) >= n_fit:
             raise ValueError("pair index outside the molecule tables")
     if shape:
+        esp_self = m == _lib.MODE_ESP
         if ref_self is None:
-            ref_self = kernels.self_overlap(ref, alpha, m == _lib.MODE_ESP, lam)
+            ref_self = kernels.self_overlap(ref, alpha, esp_self, lam if esp_self else None)
         if fit_self is None:
-            fit_self = kernels.self_overlap(fit, alpha, m == _lib.MODE_ESP, lam)
+            fit_self = kernels.self_overlap(fit, alpha, esp_self, lam if esp_self else None)
     if pharm:
         if m == _lib.MODE_PHARM:
             if ref_self is None:
@@ -194,6 +218,22 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
     d.accumulate = int(accumulate)
     d.kernel_variant = int(kernel_variant)
     d.pharm_extended = int(pharm_extended)
+    if combo:
+        rr = ref_radii.to(_f32).contiguous()
+        fr = fit_radii.to(_f32).contiguous()
+        d.ref_atoms, d.ref_radii, d.ref_atom_off = (ptr(ref_atoms.pts, _f32), ptr(rr, _f32),
+                                                    ptr(ref_atoms.off, _i32))
+        d.fit_atoms, d.fit_radii, d.fit_atom_off = (ptr(fit_atoms.pts, _f32), ptr(fr, _f32),
+                                                    ptr(fit_atoms.off, _i32))
+        d.ref_surf, d.ref_surf_off = ptr(ref_surf.pts, _f32), ptr(ref_surf.off, _i32)
+        d.fit_surf, d.fit_surf_off = ptr(fit_surf.pts, _f32), ptr(fit_surf.off, _i32)
+        d.max_ref_atoms, d.max_fit_atoms = ref_atoms.max_points, fit_atoms.max_points
+        d.max_ref_surf, d.max_fit_surf = ref_surf.max_points, fit_surf.max_points
+        d.esp_inv_lam = 1.0 / (LAM_SCALING * lam)
+        d.coulomb = COULOMB_SCALING
+        d.probe_radius = float(probe_radius)
+        d.esp_weight = float(esp_weight)
+        d.esp_stride = int(esp_stride)
     if similarity != "tanimoto":
         d.similarity, d.tversky_sigma = 1, TVERSKY_SIGMA[similarity]
     d.scratch = ptr(scratch, _i32)
@@ -363,6 +403,63 @@ def coarse_fine_pharm_align_many(anchors_1, anchors_2, vectors_1, vectors_2, typ
     R = _quat_rot(q)
     t = t - torch.einsum('bij,bj->bi', R, c_fit) + c_ref
     return sc, q, t
+
+
+def coarse_fine_esp_combo_align_many(centers_w_H_1, centers_w_H_2, centers_1, centers_2,
+                                     points_1, points_2, partial_charges_1, partial_charges_2,
+                                     point_charges_1, point_charges_2, radii_1, radii_2,
+                                     VAA=None, VBB=None, *, alpha: float, lam: float = 0.001,
+                                     probe_radius: float = 1.0, esp_weight: float = 0.5,
+                                     num_seeds: int = 50, trans_centers=None,
+                                     trans_centers_real=None, num_repeats_per_trans: int = 10,
+                                     topk: int = 30, steps_fine: int = 100, lr: float = 0.075,
+                                     N_real_centers=None, M_real_centers=None,
+                                     N_real_atoms_w_H_1=None, M_real_atoms_w_H_2=None,
+                                     N_real_surf_1=None, M_real_surf_2=None,
+                                     early_stop_patience: int = 5, early_stop_tol: float = 1e-5,
+                                     seeds: Optional[tuple] = None, esp_stride: int = 1,
+                                     **tile):
+    """vol_and_surf_esp alignment with the reference signature (esp_combo.py:334-595).
+
+    The pose follows the volumetric shape gradient of the centres, scaled by (1 - esp_weight);
+    the tracked score is esp_weight * ShaEP ESP similarity (surface points of each molecule
+    against the other's atoms with hydrogens) + (1 - esp_weight) * shape Tanimoto.
+    ``esp_stride`` = 1 scores every step as the reference's CUDA-graph loop does; 5 matches its
+    eager loop.  VAA/VBB (shape self overlaps) are recomputed when not given.
+    """
+    if trans_centers is not None:
+        raise NotImplementedError("trans_init is not part of the CUDA backend")
+    K = centers_1.shape[0]
+    dev = centers_1.device
+    cnt = lambda n, x: _default_counts(n, K, x.shape[1], dev)
+    NC, MC = cnt(N_real_centers, centers_1), cnt(M_real_centers, centers_2)
+    NA, MA = cnt(N_real_atoms_w_H_1, centers_w_H_1), cnt(M_real_atoms_w_H_2, centers_w_H_2)
+    NS, MS = cnt(N_real_surf_1, points_1), cnt(M_real_surf_2, points_2)
+    ref = CloudSet.from_padded(centers_1.to(_f32), NC)
+    fit = CloudSet.from_padded(centers_2.to(_f32), MC)
+    ra = CloudSet.from_padded(centers_w_H_1.to(_f32), NA, partial_charges_1)
+    fa = CloudSet.from_padded(centers_w_H_2.to(_f32), MA, partial_charges_2)
+    rrad = _packed_values(radii_1, NA)
+    frad = _packed_values(radii_2, MA)
+    rs = CloudSet.from_padded(points_1.to(_f32), NS, point_charges_1)
+    fs = CloudSet.from_padded(points_2.to(_f32), MS, point_charges_2)
+    pr, pf = _self_pairs(K, dev)
+    if seeds is None:
+        seeds = kernels.seeds(ref, fit, pr, pf, num_seeds)
+    return align_packed("esp_combo", ref=ref, fit=fit, pair_ref=pr, pair_fit=pf,
+                        seed_q=seeds[0], seed_t=seeds[1], steps=steps_fine, lr=lr, alpha=alpha,
+                        lam=lam, ref_self=VAA, fit_self=VBB, ref_atoms=ra, fit_atoms=fa,
+                        ref_radii=rrad, fit_radii=frad, ref_surf=rs, fit_surf=fs,
+                        probe_radius=probe_radius, esp_weight=esp_weight,
+                        esp_stride=esp_stride, **tile)
+
+
+def _packed_values(X, n_real):
+    """(K, N_pad) per-point values -> the packed order of CloudSet.from_padded."""
+    K, npad = X.shape
+    n = torch.as_tensor(n_real, device=X.device).to(torch.int64).clamp(0, npad)
+    mask = torch.arange(npad, device=X.device)[None, :] < n[:, None]
+    return X.to(_f32)[mask].contiguous()
 
 
 def coarse_fine_vol_color_align_many(centers_1, centers_2, ptype_1, ptype_2, anchors_1,

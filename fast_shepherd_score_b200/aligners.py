@@ -38,14 +38,20 @@ def _device_of(pairs) -> torch.device:
 
 
 def _ensure(pairs, attr, src, dtype, device):
-    """p.<attr> as a tensor on `device`, built from p.ref_molec/fit_molec.<src> if absent."""
+    """p.<attr> as a tensor on `device`, built from p.ref_molec/fit_molec.<src> (an attribute
+    name, or a callable of the molecule) if absent."""
     side = "ref_molec" if attr.startswith("_ref_") else "fit_molec"
     out = []
     for p in pairs:
         t = getattr(p, attr, None)
         if t is None:
             mol = getattr(p, side, None)
-            arr = None if mol is None else getattr(mol, src, None)
+            if mol is None:
+                arr = None
+            elif callable(src):
+                arr = src(mol)
+            else:
+                arr = getattr(mol, src, None)
             if arr is None:
                 raise ValueError(f"pair is missing {attr} and {side}.{src}")
             t = torch.as_tensor(np.asarray(arr), dtype=dtype)
@@ -205,6 +211,54 @@ def _align_batch_vol_esp(pairs, *, lam: float, alpha: float = 0.81, trans_init: 
     fit, fi = _cloud_set(pts_f, ch_f, device=dev)
     return _align(pairs, "vol_esp", ref, fit, None, None, ri, fi, alpha=alpha, lam=lam,
                   steps=steps_fine, lr=lr, num_seeds=num_repeats or seeds_for("vol_esp"))
+
+
+def _conformer_positions(mol):
+    """All-atom (with hydrogens) positions of a molecule's RDKit conformer."""
+    rd = getattr(mol, "mol", None)
+    return None if rd is None else rd.GetConformer().GetPositions()
+
+
+def _align_batch_vol_and_surf_esp(pairs, *, alpha: float, lam: float = 0.001,
+                                  probe_radius: float = 1.0, esp_weight: float = 0.5,
+                                  trans_init: bool = False, num_repeats: int = 50,
+                                  num_repeats_per_trans: int = 10, topk: int = 30,
+                                  steps_fine: int = 100, lr: float = 0.075,
+                                  esp_stride: int = 1):
+    """ShaEP-style combo (aligners.py:651-864): shape centres (heavy atoms when alpha is 0.81,
+    else surface points) steer the pose; the score adds the surface ESP comparison against the
+    other molecule's atoms with hydrogens.  Writes transform_vol_and_surf_esp /
+    sim_aligned_vol_and_surf_esp."""
+    if not pairs:
+        return
+    if trans_init:
+        raise NotImplementedError("trans_init=True is not part of the CUDA backend")
+    dev = _device_of(pairs)
+    sets = {}
+    for side in ("ref", "fit"):
+        surf = _ensure(pairs, f"_{side}_surf_t", "surf_pos", _f32, dev)
+        esp = _ensure(pairs, f"_{side}_surf_esp_t", "surf_esp", _f32, dev)
+        wh = _ensure(pairs, f"_{side}_centers_w_H_t", _conformer_positions, _f32, dev)
+        q = _ensure(pairs, f"_{side}_partial_t", "partial_charges", _f32, dev)
+        rad = _ensure(pairs, f"_{side}_radii_t", "radii", _f32, dev)
+        cent = (_ensure(pairs, f"_{side}_xyz_t", "atom_pos", _f32, dev) if alpha == 0.81
+                else surf)
+        dd = _shared(surf) and _shared(wh) and _shared(cent)
+        centres, idx = _cloud_set(cent, device=dev, dedup=dd)
+        atoms, _ = _cloud_set(wh, q, device=dev, dedup=dd)
+        surfs, _ = _cloud_set(surf, esp, device=dev, dedup=dd)
+        radii = torch.cat([r.reshape(-1).to(_f32) for r in (rad[:1] if dd else rad)]).to(dev)
+        sets[side] = (centres, idx, atoms, radii, surfs)
+    (ref, ri, ra, rr, rs), (fit, fi, fa, fr, fs) = sets["ref"], sets["fit"]
+    return _align(pairs, "vol_and_surf_esp", ref, fit, None, None, ri, fi, alpha=alpha, lam=lam,
+                  steps=steps_fine, lr=lr,
+                  num_seeds=num_repeats or seeds_for("vol_and_surf_esp"),
+                  ref_atoms=ra, fit_atoms=fa, ref_radii=rr, fit_radii=fr, ref_surf=rs,
+                  fit_surf=fs, probe_radius=probe_radius, esp_weight=esp_weight,
+                  esp_stride=esp_stride)
+
+
+_align_batch_esp_combo = _align_batch_vol_and_surf_esp
 
 
 def _pharm_inputs(pairs, dev, with_vectors=True):

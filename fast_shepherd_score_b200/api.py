@@ -34,7 +34,8 @@ LAM_SCALING = al.LAM_SCALING
 SHAPE_MODES = ("vol", "surf", "vol_esp", "surf_esp")
 PHARM_MODES = ("pharm",)
 COMBO_MODES = ("vol_color", "vol_pharm")
-MODES = SHAPE_MODES + PHARM_MODES + COMBO_MODES
+ESP_COMBO_MODES = ("vol_and_surf_esp",)
+MODES = SHAPE_MODES + PHARM_MODES + COMBO_MODES + ESP_COMBO_MODES
 
 
 @dataclass
@@ -186,6 +187,14 @@ def align_device(mode, ref: Optional[CloudSet], fit: Optional[CloudSet],
     ``similarity`` / ``extended_points`` / ``only_extended`` apply to mode "pharm"."""
     if mode != "pharm" and (similarity != "tanimoto" or extended_points or only_extended):
         raise ValueError("similarity and extended points apply to mode 'pharm' only")
+    if mode in ESP_COMBO_MODES:
+        # shape centres steer the pose; tile holds the ESP-comparison sets and parameters
+        if seeds is None:
+            seeds = K.seeds(ref, fit, pair_ref, pair_fit, num_seeds)
+        return al.align_packed("esp_combo", ref=ref, fit=fit, pair_ref=pair_ref,
+                               pair_fit=pair_fit, seed_q=seeds[0], seed_t=seeds[1],
+                               steps=steps, lr=lr, alpha=alpha, lam=lam, ref_self=ref_self,
+                               fit_self=fit_self, **tile)
     if mode in SHAPE_MODES:
         esp = mode in ("vol_esp", "surf_esp")
         kl = _kernel_lam(mode, lam) if esp else None

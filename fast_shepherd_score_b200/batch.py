@@ -120,6 +120,28 @@ class MoleculePairBatch:
 
     align_with_esp = align_with_surf_esp   # legacy name (accel/_modes.py LEGACY_MODE_ALIASES)
 
+    def align_with_vol_and_surf_esp(self, alpha: float, lam: float = 0.001,
+                                    probe_radius: float = 1.0, esp_weight: float = 0.5,
+                                    num_repeats: int = None, trans_init: bool = False,
+                                    lr: float = 0.1, max_num_steps: int = None,
+                                    verbose: bool = False, backend: Optional[str] = None,
+                                    return_aligned: bool = False, esp_stride: int = 1):
+        """ShaEP-style combo (_batch.py:1030): the shape centres steer the pose, the score adds
+        the surface ESP comparison.  ``esp_stride`` (this backend's knob) tracks the combo
+        score every step by default, as the reference's CUDA-graph loop; 5 matches its eager
+        loop."""
+        _resolve(backend)
+        if trans_init:
+            raise NotImplementedError("trans_init=True is not part of the CUDA backend")
+        sc = A._align_batch_vol_and_surf_esp(
+            self.pairs, alpha=alpha, lam=lam, probe_radius=probe_radius, esp_weight=esp_weight,
+            num_repeats=self._seeds("vol_and_surf_esp", num_repeats),
+            steps_fine=self._steps("vol_and_surf_esp", max_num_steps), lr=lr,
+            esp_stride=esp_stride)
+        return self._finish("vol_and_surf_esp", sc, "_fit_surf_t", return_aligned, verbose)
+
+    align_with_esp_combo = align_with_vol_and_surf_esp   # legacy name
+
     def align_with_vol_color(self, color_weight: float = 0.5, alpha: float = 0.81,
                              num_repeats: int = None, trans_init: bool = False, lr: float = 0.1,
                              max_num_steps: int = None, verbose: bool = False,

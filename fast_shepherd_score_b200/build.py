@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libfss_cuda.so")
 SOURCES = ["fss_capi.cu", "fss_align.cu", "fss_align_shape.cu", "fss_align_esp.cu",
-           "fss_align_pharm.cu", "fss_eval.cu", "fss_seeds.cu", "fss_score.cu", "fss_probe.cu",
+           "fss_align_pharm.cu", "fss_align_combo.cu", "fss_eval.cu", "fss_seeds.cu", "fss_score.cu", "fss_probe.cu",
            "fss_static.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

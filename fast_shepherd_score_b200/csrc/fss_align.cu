@@ -135,7 +135,7 @@ void auto_tile(int mode, int max_fit, int n_starts, int* lpp, int* chunks) {
 
 int align_launch(const fss_align_desc* d, cudaStream_t st) {
   if (!d) return set_error(FSS_ERR_INVALID, "fss_align: null descriptor");
-  if (d->mode < FSS_MODE_SHAPE || d->mode > FSS_MODE_SHAPE_COLOR)
+  if (d->mode < FSS_MODE_SHAPE || d->mode > FSS_MODE_ESP_COMBO)
     return set_error(FSS_ERR_INVALID, "fss_align: unknown mode");
   if (d->n_pairs < 0 || d->n_starts <= 0 || d->steps < 0)
     return set_error(FSS_ERR_INVALID, "fss_align: needs n_pairs >= 0, n_starts > 0, steps >= 0");
@@ -143,7 +143,17 @@ int align_launch(const fss_align_desc* d, cudaStream_t st) {
       !d->pair_ref || !d->pair_fit)
     return set_error(FSS_ERR_INVALID, "fss_align: missing pair, seed, row or scratch buffer");
   const bool shape = d->mode != FSS_MODE_PHARM;
-  const bool pharm = d->mode >= FSS_MODE_PHARM;
+  const bool pharm = d->mode == FSS_MODE_PHARM || d->mode == FSS_MODE_SHAPE_PHARM ||
+                     d->mode == FSS_MODE_SHAPE_COLOR;
+  const bool combo = d->mode == FSS_MODE_ESP_COMBO;
+  if (combo && (!d->ref_atoms || !d->ref_radii || !d->ref_atom_off || !d->fit_atoms ||
+                !d->fit_radii || !d->fit_atom_off || !d->ref_surf || !d->ref_surf_off ||
+                !d->fit_surf || !d->fit_surf_off))
+    return set_error(FSS_ERR_INVALID, "fss_align: ESP-comparison channel (atoms, radii, "
+                                      "surfaces) missing");
+  if (combo && (!(d->esp_inv_lam > 0.f) || !(d->probe_radius >= 0.f) || d->esp_stride < 0))
+    return set_error(FSS_ERR_INVALID, "fss_align: ESP comparison needs esp_inv_lam > 0, "
+                                      "probe_radius >= 0, esp_stride >= 0");
   if (shape && (!d->ref_pts || !d->ref_off || !d->fit_pts || !d->fit_off || !d->ref_self ||
                 !d->fit_self))
     return set_error(FSS_ERR_INVALID, "fss_align: shape channel clouds / self overlaps missing");
@@ -158,9 +168,13 @@ int align_launch(const fss_align_desc* d, cudaStream_t st) {
   if (shape && !(d->alpha > 0.f)) return set_error(FSS_ERR_INVALID, "fss_align: alpha must be > 0");
   const int maxN = shape ? d->max_ref_points : 0, maxM = shape ? d->max_fit_points : 0;
   const int maxNp = pharm ? d->max_ref_features : 0, maxMp = pharm ? d->max_fit_features : 0;
-  if (maxN < 0 || maxM < 0 || maxNp < 0 || maxMp < 0)
+  const int maxNa = combo ? d->max_ref_atoms : 0, maxMa = combo ? d->max_fit_atoms : 0;
+  const int maxNs = combo ? d->max_ref_surf : 0, maxMs = combo ? d->max_fit_surf : 0;
+  if (maxN < 0 || maxM < 0 || maxNp < 0 || maxMp < 0 || maxNa < 0 || maxMa < 0 || maxNs < 0 ||
+      maxMs < 0)
     return set_error(FSS_ERR_INVALID, "fss_align: negative extents");
-  if (maxN > kMaxPoints || maxM > kMaxPoints || maxNp > kMaxPoints || maxMp > kMaxPoints)
+  if (maxN > kMaxPoints || maxM > kMaxPoints || maxNp > kMaxPoints || maxMp > kMaxPoints ||
+      maxNa > kMaxPoints || maxMa > kMaxPoints || maxNs > kMaxPoints || maxMs > kMaxPoints)
     return set_error(FSS_ERR_UNSUPPORTED, "fss_align: more than fss_max_points() points in a molecule");
 
   cudaError_t ce = cudaMemsetAsync(d->scratch, 0, 2 * sizeof(int32_t), st);
@@ -183,14 +197,18 @@ int align_launch(const fss_align_desc* d, cudaStream_t st) {
                                       "mode PHARM, tversky_sigma in [0, 1])");
   if (tc && d->lanes_per_pose != 0 && d->lanes_per_pose != 32)
     return set_error(FSS_ERR_INVALID, "fss_align: tensor-core sums use 32 lanes per pose");
-  if (d->kernel_variant < 0 || d->kernel_variant > 3 || (!tc_mode && d->kernel_variant > 1))
+  if (d->kernel_variant < 0 || d->kernel_variant > 3 ||
+      (pharm && d->kernel_variant > 1) || (combo && d->kernel_variant == 2))
     return set_error(FSS_ERR_INVALID, "fss_align: kernel_variant must be 0..3 (0 or 1 for "
-                                      "modes with a pharmacophore channel)");
+                                      "modes with a pharmacophore channel, 0, 1 or 3 for "
+                                      "ESP_COMBO)");
   // automatic code variant: wide register tile for large clouds, roomy registers for small
   const int var = d->kernel_variant > 0 ? d->kernel_variant - 1
-                  : !tc_mode ? 0 : (maxM >= 64 ? 1 : 2);
+                  : pharm ? 0 : combo ? 2 : (maxM >= 64 ? 1 : 2);
   int lpp = tc ? 32 : d->lanes_per_pose, chunks = d->chunks;
-  auto_tile(d->mode, shape ? maxM : maxMp, d->n_starts, &lpp, &chunks);
+  // the ESP comparison splits surface points over the lanes, so it sizes the lanes
+  auto_tile(d->mode, combo ? std::max(maxNs, maxMs) : shape ? maxM : maxMp, d->n_starts, &lpp,
+            &chunks);
   if (chunks < 1 || chunks > d->n_starts)
     return set_error(FSS_ERR_INVALID, "fss_align: chunks must be in [1, n_starts]");
   const int ppc = (d->n_starts + chunks - 1) / chunks;
@@ -223,6 +241,19 @@ int align_launch(const fss_align_desc* d, cudaStream_t st) {
   p.aKc = (float)(alpha * std::pow(M_PI, 1.5) / std::pow(2.0 * alpha, 1.5));
   p.w = d->color_weight; p.lr = d->lr;
   p.sigma = d->similarity == 1 ? d->tversky_sigma : -1.f;
+  if (combo) {
+    p.ref_atoms = reinterpret_cast<const float4*>(d->ref_atoms); p.ref_radii = d->ref_radii;
+    p.ref_atom_off = d->ref_atom_off;
+    p.fit_atoms = reinterpret_cast<const float4*>(d->fit_atoms); p.fit_radii = d->fit_radii;
+    p.fit_atom_off = d->fit_atom_off;
+    p.ref_surf = reinterpret_cast<const float4*>(d->ref_surf); p.ref_surf_off = d->ref_surf_off;
+    p.fit_surf = reinterpret_cast<const float4*>(d->fit_surf); p.fit_surf_off = d->fit_surf_off;
+    p.maxNa = maxNa; p.maxMa = maxMa; p.maxNs = maxNs; p.maxMs = maxMs;
+    p.coulomb = d->coulomb; p.probe = d->probe_radius;
+    p.nkl = (float)(-(double)d->esp_inv_lam * 1.4426950408889634);
+    p.esp_w = d->esp_weight;
+    p.esp_stride = d->esp_stride > 0 ? d->esp_stride : 1;
+  }
   p.tab = make_pharm_tables(d->mode != FSS_MODE_SHAPE_COLOR);
   p.row_score = d->row_score; p.row_q = d->row_q; p.row_t = d->row_t;
   p.counter = d->scratch;
@@ -232,11 +263,16 @@ int align_launch(const fss_align_desc* d, cudaStream_t st) {
       tc ? sizeof(float4) * (kMmaP4PerBlock * nb + maxM) +
                sizeof(float2) * (kMmaC2PerBlock + kMmaQ2PerBlock) * nb + 16
          : sizeof(float4) * (2 * (size_t)maxN + maxM + 2 * (size_t)maxNp + 2 * (size_t)maxMp) +
-               sizeof(float2) * (d->mode == FSS_MODE_ESP ? (size_t)maxN : 0) + 16;
+               sizeof(float2) * (d->mode == FSS_MODE_ESP ? (size_t)maxN : 0) +
+               sizeof(float4) * ((size_t)maxNs + maxMs + maxNa + maxMa) +
+               sizeof(float) * ((size_t)maxNa + maxMa) + 16;
   int rc;
   switch (d->mode) {
     case FSS_MODE_SHAPE: rc = launch_align_shape(lpp, tc, var, p, threads, d->cta_per_sm, smem, st); break;
     case FSS_MODE_ESP: rc = launch_align_esp(lpp, tc, var, p, threads, d->cta_per_sm, smem, st); break;
+    case FSS_MODE_ESP_COMBO:
+      rc = launch_align_combo(lpp, var, p, threads, d->cta_per_sm, smem, st);
+      break;
     default:
       rc = launch_align_pharm(d->mode, lpp, d->pharm_extended, p, threads, d->cta_per_sm, smem,
                               st);

@@ -35,6 +35,14 @@ struct AlignParams {
   const float* seed_q; const float* seed_t;
   float alpha, k, e, inv2k, Kc, aKc, w, lr;
   float sigma;  // pharm mode: Tversky sigma (>= 0) or Tanimoto (< 0)
+  // vol_and_surf_esp: atoms with H (x, y, z, q) + radii, surfaces (x, y, z, pe)
+  const float4* ref_atoms; const float* ref_radii; const int* ref_atom_off;
+  const float4* fit_atoms; const float* fit_radii; const int* fit_atom_off;
+  const float4* ref_surf; const int* ref_surf_off;
+  const float4* fit_surf; const int* fit_surf_off;
+  int maxNa, maxMa, maxNs, maxMs;
+  float coulomb, probe, nkl, esp_w;  // nkl = -log2(e) / (LAM_SCALING * lam)
+  int esp_stride;
   PharmTables tab;
   float* row_score; float* row_q; float* row_t;
   int* counter;
@@ -63,8 +71,9 @@ template <int LPP, int MODE, bool TC, int VAR, int EXT = 0>
 __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
     align_kernel(const AlignParams p) {
   using V = AlignVariant<VAR>;
+  constexpr bool kCombo = MODE == FSS_MODE_ESP_COMBO;
   constexpr bool kShape = MODE == FSS_MODE_SHAPE || MODE == FSS_MODE_ESP ||
-                          MODE == FSS_MODE_SHAPE_PHARM || MODE == FSS_MODE_SHAPE_COLOR;
+                          MODE == FSS_MODE_SHAPE_PHARM || MODE == FSS_MODE_SHAPE_COLOR || kCombo;
   constexpr bool kEsp = MODE == FSS_MODE_ESP;
   constexpr bool kPharm = MODE == FSS_MODE_PHARM || MODE == FSS_MODE_SHAPE_PHARM ||
                           MODE == FSS_MODE_SHAPE_COLOR;
@@ -82,6 +91,13 @@ __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
   float2* sQc = reinterpret_cast<float2*>(sFV + p.maxMp);
   float2* sCm = reinterpret_cast<float2*>(sB + p.maxM);
   float2* sQm = sCm + kMmaC2PerBlock * nbMax;
+  // vol_and_surf_esp channel: surfaces, atoms with H, (radius + probe)^2
+  float4* sSA = sFV + p.maxMp;
+  float4* sSB = sSA + p.maxNs;
+  float4* sAA = sSB + p.maxMs;
+  float4* sAB = sAA + p.maxNa;
+  float* sRA2 = reinterpret_cast<float*>(sAB + p.maxMa);
+  float* sRB2 = sRA2 + p.maxNa;
   __shared__ float red[96];
   __shared__ int s_item;
 
@@ -111,8 +127,16 @@ __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
       Np = p.ref_ph_off[ri + 1] - rp0;
       Mp = p.fit_ph_off[fi + 1] - fp0;
     }
+    int Na = 0, Ma = 0, Ns = 0, Ms = 0, ra0 = 0, fa0 = 0, rs0 = 0, fs0 = 0;
+    if (kCombo) {
+      ra0 = p.ref_atom_off[ri]; fa0 = p.fit_atom_off[fi];
+      rs0 = p.ref_surf_off[ri]; fs0 = p.fit_surf_off[fi];
+      Na = p.ref_atom_off[ri + 1] - ra0; Ma = p.fit_atom_off[fi + 1] - fa0;
+      Ns = p.ref_surf_off[ri + 1] - rs0; Ms = p.fit_surf_off[fi + 1] - fs0;
+    }
     if (N < 0 || M < 0 || Np < 0 || Mp < 0 || N > p.maxN || M > p.maxM || Np > p.maxNp ||
-        Mp > p.maxMp) {
+        Mp > p.maxMp || Na < 0 || Ma < 0 || Ns < 0 || Ms < 0 || Na > p.maxNa ||
+        Ma > p.maxMa || Ns > p.maxNs || Ms > p.maxMs) {
       // larger than the tiles this launch was sized for: flag it, leave its rows untouched
       if (tid == 0) atomicOr(p.counter + 1, 1);
       __syncthreads();
@@ -124,6 +148,25 @@ __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
       if constexpr (TC) stage_ref_mma<kEsp>(p.ref_pts + r0, N, c, p.k, p.e, sP, sQm, sCm);
       else stage_ref<kEsp>(p.ref_pts + r0, N, c, p.k, p.e, sP, sQc);
       stage_copy(p.fit_pts + f0, M, sB);
+    }
+    if (kCombo) {
+      // reference-side arrays move into the centred frame of the shape channel
+      for (int i = tid; i < Ns; i += blockDim.x) {
+        const float4 v = p.ref_surf[rs0 + i];
+        sSA[i] = make_float4(v.x - c.x, v.y - c.y, v.z - c.z, v.w);
+      }
+      for (int i = tid; i < Na; i += blockDim.x) {
+        const float4 v = p.ref_atoms[ra0 + i];
+        sAA[i] = make_float4(v.x - c.x, v.y - c.y, v.z - c.z, v.w);
+        const float r = p.ref_radii[ra0 + i] + p.probe;
+        sRA2[i] = r * r;
+      }
+      stage_copy(p.fit_surf + fs0, Ms, sSB);
+      stage_copy(p.fit_atoms + fa0, Ma, sAB);
+      for (int i = tid; i < Ma; i += blockDim.x) {
+        const float r = p.fit_radii[fa0 + i] + p.probe;
+        sRB2[i] = r * r;
+      }
     }
     if (kPharm) {
       if (!kShape) c = block_centroid(p.ref_anc + rp0, Np, red);
@@ -177,6 +220,18 @@ __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
           if (kShape) step_combo(s, rs, Us, rc, Uc, p.w, p.lr);
           else if (p.sigma >= 0.f) step_tversky(s, rc, Dtv, p.lr);
           else step_single(s, rc, Us, p.lr);
+        } else if (kCombo) {
+          const bool scored = step % p.esp_stride == 0 || step == p.steps - 1;
+          float esp = 0.f;
+          if (scored) {
+            esp = esp_side<LPP, true>(sSA, Ns, sAB, sRB2, Ma, lane, R, s.t[0], s.t[1], s.t[2],
+                                      p.coulomb, p.nkl) +
+                  esp_side<LPP, false>(sSB, Ms, sAA, sRA2, Na, lane, R, s.t[0], s.t[1],
+                                       s.t[2], p.coulomb, p.nkl);
+#pragma unroll
+            for (int o = LPP / 2; o > 0; o >>= 1) esp += __shfl_xor_sync(0xffffffffu, esp, o);
+          }
+          step_esp_combo(s, rs, Us, esp, (float)(Ns + Ms), p.esp_w, scored, p.lr);
         } else {
           step_single(s, rs, Us, p.lr);
         }
@@ -234,5 +289,7 @@ int launch_align_esp(int lpp, bool tc, int var, const AlignParams& prm, int thre
                      size_t smem, cudaStream_t st);
 int launch_align_pharm(int mode, int lpp, int ext, const AlignParams& prm, int threads,
                        int cps, size_t smem, cudaStream_t st);
+int launch_align_combo(int lpp, int var, const AlignParams& prm, int threads, int cps,
+                       size_t smem, cudaStream_t st);
 
 }  // namespace fss

@@ -234,6 +234,67 @@ __device__ __forceinline__ void step_tversky(PoseState& s, const Reduced& m, flo
   adam_tail(s, score, gq, gt, lr);
 }
 
+// vol_and_surf_esp step (accel/drivers/esp_combo.py:497-595): the pose follows the shape
+// gradient scaled by (1 - w); on scored steps the tracked score is
+// w * (esp1 + esp2) / n_surf + (1 - w) * V / (U - V).  Unscored steps never update the best.
+__device__ __forceinline__ void step_esp_combo(PoseState& s, const Reduced& m, float U,
+                                               float esp_sum, float n_surf, float w,
+                                               bool scored, float lr) {
+  float vs, scale;
+  tanimoto(m.v, U, vs, scale);
+  const float score = scored ? w * (esp_sum / n_surf) + (1.f - w) * vs : -INFINITY;
+  const float c = -scale * (1.f - w);
+  float gq[4], gt[3];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) gq[i] = c * m.dq[i];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) gt[i] = c * m.f[i];
+  adam_tail(s, score, gq, gt, lr);
+}
+
+// One side of the ShaEP ESP comparison for one pose (cpu.py:237-261, esp_triton.py:265-346):
+//   sum over field points i of exp(-(pe_i - coulomb * sum_m q_m / max(d_im, 1e-6))^2 / lam')
+// skipping points within radius_m + probe of any atom.  Field points (x, y, z, pe) and atoms
+// (x, y, z, q) live in different frames: TO_BODY maps a field point of the reference frame into
+// the fit body frame (u = R^T (p - t)), otherwise a body-frame field point into the reference
+// frame (u = R p + t).  rp2 holds (radius + probe)^2 per atom.  Lanes split the field points;
+// returns this lane's partial sum.
+template <int LPP, bool TO_BODY>
+__device__ __forceinline__ float esp_side(const float4* __restrict__ field, int n,
+                                          const float4* __restrict__ atoms,
+                                          const float* __restrict__ rp2, int m, int lane,
+                                          const Rot& R, float tx, float ty, float tz,
+                                          float coulomb, float nkl) {
+  float total = 0.f;
+  for (int i = lane; i < n; i += LPP) {
+    const float4 f = field[i];
+    float ux, uy, uz;
+    if (TO_BODY) {
+      const float px = f.x - tx, py = f.y - ty, pz = f.z - tz;
+      ux = fmaf(R.r[0], px, fmaf(R.r[3], py, R.r[6] * pz));
+      uy = fmaf(R.r[1], px, fmaf(R.r[4], py, R.r[7] * pz));
+      uz = fmaf(R.r[2], px, fmaf(R.r[5], py, R.r[8] * pz));
+    } else {
+      const float3 p3 = rot_apply(R, f.x, f.y, f.z);
+      ux = p3.x + tx; uy = p3.y + ty; uz = p3.z + tz;
+    }
+    float esp = 0.f;
+    bool blocked = false;
+    for (int j = 0; j < m; ++j) {
+      const float4 a = atoms[j];
+      const float dx = ux - a.x, dy = uy - a.y, dz = uz - a.z;
+      const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      esp = fmaf(a.w, fminf(rsqrtf(d2), 1e6f), esp);   // 1 / max(d, 1e-6)
+      blocked = blocked || d2 < rp2[j];
+    }
+    if (!blocked) {
+      const float diff = fmaf(-coulomb, esp, f.w);
+      total += ex2(nkl * diff * diff);
+    }
+  }
+  return total;
+}
+
 // Two-channel step (1-w) * shape + w * pharm, the joint gradient of cpu_fused.py:111-167.
 __device__ __forceinline__ void step_combo(PoseState& s, const Reduced& ms, float Us,
                                            const Reduced& mc, float Uc, float w, float lr) {

@@ -23,8 +23,9 @@ MODE_SEEDS = {"vol": 10, "surf": 8, "surf_esp": 8, "vol_esp": 16, "vol_and_surf_
               "pharm": 32, "vol_color": 16, "vol_pharm": 16}
 MODE_STEPS = {"vol": 30, "surf": 40, "surf_esp": 40, "vol_esp": 50, "vol_and_surf_esp": 60,
               "pharm": 50, "vol_color": 40, "vol_pharm": 40}
-# modes the CUDA backend implements (vol_and_surf_esp's ShaEP comparison is not on the path)
-CUDA_MODES = ("vol", "vol_esp", "surf", "surf_esp", "pharm", "vol_color", "vol_pharm")
+# modes the CUDA backend implements
+CUDA_MODES = ("vol", "vol_esp", "surf", "surf_esp", "vol_and_surf_esp", "pharm", "vol_color",
+              "vol_pharm")
 
 
 def canonical(mode: str) -> str:

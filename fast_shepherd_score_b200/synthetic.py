@@ -194,3 +194,47 @@ def library_on_device(n_mol, seed=5, device="cuda", atom_lo=15, atom_hi=60, ph_l
     pc = npf.cpu().numpy().astype(np.int64)
     pharm = PharmSet(anc, vec, torch.from_numpy(_offsets(pc)).to(dev), pc, int(pc.max()))
     return atoms, pharm
+
+
+COULOMB_SCALING = 1e4 / (4 * 55.263 * np.pi)   # eV*A/e^2 (score/constants.py:16)
+
+
+def esp_combo_molecules(n_mol, rng, heavy_lo=10, heavy_hi=25, surf_lo=100, surf_hi=200,
+                        h_per_heavy=0.8, charge_sd=0.2):
+    """Molecules for the ShaEP combo mode: heavy-atom shape centres (uniform in a ball, >= 1.2 A
+    apart), the same atoms plus hydrogens 1.1 A from random heavy atoms (the "atoms with H"),
+    net-neutral partial charges N(0, 0.2^2), van der Waals radii (1.2 A for H, U(1.5, 1.9) for
+    heavy atoms), surface points on a sphere 2 A outside the farthest atom, and the
+    molecule's own Coulomb potential at those points (COULOMB_SCALING * sum_m q_m / d)."""
+    nh = rng.integers(heavy_lo, heavy_hi + 1, n_mol)
+    heavy = ball_clouds(rng, nh, radius=4.0)
+    out = []
+    for X in heavy:
+        n_h = int(round(h_per_heavy * len(X)))
+        anchor = rng.integers(0, len(X), n_h)
+        u = rng.standard_normal((n_h, 3))
+        u /= np.linalg.norm(u, axis=1, keepdims=True)
+        H = X[anchor] + 1.1 * u
+        atoms = np.concatenate([X, H]).astype(np.float32)
+        q = charge_sd * rng.standard_normal(len(atoms))
+        q -= q.mean()
+        radii = np.concatenate([rng.uniform(1.5, 1.9, len(X)), np.full(n_h, 1.2)])
+        ns = int(rng.integers(surf_lo, surf_hi + 1))
+        v = rng.standard_normal((ns, 3))
+        v /= np.linalg.norm(v, axis=1, keepdims=True)
+        c = atoms.mean(0)
+        rad = float(np.linalg.norm(atoms - c, axis=1).max()) + 2.0
+        surf = (c + rad * v).astype(np.float32)
+        d = np.linalg.norm(surf[:, None, :].astype(np.float64) - atoms[None].astype(np.float64),
+                           axis=-1)
+        esp = COULOMB_SCALING * (q[None, :] / np.maximum(d, 1e-6)).sum(1)
+        out.append(dict(centers=X.astype(np.float32), atoms=atoms,
+                        charges=q.astype(np.float32), radii=radii.astype(np.float32),
+                        surf=surf, surf_esp=esp.astype(np.float32)))
+    return out
+
+
+def esp_combo_pairs(n_pairs, seed=6, **kw):
+    """Pairs (ref list, fit list) of :func:`esp_combo_molecules`."""
+    rng = np.random.default_rng(seed)
+    return esp_combo_molecules(n_pairs, rng, **kw), esp_combo_molecules(n_pairs, rng, **kw)

@@ -42,7 +42,10 @@ enum fss_mode {
   FSS_MODE_ESP = 1,        /* vol_esp / surf_esp: charge-weighted shape Tanimoto */
   FSS_MODE_PHARM = 2,      /* pharm: directional typed pharmacophore Tanimoto */
   FSS_MODE_SHAPE_PHARM = 3,/* (1-w) shape + w directional pharm, one shared pose */
-  FSS_MODE_SHAPE_COLOR = 4 /* vol_color: (1-w) shape + w directionless colour */
+  FSS_MODE_SHAPE_COLOR = 4,/* vol_color: (1-w) shape + w directionless colour */
+  FSS_MODE_ESP_COMBO = 5   /* vol_and_surf_esp: pose steered by the shape gradient, score
+                            * w * ShaEP ESP comparison + (1-w) shape Tanimoto
+                            * (accel/drivers/esp_combo.py:334-595) */
 };
 
 /* Library identification. */
@@ -166,6 +169,21 @@ typedef struct fss_align_desc {
   float tversky_sigma;       /* Tversky D = sigma V_AA + (1 - sigma) V_BB, sigma in [0, 1]
                               * (accel/drivers/pharm.py:40: tversky 0.95, tversky_ref 1.0,
                               * tversky_fit 0.05) */
+  /* ShaEP ESP channel of mode ESP_COMBO: atoms with hydrogens (x, y, z, partial charge) with
+   * van der Waals radii, and surface points (x, y, z, ESP at the point), packed per molecule
+   * with int32 prefix offsets like the shape clouds (the shape channel uses ref_pts/fit_pts
+   * as the volumetric centres) */
+  const float *ref_atoms; const float *ref_radii; const int32_t *ref_atom_off;
+  const float *fit_atoms; const float *fit_radii; const int32_t *fit_atom_off;
+  const float *ref_surf; const int32_t *ref_surf_off;
+  const float *fit_surf; const int32_t *fit_surf_off;
+  int32_t max_ref_atoms, max_fit_atoms, max_ref_surf, max_fit_surf;
+  float esp_inv_lam;         /* 1 / (LAM_SCALING * lam) (esp_triton.py:378) */
+  float coulomb;             /* COULOMB_SCALING, score/constants.py:16 */
+  float probe_radius;        /* a surface point within radius + probe of an atom is masked */
+  float esp_weight;          /* w of the combo score */
+  int32_t esp_stride;        /* the combo score is tracked on steps that are multiples of
+                              * esp_stride and on the last step (0 or 1: every step) */
   /* scratch: two device int32 -- [0] work counter, [1] status flags (bit 0: a pair was
    * larger than the max_* extents).  The launch zeroes both on `stream`. */
   int32_t *scratch;

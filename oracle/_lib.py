@@ -45,6 +45,14 @@ def lib():
                                                   ctypes.c_double] + [_vp] * 3 +
             [ctypes.c_int] * 3)
         L.fsso_fine_loop_flat.restype = ctypes.c_int
+        L.fsso_esp_compare.argtypes = [ctypes.c_int] * 3 + [_vp] * 7 + [ctypes.c_double] * 3 + [_vp]
+        L.fsso_esp_compare.restype = None
+        L.fsso_esp_combo_loop.argtypes = (
+            [ctypes.c_int] * 3 + [_vp] * 4 + [ctypes.c_int] * 2 + [_vp] * 8 +
+            [ctypes.c_int] * 2 + [_vp] * 6 + [ctypes.c_double] * 5 + [ctypes.c_int, _vp, _vp, _vp,
+                                                                       ctypes.c_int, ctypes.c_float,
+                                                                       _vp, _vp, _vp, ctypes.c_int])
+        L.fsso_esp_combo_loop.restype = None
         L.fsso_max_threads.restype = ctypes.c_int
         _LIB = L
     return _LIB

@@ -320,3 +320,65 @@ def align_combo(A, B, N_real, M_real, PA, PB, PRV, PFV, PAt, PBt, PN_real, PM_re
         w=w, nthreads=nthreads)
     out = _pick(best, bq, bt, nb, S)
     return (out + ((best, bq, bt),)) if return_rows else out
+
+
+# --------------------------------------------------------------------------------------------
+# vol_and_surf_esp (ShaEP ESP comparison + volumetric shape), accel/drivers/esp_combo.py
+# --------------------------------------------------------------------------------------------
+COULOMB_SCALING = 1e4 / (4 * 55.263 * np.pi)     # score/constants.py:16
+LAM_SCALING = COULOMB_SCALING ** 2               # score/constants.py:17
+
+
+def esp_compare(P, PE, A, Q, R, N_real, M_real, *, lam=0.001, probe_radius=1.0):
+    """esp_comparison_batch (cpu.py:264-285): per row, the masked Gaussian-of-ESP-difference
+    sum over the field points P (K,N,3) with ESP PE (K,N) against atoms A (K,M,3) with charges
+    Q and radii R (K,M), all in one frame."""
+    P, PE, A, Q, R = _f32(P), _f32(PE), _f32(A), _f32(Q), _f32(R)
+    K, Npad, _ = P.shape
+    Mpad = A.shape[1]
+    out = np.zeros(K, np.float64)
+    L = _lib.ptr
+    _lib.lib().fsso_esp_compare(K, Npad, Mpad, L(P), L(PE), L(A), L(Q), L(R),
+                                L(_i32(N_real)), L(_i32(M_real)),
+                                1.0 / (LAM_SCALING * float(lam)), float(COULOMB_SCALING),
+                                float(probe_radius), L(out))
+    return out
+
+
+def align_esp_combo(C1, C2, CN, CM, A1, A2, Q1, Q2, R1, R2, AN, AM, S1, S2, PE1, PE2, SN, SM,
+                    *, alpha=0.81, lam=0.001, probe_radius=1.0, esp_weight=0.5, num_seeds=8,
+                    steps=60, lr=0.1, stride=5, seeds=None, nthreads=None, return_rows=False):
+    """coarse_fine_esp_combo_align_many (esp_combo.py:334-595) without the coarse grid: seeds
+    on the shape centres, the shape gradient scaled by (1 - esp_weight) steers the pose, and the
+    combo score is tracked every `stride` steps and on the last one (the reference's eager loop
+    uses 5; its CUDA-graph loop scores every step, i.e. 1)."""
+    nb = np.asarray(C1).shape[0]
+    if seeds is None:
+        seeds = batched_seeds(C1, C2, CN, CM, num_seeds)
+    qs, ts = seeds
+    S = qs.shape[1]
+    norm = (self_overlap(C1, CN, alpha=alpha, nthreads=nthreads)
+            + self_overlap(C2, CM, alpha=alpha, nthreads=nthreads)).astype(np.float32)
+    rep = lambda x, f=_f32: f(_rep(x, S))
+    q = np.array(qs.reshape(-1, 4), np.float32, copy=True, order="C")
+    t = np.array(ts.reshape(-1, 3), np.float32, copy=True, order="C")
+    K = q.shape[0]
+    best = np.empty(K, np.float32)
+    bq = np.empty((K, 4), np.float32)
+    bt = np.empty((K, 3), np.float32)
+    arrs = dict(C1=rep(C1), C2=rep(C2), CN=rep(CN, _i32), CM=rep(CM, _i32), A1=rep(A1),
+                A2=rep(A2), Q1=rep(Q1), Q2=rep(Q2), R1=rep(R1), R2=rep(R2), AN=rep(AN, _i32),
+                AM=rep(AM, _i32), S1=rep(S1), S2=rep(S2), PE1=rep(PE1), PE2=rep(PE2),
+                SN=rep(SN, _i32), SM=rep(SM, _i32), norm=_rep(norm, S).astype(np.float32))
+    a = arrs
+    L = _lib.ptr
+    _lib.lib().fsso_esp_combo_loop(
+        K, a["C1"].shape[1], a["C2"].shape[1], L(a["C1"]), L(a["C2"]), L(a["CN"]), L(a["CM"]),
+        a["A1"].shape[1], a["A2"].shape[1], L(a["A1"]), L(a["A2"]), L(a["Q1"]), L(a["Q2"]),
+        L(a["R1"]), L(a["R2"]), L(a["AN"]), L(a["AM"]), a["S1"].shape[1], a["S2"].shape[1],
+        L(a["S1"]), L(a["S2"]), L(a["PE1"]), L(a["PE2"]), L(a["SN"]), L(a["SM"]),
+        float(alpha), 1.0 / (LAM_SCALING * float(lam)), float(COULOMB_SCALING),
+        float(probe_radius), float(esp_weight), int(stride), L(a["norm"]), L(q), L(t),
+        int(steps), float(np.float32(lr)), L(best), L(bq), L(bt), _threads(nthreads))
+    out = _pick(best, bq, bt, nb, S)
+    return (out + ((best, bq, bt),)) if return_rows else out

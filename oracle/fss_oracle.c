@@ -16,6 +16,8 @@
  *   pose_pharm ext!=0   <- analytical_gradients/_torch.py:223-355 (extended_points /
  *                          only_extended of compute_overlap_and_grad_pharm)
  *   tail_tversky        <- accel/drivers/pharm.py:417-426 + pharm_overlap.py:36-59
+ *   esp_compare         <- cpu.py:237-261 (_esp_comparison_kernel, ShaEP ESP comparison)
+ *   fsso_esp_combo_loop <- accel/drivers/esp_combo.py:497-595 (vol_and_surf_esp fine loop)
  *   tail_combo          <- cpu_fused.py:111-167 (_tail_vol_color)
  *   fsso_fine_loop      <- cpu_fused.py:179-217 (fine_loop_cpu) + the per-mode glue
  *                          cpu_fused.py:225-338
@@ -541,4 +543,147 @@ int fsso_fine_loop_flat(int mode, int K, int Npad, int Mpad, const float *A, con
 int fsso_max_threads(void) {
     const long n = sysconf(_SC_NPROCESSORS_ONLN);
     return n > 0 ? (int)n : 1;
+}
+
+/* ------------------------------------------------------------------------- */
+/* ShaEP ESP comparison and the vol_and_surf_esp fine loop.                   */
+/* ------------------------------------------------------------------------- */
+/* Sum over field points i of exp(-(pe_i - coulomb * sum_m q_m / max(d_im, 1e-6))^2 * inv_lam),
+ * skipping every point within radius_m + probe of some atom (cpu.py:237-261).  P (n,3) field
+ * points and A (m,3) atoms are in one frame (double), PE (n) the field points' ESP, Q/R (m)
+ * the atoms' charges and radii. */
+static double esp_compare(const double *P, const float *PE, int n, const double *A,
+                          const float *Q, const float *Rr, int m, double inv_lam,
+                          double coulomb, double probe) {
+    double total = 0.0;
+    for (int i = 0; i < n; ++i) {
+        double esp = 0.0;
+        int blocked = 0;
+        for (int j = 0; j < m; ++j) {
+            const double dx = P[3 * i] - A[3 * j], dy = P[3 * i + 1] - A[3 * j + 1],
+                         dz = P[3 * i + 2] - A[3 * j + 2];
+            double d = sqrt(dx * dx + dy * dy + dz * dz);
+            if (d < 1e-6) d = 1e-6;
+            esp += Q[j] / d;
+            if (d < (double)Rr[j] + probe) blocked = 1;
+        }
+        esp *= coulomb;
+        if (!blocked) {
+            const double diff = PE[i] - esp;
+            total += exp(-(diff * diff) * inv_lam);
+        }
+    }
+    return total;
+}
+
+static void to_double(const float *X, int n, double *out) {
+    for (int i = 0; i < 3 * n; ++i) out[i] = X[i];
+}
+
+static void transform(const float *X, int n, const float *q, const float *t, double *out) {
+    double R[9];
+    rotmat(q, R);
+    for (int i = 0; i < n; ++i) {
+        const double x = X[3 * i], y = X[3 * i + 1], z = X[3 * i + 2];
+        out[3 * i] = R[0] * x + R[1] * y + R[2] * z + t[0];
+        out[3 * i + 1] = R[3] * x + R[4] * y + R[5] * z + t[1];
+        out[3 * i + 2] = R[6] * x + R[7] * y + R[8] * z + t[2];
+    }
+}
+
+/* Batched comparison (esp_comparison_batch): K rows of padded field points / atoms. */
+void fsso_esp_compare(int K, int Npad, int Mpad, const float *P, const float *PE,
+                      const float *A, const float *Q, const float *Rr, const int32_t *Nr,
+                      const int32_t *Mr, double inv_lam, double coulomb, double probe,
+                      double *out) {
+    double *pd = malloc(sizeof(double) * 3 * (size_t)(Npad > 0 ? Npad : 1));
+    double *ad = malloc(sizeof(double) * 3 * (size_t)(Mpad > 0 ? Mpad : 1));
+    for (int k = 0; k < K; ++k) {
+        to_double(P + (size_t)k * Npad * 3, Nr[k], pd);
+        to_double(A + (size_t)k * Mpad * 3, Mr[k], ad);
+        out[k] = esp_compare(pd, PE + (size_t)k * Npad, Nr[k], ad, Q + (size_t)k * Mpad,
+                             Rr + (size_t)k * Mpad, Mr[k], inv_lam, coulomb, probe);
+    }
+    free(pd);
+    free(ad);
+}
+
+typedef struct {
+    int K;
+    int Cn, Cm; const float *CA, *CB; const int32_t *CNr, *CMr;     /* shape centres */
+    int An, Am; const float *AA, *AB, *QA, *QB, *RA, *RB;           /* atoms with H */
+    const int32_t *ANr, *AMr;
+    int Sn, Sm; const float *SA, *SB, *PEA, *PEB;                   /* surfaces + ESP */
+    const int32_t *SNr, *SMr;
+    double alpha, inv_lam, coulomb, probe, w;
+    int stride, steps;
+    const float *norm;                                              /* V_AA + V_BB */
+    float *q, *t, *best, *bq, *bt;
+    float lr;
+} combo_args;
+
+/* One row of the vol_and_surf_esp fine loop: the pose follows the shape gradient scaled by
+ * (1 - w); the tracked score w * ESP similarity + (1 - w) * shape Tanimoto is evaluated on
+ * steps that are multiples of `stride` and on the last step (esp_combo.py:497-595). */
+static void combo_row(void *ctx, int k) {
+    const combo_args *a = (const combo_args *)ctx;
+    float *q = a->q + 4 * (size_t)k, *t = a->t + 3 * (size_t)k;
+    float mq[4] = {0, 0, 0, 0}, vq[4] = {0, 0, 0, 0}, mt[3] = {0, 0, 0}, vt[3] = {0, 0, 0};
+    float *best = a->best + k, *bq = a->bq + 4 * (size_t)k, *bt = a->bt + 3 * (size_t)k;
+    *best = -INFINITY;
+    memcpy(bq, q, 4 * sizeof(float));
+    memcpy(bt, t, 3 * sizeof(float));
+    const int na = a->ANr[k], ma = a->AMr[k], ns = a->SNr[k], ms = a->SMr[k];
+    double *sa = malloc(sizeof(double) * 3 * (size_t)(ns > 0 ? ns : 1));
+    double *aa = malloc(sizeof(double) * 3 * (size_t)(na > 0 ? na : 1));
+    double *sb = malloc(sizeof(double) * 3 * (size_t)(ms > 0 ? ms : 1));
+    double *ab = malloc(sizeof(double) * 3 * (size_t)(ma > 0 ? ma : 1));
+    to_double(a->SA + (size_t)k * a->Sn * 3, ns, sa);
+    to_double(a->AA + (size_t)k * a->An * 3, na, aa);
+    const float U = a->norm[k];
+    const float wf = (float)a->w;
+    for (int step = 0; step < a->steps; ++step) {
+        double V, dQ[4], dT[3];
+        pose_overlap(a->CA + (size_t)k * a->Cn * 3, a->CB + (size_t)k * a->Cm * 3, NULL, NULL,
+                     q, t, a->CNr[k], a->CMr[k], a->alpha, 0.0, 1, &V, dQ, dT);
+        const float Vf = (float)V;
+        const float denom = U - Vf;
+        const float scale = U / (denom * denom);
+        if (step % a->stride == 0 || step == a->steps - 1) {
+            transform(a->AB + (size_t)k * a->Am * 3, ma, q, t, ab);
+            transform(a->SB + (size_t)k * a->Sm * 3, ms, q, t, sb);
+            const double e1 = esp_compare(sa, a->PEA + (size_t)k * a->Sn, ns, ab,
+                                          a->QB + (size_t)k * a->Am, a->RB + (size_t)k * a->Am,
+                                          ma, a->inv_lam, a->coulomb, a->probe);
+            const double e2 = esp_compare(sb, a->PEB + (size_t)k * a->Sm, ms, aa,
+                                          a->QA + (size_t)k * a->An, a->RA + (size_t)k * a->An,
+                                          na, a->inv_lam, a->coulomb, a->probe);
+            const float es = ((float)e1 + (float)e2) / (float)(ns + ms);
+            const float vs = Vf / denom;
+            const float score = wf * es + (1.0f - wf) * vs;
+            track_best(score, q, t, best, bq, bt);
+        }
+        const float c = -scale * (1.0f - wf);
+        double gq[4], gt[3];
+        for (int i = 0; i < 4; ++i) gq[i] = c * (float)dQ[i];
+        for (int i = 0; i < 3; ++i) gt[i] = c * (float)dT[i];
+        adam_update(q, t, gq, gt, mq, vq, mt, vt, a->lr);
+    }
+    free(sa); free(aa); free(sb); free(ab);
+}
+
+void fsso_esp_combo_loop(int K, int Cn, int Cm, const float *CA, const float *CB,
+                         const int32_t *CNr, const int32_t *CMr, int An, int Am,
+                         const float *AA, const float *AB, const float *QA, const float *QB,
+                         const float *RA, const float *RB, const int32_t *ANr,
+                         const int32_t *AMr, int Sn, int Sm, const float *SA, const float *SB,
+                         const float *PEA, const float *PEB, const int32_t *SNr,
+                         const int32_t *SMr, double alpha, double inv_lam, double coulomb,
+                         double probe, double w, int stride, const float *norm, float *q_io,
+                         float *t_io, int steps, float lr, float *best, float *bq, float *bt,
+                         int nthreads) {
+    combo_args a = {K, Cn, Cm, CA, CB, CNr, CMr, An, Am, AA, AB, QA, QB, RA, RB, ANr, AMr,
+                    Sn, Sm, SA, SB, PEA, PEB, SNr, SMr, alpha, inv_lam, coulomb, probe, w,
+                    stride > 0 ? stride : 1, steps, norm, q_io, t_io, best, bq, bt, lr};
+    parallel_for(K, nthreads, 1, combo_row, &a);
 }

@@ -83,6 +83,8 @@ def main():
     sys.path.insert(0, args.reference)
     if args.only == "pharm_ext":
         return make_pharm_ext()
+    if args.only == "esp_combo":
+        return make_esp_combo()
     import torch
     torch.set_num_threads(max(1, os.cpu_count() or 1))
     from shepherd_score.accel.kernels import cpu as rk
@@ -268,6 +270,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "scores.npz"), **out)
     print("scores.npz")
     make_pharm_ext()
+    make_esp_combo()
 
 
 def make_pharm_ext():
@@ -337,6 +340,67 @@ def make_pharm_ext():
                     f"{tag}_score": sc.numpy(), f"{tag}_q": bq.numpy(), f"{tag}_t": bt.numpy()})
     np.savez_compressed(os.path.join(HERE, "pharm_ext.npz"), **out)
     print("pharm_ext.npz")
+
+
+
+def make_esp_combo():
+    """esp_combo.npz: the ShaEP ESP comparison (esp_comparison_batch, numba twin) on ragged
+    rows, and vol_and_surf_esp alignments (coarse_fine_esp_combo_align_many, CPU eager loop:
+    combo score tracked every 5th step and on the last) on their own seeded molecules."""
+    import torch
+    from shepherd_score.accel.kernels import cpu as rk
+    from shepherd_score.accel.drivers.esp_combo import (coarse_fine_esp_combo_align_many,
+                                                        _self_overlap_chunks)
+
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a))
+    rng = np.random.default_rng(77)
+    out = {}
+    refs, fits = syn.esp_combo_pairs(5, seed=31)
+    # comparison rows: ref surface + ESP against the fit atoms moved onto the ref centre
+    moved = []
+    for r, f in zip(refs, fits):
+        Rr = syn.random_rotation(rng)
+        a = (f["atoms"] - f["atoms"].mean(0)) @ Rr.T + r["atoms"].mean(0) + 0.5 * rng.standard_normal(3)
+        moved.append(a.astype(np.float32))
+    P, PN = pad([r["surf"] for r in refs])
+    PE, _ = pad([r["surf_esp"] for r in refs])
+    A, AM = pad(moved)
+    Q, _ = pad([f["charges"] for f in fits])
+    R, _ = pad([f["radii"] for f in fits])
+    S = rk.esp_comparison_batch(T(P), T(A), T(Q), T(PE), T(R), N_real=T(PN), M_real=T(AM),
+                                probe_radius=1.0, lam=0.001)
+    out.update(cmp_P=P, cmp_PE=PE, cmp_A=A, cmp_Q=Q, cmp_R=R, cmp_N=PN, cmp_M=AM,
+               cmp_S=S.numpy())
+
+    # alignments: pair 0 is a rotated, shifted copy of its reference
+    refs, fits = syn.esp_combo_pairs(4, seed=32)
+    Rr = syn.random_rotation(rng)
+    sh = rng.standard_normal(3)
+    f0 = dict(refs[0])
+    for k in ("centers", "atoms", "surf"):
+        f0[k] = (refs[0][k] @ Rr.T + sh).astype(np.float32)
+    fits[0] = f0
+    arr = {}
+    for side, mols in (("1", refs), ("2", fits)):
+        arr["C" + side], arr["CN" + side] = pad([m["centers"] for m in mols])
+        arr["A" + side], arr["AN" + side] = pad([m["atoms"] for m in mols])
+        arr["Q" + side], _ = pad([m["charges"] for m in mols])
+        arr["R" + side], _ = pad([m["radii"] for m in mols])
+        arr["S" + side], arr["SN" + side] = pad([m["surf"] for m in mols])
+        arr["PE" + side], _ = pad([m["surf_esp"] for m in mols])
+    VAA = _self_overlap_chunks(T(arr["C1"]), T(arr["CN1"]), 0.81)
+    VBB = _self_overlap_chunks(T(arr["C2"]), T(arr["CN2"]), 0.81)
+    sc, bq, bt = coarse_fine_esp_combo_align_many(
+        T(arr["A1"]), T(arr["A2"]), T(arr["C1"]), T(arr["C2"]), T(arr["S1"]), T(arr["S2"]),
+        T(arr["Q1"]), T(arr["Q2"]), T(arr["PE1"]), T(arr["PE2"]), T(arr["R1"]), T(arr["R2"]),
+        VAA, VBB, alpha=0.81, lam=0.001, probe_radius=1.0, esp_weight=0.5, num_seeds=8,
+        steps_fine=30, lr=0.1, N_real_centers=T(arr["CN1"]), M_real_centers=T(arr["CN2"]),
+        N_real_atoms_w_H_1=T(arr["AN1"]), M_real_atoms_w_H_2=T(arr["AN2"]),
+        N_real_surf_1=T(arr["SN1"]), M_real_surf_2=T(arr["SN2"]), early_stop_patience=10 ** 9)
+    out.update({"al_" + k: v for k, v in arr.items()})
+    out.update(al_score=sc.numpy(), al_q=bq.numpy(), al_t=bt.numpy())
+    np.savez_compressed(os.path.join(HERE, "esp_combo.npz"), **out)
+    print("esp_combo.npz")
 
 
 if __name__ == "__main__":

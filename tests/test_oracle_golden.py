@@ -173,3 +173,27 @@ def test_align_pharm_tversky_and_extended(golden, tag, sim, ext, only):
     ref = g[f"{tag}_score"]
     assert sc[0] > 0.99 and ref[0] > 0.99
     np.testing.assert_allclose(sc, ref, atol=2e-3)
+
+
+def test_esp_comparison(golden):
+    """ShaEP ESP comparison (esp_comparison_batch): masked Gaussian of the ESP difference."""
+    g = golden["esp_combo"]
+    S = oa.esp_compare(g["cmp_P"], g["cmp_PE"], g["cmp_A"], g["cmp_Q"], g["cmp_R"], g["cmp_N"],
+                       g["cmp_M"], lam=0.001, probe_radius=1.0)
+    np.testing.assert_allclose(S, g["cmp_S"], rtol=1e-6)
+    assert np.all(S > 0) and np.all(S < g["cmp_N"])     # some points blocked, some kept
+
+
+def _combo_args(g):
+    return [g["al_" + k] for k in ("C1", "C2", "CN1", "CN2", "A1", "A2", "Q1", "Q2", "R1", "R2",
+                                   "AN1", "AN2", "S1", "S2", "PE1", "PE2", "SN1", "SN2")]
+
+
+def test_align_esp_combo(golden):
+    """vol_and_surf_esp fine loop (shape-steered pose, combo score tracked every 5th step and
+    on the last, as the reference's eager loop): best scores within 1e-4 of the reference's."""
+    g = golden["esp_combo"]
+    sc, q, t = oa.align_esp_combo(*_combo_args(g), alpha=0.81, lam=0.001, probe_radius=1.0,
+                                  esp_weight=0.5, num_seeds=8, steps=30, lr=0.1, stride=5)
+    np.testing.assert_allclose(sc, g["al_score"], atol=1e-4)
+    assert sc[0] > 0.9
