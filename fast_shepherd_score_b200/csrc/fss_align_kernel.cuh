@@ -82,7 +82,9 @@ __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
   // FP32 path: sP = 2 * maxN duplicated expanded reference (+ sQc).  Tensor-core path:
   // sP = 8 * nbMax block-interleaved reference, sCm/sQm after the fit cloud.
   const int nbMax = (p.maxN + 7) >> 3;
-  float4* sP = smem;
+  // parked optimiser state: kColdFields floats per thread (a multiple of 16 bytes per CTA)
+  volatile float* sCold = reinterpret_cast<float*>(smem) + threadIdx.x;
+  float4* sP = smem + kColdFields * blockDim.x / 4;
   float4* sB = sP + (TC ? kMmaP4PerBlock * nbMax : 2 * p.maxN);
   float4* sRA = sB + p.maxM;
   float4* sRV = sRA + p.maxNp;
@@ -192,6 +194,7 @@ __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
         t0[1] = p.seed_t[row * 3 + 1] - c.y;
         t0[2] = p.seed_t[row * 3 + 2] - c.z;
         pose_init(s, q0, t0);
+        cold_store(s, sCold, blockDim.x);
       }
       for (int step = 0; step < p.steps; ++step) {
         const Rot R = quat_to_rot(s.q);
@@ -217,9 +220,11 @@ __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
           Reduced rc;
           rc.from(mc, s.q);
           rc.template group_sum<LPP>();
+          cold_load(s, sCold, blockDim.x);
           if (kShape) step_combo(s, rs, Us, rc, Uc, p.w, p.lr);
           else if (p.sigma >= 0.f) step_tversky(s, rc, Dtv, p.lr);
           else step_single(s, rc, Us, p.lr);
+          cold_store(s, sCold, blockDim.x);
         } else if (kCombo) {
           const bool scored = step % p.esp_stride == 0 || step == p.steps - 1;
           float esp = 0.f;
@@ -231,11 +236,16 @@ __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
 #pragma unroll
             for (int o = LPP / 2; o > 0; o >>= 1) esp += __shfl_xor_sync(0xffffffffu, esp, o);
           }
+          cold_load(s, sCold, blockDim.x);
           step_esp_combo(s, rs, Us, esp, (float)(Ns + Ms), p.esp_w, scored, p.lr);
+          cold_store(s, sCold, blockDim.x);
         } else {
+          cold_load(s, sCold, blockDim.x);
           step_single(s, rs, Us, p.lr);
+          cold_store(s, sCold, blockDim.x);
         }
       }
+      cold_load(s, sCold, blockDim.x);
       if (active && lane == 0) {
         const size_t r = (size_t)pidx * p.n_starts + start;
         p.row_score[r] = s.best;

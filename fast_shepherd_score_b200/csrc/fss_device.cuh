@@ -160,6 +160,46 @@ struct PoseState {
   float best, bq[4], bt[3];
 };
 
+// The optimiser state that the hot loop does not read (Adam moments, best score and pose) is
+// parked in shared memory between tails, so the registers go to the pairwise loop.  Each
+// thread owns one column (field f of thread x at f * nthreads + x), so no synchronisation is
+// needed; volatile keeps the compiler from carrying the values in registers across the loop.
+constexpr int kColdFields = 22;
+
+__device__ __forceinline__ void cold_store(const PoseState& s, volatile float* c, int stride) {
+  int f = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) c[(f++) * stride] = s.mq[i];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) c[(f++) * stride] = s.vq[i];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) c[(f++) * stride] = s.mt[i];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) c[(f++) * stride] = s.vt[i];
+  c[(f++) * stride] = s.best;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) c[(f++) * stride] = s.bq[i];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) c[(f++) * stride] = s.bt[i];
+}
+
+__device__ __forceinline__ void cold_load(PoseState& s, const volatile float* c, int stride) {
+  int f = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) s.mq[i] = c[(f++) * stride];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) s.vq[i] = c[(f++) * stride];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) s.mt[i] = c[(f++) * stride];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) s.vt[i] = c[(f++) * stride];
+  s.best = c[(f++) * stride];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) s.bq[i] = c[(f++) * stride];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) s.bt[i] = c[(f++) * stride];
+}
+
 __device__ __forceinline__ void pose_init(PoseState& s, const float q0[4], const float t0[3]) {
 #pragma unroll
   for (int i = 0; i < 4; ++i) { s.q[i] = q0[i]; s.bq[i] = q0[i]; s.mq[i] = 0.f; s.vq[i] = 0.f; }
