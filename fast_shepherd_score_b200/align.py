@@ -170,9 +170,13 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
             order = cost_order(ref_ph.counts[pr], fit_ph.counts[pf], dev)
     if (lanes_per_pose == 0 and chunks == 0 and cta_per_sm == 0 and accumulate == 0
             and kernel_variant == 0 and autotune.enabled() and P >= 64 and steps > 0):
+        extra = (dict(ref_atoms=ref_atoms, fit_atoms=fit_atoms, ref_radii=ref_radii,
+                      fit_radii=fit_radii, ref_surf=ref_surf, fit_surf=fit_surf,
+                      probe_radius=probe_radius, esp_weight=esp_weight, esp_stride=esp_stride)
+                 if combo else dict(similarity=similarity, pharm_extended=pharm_extended))
         tile = _tuned_tile(mode, shape, ref, fit, ref_ph, fit_ph, pair_ref, pair_fit, seed_q,
                            seed_t, steps, lr, alpha, lam, color_weight, ref_self, fit_self,
-                           ref_self_ph, fit_self_ph)
+                           ref_self_ph, fit_self_ph, extra)
         lanes_per_pose, chunks, cta_per_sm = (tile["lanes_per_pose"], tile["chunks"],
                                               tile["cta_per_sm"])
         accumulate = tile.get("accumulate", 0)
@@ -249,7 +253,7 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
 
 def _tuned_tile(mode, shape, ref, fit, ref_ph, fit_ph, pair_ref, pair_fit, seed_q, seed_t,
                 steps, lr, alpha, lam, color_weight, ref_self, fit_self, ref_self_ph,
-                fit_self_ph):
+                fit_self_ph, extra=None):
     """The autotuned tile for this launch's shape bucket (tuned on first sight)."""
     cs_r, cs_f = (ref, fit) if shape else (ref_ph, fit_ph)
     S = int(seed_q.shape[1])
@@ -262,8 +266,9 @@ def _tuned_tile(mode, shape, ref, fit, ref_ph, fit_ph, pair_ref, pair_fit, seed_
     pr = pair_ref.cpu().numpy()
     pf = pair_fit.cpu().numpy()
     cost = cs_r.counts[pr].astype(np.int64) * cs_f.counts[pf].astype(np.int64)
-    # enough pairs for several waves of CTAs, so the sample is throughput- not latency-bound
-    k = min(P, 8 * torch.cuda.get_device_properties(seed_q.device).multi_processor_count)
+    # enough pairs for many waves of CTAs, so the sample is throughput- not latency-bound and
+    # its load balance resembles the full launch's
+    k = min(P, 16 * torch.cuda.get_device_properties(seed_q.device).multi_processor_count)
     sel = torch.from_numpy(autotune.sample_pairs(cost, k)).to(seed_q.device)
     sub = dict(ref=ref, fit=fit, ref_ph=ref_ph, fit_ph=fit_ph, pair_ref=pair_ref[sel],
                pair_fit=pair_fit[sel], seed_q=seed_q[sel], seed_t=seed_t[sel],
@@ -271,11 +276,18 @@ def _tuned_tile(mode, shape, ref, fit, ref_ph, fit_ph, pair_ref, pair_fit, seed_
                color_weight=color_weight, ref_self=ref_self, fit_self=fit_self,
                ref_self_ph=ref_self_ph, fit_self_ph=fit_self_ph, check_status=False,
                scratch=torch.zeros(2, dtype=_i32, device=seed_q.device))
+    sub.update(extra or {})
 
     def run(**tile):
         align_packed(mode, **sub, **tile)
 
-    return autotune.tune(run, key, autotune.candidates(mode, cs_f.max_points, S))
+    # small problems: lengthen the sample until one run takes a few ms, so launch latency and
+    # jitter do not decide the ranking (capped at the real step count)
+    cands = autotune.candidates(mode, cs_f.max_points, S)
+    ms = autotune.time_once(run, **cands[0])   # an explicit tile: no recursive tuning
+    if ms < 3.0 and sub["steps"] < steps:
+        sub["steps"] = int(min(steps, math.ceil(sub["steps"] * 3.0 / max(ms, 1e-3))))
+    return autotune.tune(run, key, cands, repeats=3)
 
 
 # ------------------------------------------------------------------------------------------

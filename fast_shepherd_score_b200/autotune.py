@@ -7,7 +7,7 @@ Tunables of one launch (``fss_align_desc``):
   accumulate      1 = value/gradient sums on the FP32 lanes, 2 = on the tensor cores
                   (shape/ESP modes; 32 lanes per pose)
   kernel_variant  code variant of the FP32-lane loop (shape/ESP modes): 1 base, 2 wide
-                  register tile, 3 one-CTA/SM register budget
+                  register tile, 3 one-CTA/SM register budget, 4 base tile unrolled 4x
 
 For a new problem shape the tuner times each candidate on a sample of the batch's pairs
 (the costliest and a spread of the rest) for a few Adam steps, with CUDA events, and keeps
@@ -81,7 +81,8 @@ def shape_key(device, mode: str, max_ref: int, max_fit: int, mean_fit: float, n_
 
 def candidates(mode: str, max_fit: int, n_starts: int):
     out = []
-    variants = (1, 2, 3) if mode in ("shape", "esp") else (0,)
+    variants = ((1, 2, 3, 4) if mode in ("shape", "esp") else
+                (1, 3) if mode == "esp_combo" else (0,))
     for lpp in LANES:
         if mode != "pharm" and lpp > 4 and lpp // 2 >= max(max_fit, 1):
             continue  # more lanes than fit points: idle lanes
@@ -126,6 +127,18 @@ def lookup(key: str) -> Optional[dict]:
     with _LOCK:
         _load()
         return _MEM.get(key)
+
+
+def time_once(run, **tile) -> float:
+    """Milliseconds of one warm ``run(**tile)`` (CUDA events on the current stream)."""
+    run(**tile)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    run(**tile)
+    e1.record()
+    e1.synchronize()
+    return e0.elapsed_time(e1)
 
 
 def tune(run, key: str, cands, repeats: int = 2) -> dict:

@@ -10,7 +10,8 @@ int launch_align_esp(int lpp, bool tc, int var, const AlignParams& prm, int thre
     case 0: return dispatch_lanes<FSS_MODE_ESP, 0>(lpp, prm, threads, cps, smem, st);
     case 1: return dispatch_lanes<FSS_MODE_ESP, 1>(lpp, prm, threads, cps, smem, st);
     case 2: return dispatch_lanes<FSS_MODE_ESP, 2>(lpp, prm, threads, cps, smem, st);
-    default: return set_error(FSS_ERR_INVALID, "fss_align: kernel_variant must be 0..3");
+    case 3: return dispatch_lanes<FSS_MODE_ESP, 3>(lpp, prm, threads, cps, smem, st);
+    default: return set_error(FSS_ERR_INVALID, "fss_align: kernel_variant must be 0..4");
   }
 }
 

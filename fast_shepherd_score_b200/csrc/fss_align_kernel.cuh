@@ -56,6 +56,7 @@ constexpr int kMaxThreads = 320;  // 10 warps
 //      chains per warp (large clouds)
 //   2  4 fit points per lane, unrolled 4x, register budget of one 320-thread CTA per SM:
 //      no spills, fewer resident warps (small clouds, whose poses are tail-heavy)
+//   3  4 fit points per lane, unrolled 4x, <= 96 registers
 template <int VAR>
 struct AlignVariant;
 template <>
@@ -64,6 +65,8 @@ template <>
 struct AlignVariant<1> { static constexpr int kJB2 = 3, kUnroll = 4, kMinCtas = 2; };
 template <>
 struct AlignVariant<2> { static constexpr int kJB2 = 2, kUnroll = 4, kMinCtas = 1; };
+template <>
+struct AlignVariant<3> { static constexpr int kJB2 = 2, kUnroll = 4, kMinCtas = 2; };
 
 // TC: shape/ESP sums on the tensor cores (fss_mma.cuh); requires LPP == 32 and a mode
 // without a pharmacophore channel.  EXT: extended pharmacophore points (pharm_pose).

@@ -160,8 +160,9 @@ typedef struct fss_align_desc {
   int32_t kernel_variant;    /* code variant of the FP32-lane loop: 0 automatic, 1 base (4 fit
                               * points per lane, 2 CTAs/SM register budget), 2 wide (6 fit
                               * points per lane, deeper unroll), 3 roomy (4 fit points, one
-                              * CTA/SM register budget); 2 and 3 for modes SHAPE and ESP, 3
-                              * also for ESP_COMBO */
+                              * CTA/SM register budget), 4 unrolled (4 fit points, 4x unroll,
+                              * 2 CTAs/SM budget); 2-4 for modes SHAPE and ESP, 3 also for
+                              * ESP_COMBO */
   int32_t pharm_extended;    /* mode PHARM: 0 cosine-weighted directional features, 1 extended
                               * points (anchor + unit vector) plus anchors, 2 extended points
                               * only (extended_points / only_extended of
