@@ -50,12 +50,20 @@ WORKLOADS = {
                       lr=0.1, alpha=0.81, lam=0.0,
                       desc="combined shape+pharmacophore: 16384 pairs, 15-60 atoms + 3-20 "
                            "features, 50 starts x 200 Adam steps"),
+    "vol_and_surf_esp": dict(mode="vol_and_surf_esp", pairs=4096, lo=10, hi=25, starts=8,
+                             steps=60, lr=0.1, alpha=0.81, lam=0.001,
+                             desc="ShaEP combo: 4096 pairs, 10-25 heavy atoms (+H), 100-200 "
+                                  "surface points with ESP, 8 starts x 60 Adam steps, combo "
+                                  "score every step"),
 }
 
 
 def make_inputs(wl, n_pairs, seed):
     from fast_shepherd_score_b200 import synthetic as syn
     from fast_shepherd_score_b200.api import HostBatch
+    if wl["mode"] == "vol_and_surf_esp":
+        refs, fits = syn.esp_combo_pairs(n_pairs, seed=seed, heavy_lo=wl["lo"], heavy_hi=wl["hi"])
+        return None, None, (refs, fits)
     if wl["mode"] == "surf_esp":
         refs, fits = syn.esp_surface_pairs(n_pairs, seed=seed, lo=wl["lo"], hi=wl["hi"])
         ref = HostBatch.from_lists([p for p, _ in refs], [c for _, c in refs])
@@ -348,7 +356,17 @@ def cpu_align_sample(wl, raw, k, nthreads=None):
     from oracle import align as oa
     refs, fits = raw
     t0 = time.perf_counter()
-    if wl["mode"] == "surf_esp":
+    if wl["mode"] == "vol_and_surf_esp":
+        pads = []
+        for key in ("centers", "atoms", "charges", "radii", "surf", "surf_esp"):
+            for ms in (refs, fits):
+                pads.append(_pad([m[key] for m in ms[:k]]))
+        (C1, CN), (C2, CM), (A1, AN), (A2, AM), (Q1, _), (Q2, _), (R1, _), (R2, _), \
+            (S1, SN), (S2, SM), (P1, _), (P2, _) = pads
+        oa.align_esp_combo(C1, C2, CN, CM, A1, A2, Q1, Q2, R1, R2, AN, AM, S1, S2, P1, P2, SN, SM,
+                           alpha=wl["alpha"], lam=wl["lam"], num_seeds=wl["starts"],
+                           steps=wl["steps"], lr=wl["lr"], stride=1, nthreads=nthreads)
+    elif wl["mode"] == "surf_esp":
         A, N = _pad([p for p, _ in refs[:k]]); B, M = _pad([p for p, _ in fits[:k]])
         CA, _ = _pad([c for _, c in refs[:k]]); CB, _ = _pad([c for _, c in fits[:k]])
         oa.align_esp(A, B, CA, CB, N, M, alpha=wl["alpha"], lam=oa.LAM_SCALING * wl["lam"],
@@ -485,8 +503,12 @@ def server_bench(dev, duration=20.0, n_lib=1_000_000, load=0.6, seed=7):
     al.align_packed("shape_pharm", ref=qset, fit=atoms, ref_ph=qph, fit_ph=ph, pair_ref=pr,
                     pair_fit=pf, seed_q=sq, seed_t=st, steps=100, lr=0.1)
     lpp = al.LAST_TILE.get("lanes_per_pose") or 8
+    tile = {k: al.LAST_TILE[k] for k in ("chunks", "cta_per_sm", "kernel_variant")
+            if k in al.LAST_TILE}
+    # library bytes a pair reads from HBM: the molecule's packed atoms + pharmacophores
+    mol_bytes = (atoms.pts.nbytes + ph.anc.nbytes + ph.vec.nbytes) / n_lib
     with ScreenServer((atoms, ph), mode="vol_pharm", starts=20, steps=100, lanes_per_pose=lpp,
-                      max_pairs_per_launch=65536) as srv:
+                      max_pairs_per_launch=65536, tile=tile) as srv:
         # capacity: one large request alone
         t1 = time.perf_counter()
         srv.submit(pool[0], rng.choice(n_lib, 131072, replace=False), top_k=100).result()
@@ -517,8 +539,157 @@ def server_bench(dev, duration=20.0, n_lib=1_000_000, load=0.6, seed=7):
             "pairs_per_s": round((st["pairs_done"] - 131072) / wall, 1),
             "p50_ms": round(float(np.percentile(lat, 50)), 2),
             "p99_ms": round(float(np.percentile(lat, 99)), 2),
-            "max_queue_depth": st["max_queue_depth"], "lanes_per_pose": int(lpp),
+            "max_queue_depth": st["max_queue_depth"], "tile": dict(tile, lanes_per_pose=lpp),
+            "library_bytes_per_molecule": round(mol_bytes, 1),
+            "library_hbm_gbs_at_capacity": round(cap * mol_bytes / 1e9, 3),
             "library_build_s": round(gen_s, 1)}
+
+
+def run_esp_combo(args, wl):
+    """vol_and_surf_esp: device-resident step (self overlaps + seeds + fused kernel + pick) and
+    an end-to-end leg from pinned host arrays (H2D of every cloud, align, D2H of the results).
+    Work units: shape terms S*T*N_c*M_c plus ESP-comparison pairs S*T*(N_s*M_a + M_s*N_a)
+    (each one MUFU rsqrt or ex2)."""
+    import torch
+    import torch.distributed as dist
+    from fast_shepherd_score_b200 import align as al, kernels as K
+    from fast_shepherd_score_b200.layout import CloudSet
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    n_pairs = args.pairs or wl["pairs"]
+    _, _, raw = make_inputs(wl, n_pairs, seed=1 + rank)
+    refs, fits = raw
+    S, T = wl["starts"], wl["steps"]
+    cnt = lambda ms, k: np.array([len(m[k]) for m in ms], np.int64)
+    terms = int(S * T * ((cnt(refs, "centers") * cnt(fits, "centers")).sum() +
+                         (cnt(refs, "surf") * cnt(fits, "atoms")).sum() +
+                         (cnt(fits, "surf") * cnt(refs, "atoms")).sum()))
+
+    def sets(ms, non_blocking=False):
+        g = lambda k: [m[k] for m in ms]
+        c = CloudSet.from_arrays(g("centers"), device=dev, non_blocking=non_blocking)
+        a = CloudSet.from_arrays(g("atoms"), g("charges"), device=dev, non_blocking=non_blocking)
+        r = torch.from_numpy(np.concatenate(g("radii")).astype(np.float32))
+        r = (r.pin_memory() if non_blocking else r).to(dev, non_blocking=non_blocking)
+        sf = CloudSet.from_arrays(g("surf"), g("surf_esp"), device=dev, non_blocking=non_blocking)
+        return c, a, r, sf
+
+    rc, ra, rr, rs = sets(refs)
+    fc, fa, fr, fs = sets(fits)
+    idx = torch.arange(n_pairs, dtype=torch.int32, device=dev)
+    tile = {}
+    if args.tile:
+        v = [int(x) for x in args.tile.split(",")]
+        tile = dict(zip(("lanes_per_pose", "chunks", "cta_per_sm", "accumulate"), v))
+    kern = []
+
+    def step(c1, c2, a1, a2, r1, r2, s1, s2, record=False):
+        vs = K.self_overlap(c1, wl["alpha"]); vf = K.self_overlap(c2, wl["alpha"])
+        sq, st = K.seeds(c1, c2, idx, idx, S)
+        if record:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+        out = al.align_packed("esp_combo", ref=c1, fit=c2, pair_ref=idx, pair_fit=idx,
+                              seed_q=sq, seed_t=st, steps=T, lr=wl["lr"], alpha=wl["alpha"],
+                              lam=wl["lam"], ref_self=vs, fit_self=vf, ref_atoms=a1,
+                              fit_atoms=a2, ref_radii=r1, fit_radii=r2, ref_surf=s1,
+                              fit_surf=s2, esp_stride=1, check_status=False, validate=False,
+                              **tile)
+        if record:
+            e1.record()
+            kern.append((e0, e1))
+        return out
+
+    args_dev = (rc, fc, ra, fa, rr, fr, rs, fs)
+    l2 = torch.empty(64 << 20, device=dev)
+    for _ in range(args.warmup):
+        step(*args_dev)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local).start()
+    times = []
+    for _ in range(args.steps):
+        flush_l2(l2)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step(*args_dev, record=True)
+        e1.record()
+        times.append((e0, e1))
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    t_max = torch.tensor([sum(a.elapsed_time(b) for a, b in times)], device=dev,
+                         dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    ms_per_step = float(t_max.item()) / args.steps
+    value = n_pairs * world / (ms_per_step * 1e-3)
+
+    # end to end: pinned host arrays -> device sets -> align -> scores/poses on the host
+    e2e_ms, h2d = [], 0
+    for i in range((max(1, min(args.steps, 3)) + 1) if args.e2e else 0):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        r4 = sets(refs, True)
+        f4 = sets(fits, True)
+        sc, q, t = step(r4[0], f4[0], r4[1], f4[1], r4[2], f4[2], r4[3], f4[3])
+        host = torch.cat([sc[:, None], q, t], 1).cpu()
+        t1 = time.perf_counter()
+        if i:
+            e2e_ms.append((t1 - t0) * 1e3)
+        h2d = sum(x.pts.nbytes for x in (r4[0], r4[1], r4[3], f4[0], f4[1], f4[3])) + \
+            r4[2].nbytes + f4[2].nbytes
+    e2e_t = torch.tensor([statistics.median(e2e_ms) if e2e_ms else float("nan")], device=dev,
+                         dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    if rank != 0:
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return None
+    peak = measure_peak(dev)
+    kavg = statistics.mean(a.elapsed_time(b) for a, b in kern)
+    achieved = terms / (kavg * 1e-3)
+    line = {
+        "metric": "aligned pairs/s (vol_and_surf_esp: 8 starts x 60 Adam steps), batched fused "
+                  "kernel",
+        "value": round(value, 2), "unit": "aligned pairs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": wl["desc"], "mode": wl["mode"], "pairs_per_gpu": n_pairs,
+                   "starts": S, "adam_steps": T, "lr": wl["lr"], "alpha": wl["alpha"],
+                   "lam": wl["lam"], "esp_stride": 1,
+                   "l2": "flushed between timed steps (256 MB write outside timed windows)",
+                   "parallelism": f"dp{world} (independent pair shards, no collective)",
+                   "tile": dict(al.LAST_TILE)},
+        "e2e": {"value": round(n_pairs * world / (float(e2e_t.item()) * 1e-3), 2),
+                "unit": "aligned pairs/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": n_pairs * 8 * 4,
+                "api": "fast_shepherd_score_b200.align.align_packed from pinned host arrays"},
+        "gpu_launches": 5 * args.steps,
+        "roofline": {"bound": "mufu", "achieved": round(achieved / 1e9, 1),
+                     "peak": round(peak["ex2"] / 1e9, 1), "unit": "Gterm/s",
+                     "frac": round(achieved / peak["ex2"], 4), "traffic": None,
+                     "peak_source": "measured ex2 rate (one MUFU op per shape term and per "
+                                    "ESP-comparison pair)",
+                     "terms_per_launch": terms, "kernel_ms": round(kavg, 3)},
+        "clocks": clk,
+    }
+    if args.cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(wl, raw, budget_s=args.cpu_seconds)
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return line
 
 
 def run_reference(args, wl):
@@ -544,7 +715,8 @@ def run_reference(args, wl):
         times.append(dt)
     ms = statistics.median(times) * 1e3
     value = k / (ms * 1e-3)
-    line = {"impl": "reference", "metric": "aligned pairs/s (50 starts x 200 Adam steps)",
+    line = {"impl": "reference",
+            "metric": f"aligned pairs/s ({wl['starts']} starts x {wl['steps']} Adam steps)",
             "value": round(value, 3), "unit": "aligned pairs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -584,6 +756,8 @@ def main(argv=None):
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
         return run_reference(args, wl)
+    if wl["mode"] == "vol_and_surf_esp":
+        return run_esp_combo(args, wl)
     return run_cuda(args, wl)
 
 

@@ -163,13 +163,17 @@ class ScreenServer:
                  lr: float = 0.1, alpha: float = 0.81, color_weight: float = 0.5,
                  max_pairs_per_launch: int = 65536, hbm_budget_bytes: Optional[int] = None,
                  lanes_per_pose: int = 8, max_in_flight: int = 2, slice_pairs: int = 8192,
-                 ids=None, device=None):
+                 ids=None, device=None, tile: Optional[dict] = None):
         self.atoms, self.pharm = library
         self.dev = torch.device(device or self.atoms.pts.device)
         self.mode = mode
         self.S, self.steps, self.lr = int(starts), int(steps), float(lr)
         self.alpha, self.w = float(alpha), float(color_weight)
         self.lpp = int(lanes_per_pose)
+        # the remaining tile fields (chunks, cta_per_sm, kernel_variant), fixed for the server's
+        # life so a request's result does not depend on its launch-mates
+        self.tile = {k: int(v) for k, v in (tile or {}).items()
+                     if k in ("chunks", "cta_per_sm", "kernel_variant")}
         self.ids = ids
         self.max_in_flight = int(max_in_flight)
         directional = mode == "vol_pharm"
@@ -302,7 +306,8 @@ class ScreenServer:
                               steps=self.steps, lr=self.lr, alpha=self.alpha,
                               color_weight=self.w, ref_self=q_self, fit_self=self.lib_self,
                               ref_self_ph=q_self_ph, fit_self_ph=self.lib_self_ph, order=ord_d,
-                              lanes_per_pose=self.lpp, check_status=False, validate=False)
+                              lanes_per_pose=self.lpp, check_status=False, validate=False,
+                              **self.tile)
         sc, q, t = res
         host = torch.empty(P, 8, dtype=torch.float32, pin_memory=True)
         host.copy_(torch.cat([sc[:, None], q, t], 1), non_blocking=True)
