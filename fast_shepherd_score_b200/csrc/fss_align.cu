@@ -265,8 +265,8 @@ int align_launch(const fss_align_desc* d, cudaStream_t st) {
                sizeof(float2) * (kMmaC2PerBlock + kMmaQ2PerBlock) * nb + 16
          : sizeof(float4) * (2 * (size_t)maxN + maxM + 2 * (size_t)maxNp + 2 * (size_t)maxMp) +
                sizeof(float2) * (d->mode == FSS_MODE_ESP ? (size_t)maxN : 0) +
-               sizeof(float4) * ((size_t)maxNs + maxMs + maxNa + maxMa) +
-               sizeof(float) * ((size_t)maxNa + maxMa) + 16);
+               sizeof(float4) * ((size_t)maxNs + maxMs + 2 * ((size_t)maxNa + maxMa)) +
+               sizeof(float2) * ((size_t)maxNa + maxMa) + 16);
   int rc;
   switch (d->mode) {
     case FSS_MODE_SHAPE: rc = launch_align_shape(lpp, tc, var, p, threads, d->cta_per_sm, smem, st); break;

@@ -96,13 +96,14 @@ __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
   float2* sQc = reinterpret_cast<float2*>(sFV + p.maxMp);
   float2* sCm = reinterpret_cast<float2*>(sB + p.maxM);
   float2* sQm = sCm + kMmaC2PerBlock * nbMax;
-  // vol_and_surf_esp channel: surfaces, atoms with H, (radius + probe)^2
+  // vol_and_surf_esp channel: surfaces, atoms with H (negated, duplicated: 2 float4 each),
+  // -(radius + probe)^2 duplicated (float2)
   float4* sSA = sFV + p.maxMp;
   float4* sSB = sSA + p.maxNs;
   float4* sAA = sSB + p.maxMs;
-  float4* sAB = sAA + p.maxNa;
-  float* sRA2 = reinterpret_cast<float*>(sAB + p.maxMa);
-  float* sRB2 = sRA2 + p.maxNa;
+  float4* sAB = sAA + 2 * p.maxNa;
+  float2* sRA2 = reinterpret_cast<float2*>(sAB + 2 * p.maxMa);
+  float2* sRB2 = sRA2 + p.maxNa;
   __shared__ float red[96];
   __shared__ int s_item;
 
@@ -160,17 +161,21 @@ __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
         const float4 v = p.ref_surf[rs0 + i];
         sSA[i] = make_float4(v.x - c.x, v.y - c.y, v.z - c.z, v.w);
       }
+      stage_copy(p.fit_surf + fs0, Ms, sSB);
       for (int i = tid; i < Na; i += blockDim.x) {
         const float4 v = p.ref_atoms[ra0 + i];
-        sAA[i] = make_float4(v.x - c.x, v.y - c.y, v.z - c.z, v.w);
+        const float x = c.x - v.x, y = c.y - v.y, z = c.z - v.z;
+        sAA[2 * i] = make_float4(x, x, y, y);
+        sAA[2 * i + 1] = make_float4(z, z, v.w, v.w);
         const float r = p.ref_radii[ra0 + i] + p.probe;
-        sRA2[i] = r * r;
+        sRA2[i] = make_float2(-r * r, -r * r);
       }
-      stage_copy(p.fit_surf + fs0, Ms, sSB);
-      stage_copy(p.fit_atoms + fa0, Ma, sAB);
       for (int i = tid; i < Ma; i += blockDim.x) {
+        const float4 v = p.fit_atoms[fa0 + i];
+        sAB[2 * i] = make_float4(-v.x, -v.x, -v.y, -v.y);
+        sAB[2 * i + 1] = make_float4(-v.z, -v.z, v.w, v.w);
         const float r = p.fit_radii[fa0 + i] + p.probe;
-        sRB2[i] = r * r;
+        sRB2[i] = make_float2(-r * r, -r * r);
       }
     }
     if (kPharm) {

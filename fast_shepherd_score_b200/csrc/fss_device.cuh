@@ -42,6 +42,8 @@ __device__ __forceinline__ float ex2(float x) {
   return y;
 }
 
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
 struct Rot {
   float r[9];
 };
@@ -295,40 +297,60 @@ __device__ __forceinline__ void step_esp_combo(PoseState& s, const Reduced& m, f
 // One side of the ShaEP ESP comparison for one pose (cpu.py:237-261, esp_triton.py:265-346):
 //   sum over field points i of exp(-(pe_i - coulomb * sum_m q_m / max(d_im, 1e-6))^2 / lam')
 // skipping points within radius_m + probe of any atom.  Field points (x, y, z, pe) and atoms
-// (x, y, z, q) live in different frames: TO_BODY maps a field point of the reference frame into
-// the fit body frame (u = R^T (p - t)), otherwise a body-frame field point into the reference
-// frame (u = R p + t).  rp2 holds (radius + probe)^2 per atom.  Lanes split the field points;
-// returns this lane's partial sum.
+// live in different frames: TO_BODY maps a field point of the reference frame into the fit
+// body frame (u = R^T (p - t)), otherwise a body-frame field point into the reference frame
+// (u = R p + t).  Atoms are staged negated and duplicated for f32x2 arithmetic over two field
+// points per lane: atoms[2m] = (-x, -x, -y, -y), atoms[2m+1] = (-z, -z, q, q),
+// rp2[m] = (-(r+probe)^2, same).
+// The 1e-6 distance floor never matters: an atom that close blocks the point, and blocked
+// points contribute nothing, so 1/d is a plain rsqrt.  Lanes split the field points; returns
+// this lane's partial sum (nkl = -log2(e) / lam').
 template <int LPP, bool TO_BODY>
 __device__ __forceinline__ float esp_side(const float4* __restrict__ field, int n,
                                           const float4* __restrict__ atoms,
-                                          const float* __restrict__ rp2, int m, int lane,
+                                          const float2* __restrict__ rp2, int m, int lane,
                                           const Rot& R, float tx, float ty, float tz,
                                           float coulomb, float nkl) {
   float total = 0.f;
-  for (int i = lane; i < n; i += LPP) {
-    const float4 f = field[i];
-    float ux, uy, uz;
-    if (TO_BODY) {
-      const float px = f.x - tx, py = f.y - ty, pz = f.z - tz;
-      ux = fmaf(R.r[0], px, fmaf(R.r[3], py, R.r[6] * pz));
-      uy = fmaf(R.r[1], px, fmaf(R.r[4], py, R.r[7] * pz));
-      uz = fmaf(R.r[2], px, fmaf(R.r[5], py, R.r[8] * pz));
-    } else {
-      const float3 p3 = rot_apply(R, f.x, f.y, f.z);
-      ux = p3.x + tx; uy = p3.y + ty; uz = p3.z + tz;
+  for (int i0 = lane; i0 < n; i0 += 2 * LPP) {
+    const int i1 = i0 + LPP;
+    const bool has1 = i1 < n;
+    const float4 fa = field[i0];
+    const float4 fb = has1 ? field[i1] : fa;
+    float u[2][3];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const float4 f = h ? fb : fa;
+      if (TO_BODY) {
+        const float px = f.x - tx, py = f.y - ty, pz = f.z - tz;
+        u[h][0] = fmaf(R.r[0], px, fmaf(R.r[3], py, R.r[6] * pz));
+        u[h][1] = fmaf(R.r[1], px, fmaf(R.r[4], py, R.r[7] * pz));
+        u[h][2] = fmaf(R.r[2], px, fmaf(R.r[5], py, R.r[8] * pz));
+      } else {
+        const float3 p3 = rot_apply(R, f.x, f.y, f.z);
+        u[h][0] = p3.x + tx; u[h][1] = p3.y + ty; u[h][2] = p3.z + tz;
+      }
     }
-    float esp = 0.f;
-    bool blocked = false;
+    const float2 UX = f2(u[0][0], u[1][0]), UY = f2(u[0][1], u[1][1]), UZ = f2(u[0][2], u[1][2]);
+    float2 esp = f2(0.f, 0.f);
+    float gap0 = INFINITY, gap1 = INFINITY;  // min over atoms of d^2 - (r + probe)^2
+#pragma unroll 2
     for (int j = 0; j < m; ++j) {
-      const float4 a = atoms[j];
-      const float dx = ux - a.x, dy = uy - a.y, dz = uz - a.z;
-      const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      esp = fmaf(a.w, fminf(rsqrtf(d2), 1e6f), esp);   // 1 / max(d, 1e-6)
-      blocked = blocked || d2 < rp2[j];
+      const float4 a = atoms[2 * j], b = atoms[2 * j + 1];
+      const float2 dx = __fadd2_rn(UX, f2(a.x, a.y)), dy = __fadd2_rn(UY, f2(a.z, a.w));
+      const float2 dz = __fadd2_rn(UZ, f2(b.x, b.y));
+      const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+      esp = __ffma2_rn(f2(b.z, b.w), f2(rsqrtf(d2.x), rsqrtf(d2.y)), esp);
+      const float2 gap = __fadd2_rn(d2, rp2[j]);
+      gap0 = fminf(gap0, gap.x);
+      gap1 = fminf(gap1, gap.y);
     }
-    if (!blocked) {
-      const float diff = fmaf(-coulomb, esp, f.w);
+    if (gap0 >= 0.f) {
+      const float diff = fmaf(-coulomb, esp.x, fa.w);
+      total += ex2(nkl * diff * diff);
+    }
+    if (has1 && gap1 >= 0.f) {
+      const float diff = fmaf(-coulomb, esp.y, fb.w);
       total += ex2(nkl * diff * diff);
     }
   }
@@ -373,7 +395,6 @@ __device__ __forceinline__ void step_combo(PoseState& s, const Reduced& ms, floa
 // ---------------------------------------------------------------------------------------
 constexpr float kFactorMax = 96.f;
 
-__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
 template <int JB, bool ESP>
 __device__ __forceinline__ void shape_chunk_plain(const float4* __restrict__ sPd,
