@@ -169,9 +169,9 @@ def flush_l2(buf):
 
 
 # DRAM bytes (read + write) per pair of one fused-kernel launch, from an ncu capture of the
-# same workload at 256 pairs (dram__bytes_read.sum + dram__bytes_write.sum = 4.14 MB +
-# 0.23 MB), scaled by pairs; the kernel's traffic grows with the pairs it processes.
-DRAM_BYTES_PER_PAIR = {"surf_esp": (4.14336e6 + 2.3424e5) / 256}
+# same workload at 256 pairs (dram__bytes_read.sum + dram__bytes_write.sum = 3.318 MB + 0 B),
+# scaled by pairs; the kernel's traffic grows with the pairs it processes.
+DRAM_BYTES_PER_PAIR = {"surf_esp": (3.318272e6 + 0.0) / 256}
 
 
 def run_cuda(args, wl):
