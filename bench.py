@@ -50,6 +50,12 @@ WORKLOADS = {
                       lr=0.1, alpha=0.81, lam=0.0,
                       desc="combined shape+pharmacophore: 16384 pairs, 15-60 atoms + 3-20 "
                            "features, 50 starts x 200 Adam steps"),
+    "score_grad": dict(mode="score_grad", pairs=1024, lo=60, hi=300, starts=1, steps=1,
+                       lr=0.0, alpha=0.81, lam=0.3,
+                       desc="differentiable scoring: 1024 queries of 60 atoms + 300 surface "
+                            "points (charges N(0, 0.1^2)) vs 4 fixed targets; vol Tanimoto "
+                            "(alpha 0.81) + surface ESP Tanimoto (alpha 1.216) and their "
+                            "coordinate/charge gradients"),
     "vol_and_surf_esp": dict(mode="vol_and_surf_esp", pairs=4096, lo=10, hi=25, starts=8,
                              steps=60, lr=0.1, alpha=0.81, lam=0.001,
                              desc="ShaEP combo: 4096 pairs, 10-25 heavy atoms (+H), 100-200 "
@@ -545,6 +551,141 @@ def server_bench(dev, duration=20.0, n_lib=1_000_000, load=0.6, seed=7):
             "library_build_s": round(gen_s, 1)}
 
 
+def _score_grad_inputs(nq, seed, n_atoms=60, n_surf=300, nt=4):
+    from fast_shepherd_score_b200 import synthetic as syn
+    rng = np.random.default_rng(seed)
+    atoms = syn.ball_clouds(rng, [n_atoms] * (nq + nt))
+    surf = syn.sphere_clouds(rng, [n_surf] * (nq + nt))
+    A = np.stack(atoms).astype(np.float32)
+    S = np.stack([p for p, _ in surf]).astype(np.float32)
+    Q = np.stack([c for _, c in surf]).astype(np.float32)
+    tgt = np.arange(nq) % nt
+    return A, S, Q, tgt
+
+
+def run_score_grad(args, wl):
+    """Differentiable scoring: one step = forward (vol + surface ESP Tanimoto of every query
+    against its target) and backward (d score / d coordinates and charges) through
+    fast_shepherd_score_b200.autograd.  Work units: pair-terms of the forward and the adjoint
+    (each one MUFU ex2)."""
+    import torch
+    import torch.distributed as dist
+    from fast_shepherd_score_b200 import autograd as AG
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    nq = args.pairs or wl["pairs"]
+    A, S, Q, tgt = _score_grad_inputs(nq, 1 + rank)
+    terms = int(2 * nq * (A.shape[1] ** 2 + S.shape[1] ** 2))
+    surf_alpha, lam = 1.216, wl["lam"] * AG.LAM_SCALING
+
+    def step(qa, qs, qc, ta, ts, tc):
+        qa.grad = qs.grad = qc.grad = None
+        vol = AG.get_overlap(ta, qa, alpha=wl["alpha"])
+        esp = AG.get_overlap_esp(ts, qs, tc, qc, alpha=surf_alpha, lam=lam)
+        (vol.sum() + esp.sum()).backward()
+        return vol, esp
+
+    Ad, Sd, Qd = (torch.from_numpy(x).to(dev) for x in (A, S, Q))
+    ti = torch.from_numpy(tgt).to(dev)
+    ta, ts, tc = Ad[nq:][ti], Sd[nq:][ti], Qd[nq:][ti]
+    qa, qs, qc = (x[:nq].clone().requires_grad_(True) for x in (Ad, Sd, Qd))
+    l2 = torch.empty(64 << 20, device=dev)
+    for _ in range(args.warmup):
+        step(qa, qs, qc, ta, ts, tc)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local).start()
+    times = []
+    for _ in range(args.steps):
+        flush_l2(l2)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step(qa, qs, qc, ta, ts, tc)
+        e1.record()
+        times.append((e0, e1))
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    t_max = torch.tensor([sum(a.elapsed_time(b) for a, b in times)], device=dev,
+                         dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    ms_per_step = float(t_max.item()) / args.steps
+    value = nq * world / (ms_per_step * 1e-3)
+
+    # end to end: pinned host queries -> device -> scores + gradients back on the host
+    hq = [torch.from_numpy(x[:nq]).pin_memory() for x in (A, S, Q)]
+    e2e_ms = []
+    for i in range((max(1, min(args.steps, 3)) + 1) if args.e2e else 0):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        a, s_, c = (x.to(dev, non_blocking=True).requires_grad_(True) for x in hq)
+        vol, esp = step(a, s_, c, ta, ts, tc)
+        out = [vol.detach().cpu(), esp.detach().cpu(), a.grad.cpu(), s_.grad.cpu(), c.grad.cpu()]
+        t1 = time.perf_counter()
+        if i:
+            e2e_ms.append((t1 - t0) * 1e3)
+    e2e_t = torch.tensor([statistics.median(e2e_ms) if e2e_ms else float("nan")], device=dev,
+                         dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    if rank != 0:
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return None
+    peak = measure_peak(dev)
+    achieved = terms / (ms_per_step * 1e-3)
+    h2d = sum(x.nbytes for x in hq)
+    d2h = nq * 4 * 2 + h2d
+    line = {
+        "metric": "scored queries/s (vol + surface-ESP Tanimoto with coordinate and charge "
+                  "gradients)",
+        "value": round(value, 2), "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": wl["desc"], "mode": "score_grad", "queries_per_gpu": nq,
+                   "l2": "flushed between timed steps (256 MB write outside timed windows)",
+                   "parallelism": f"dp{world} (independent query shards, no collective)"},
+        "e2e": {"value": round(nq * world / (float(e2e_t.item()) * 1e-3), 2), "unit": "queries/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "api": "fast_shepherd_score_b200.autograd.get_overlap / get_overlap_esp"},
+        "gpu_launches": 4 * args.steps,
+        "roofline": {"bound": "mufu", "achieved": round(achieved / 1e9, 1),
+                     "peak": round(peak["ex2"] / 1e9, 1), "unit": "Gterm/s",
+                     "frac": round(achieved / peak["ex2"], 4), "traffic": None,
+                     "peak_source": "measured ex2 rate; step time includes torch's packing of "
+                                    "the query tensors",
+                     "terms_per_step": terms},
+        "clocks": clk,
+    }
+    if args.cpu_baseline and world == 1:
+        from oracle import scores as osc
+        k, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < min(args.cpu_seconds, 10.0) and k < nq:
+            i = nq + int(tgt[k])
+            osc.shape_tanimoto_grad(A[i], A[k], wl["alpha"])
+            osc.esp_tanimoto_grad(S[i], S[k], Q[i], Q[k], surf_alpha, lam)
+            k += 1
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": round(k / dt, 3), "unit": "queries/s", "cores": 1,
+                                "kind": "port",
+                                "sample": f"{k} queries (fp64 numpy restatement of the "
+                                          "reference's torch scoring and its gradients, one "
+                                          "thread)"}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return line
+
+
 def run_esp_combo(args, wl):
     """vol_and_surf_esp: device-resident step (self overlaps + seeds + fused kernel + pick) and
     an end-to-end leg from pinned host arrays (H2D of every cloud, align, D2H of the results).
@@ -692,12 +833,47 @@ def run_esp_combo(args, wl):
     return line
 
 
+def _reference_score_grad(args, wl, world):
+    """CPU arm of the differentiable-scoring workload: the fp64 numpy restatement of the
+    reference's torch scores and gradients, one thread, bounded sample per step."""
+    from fast_shepherd_score_b200.autograd import LAM_SCALING
+    from oracle import scores as osc
+    nq = args.pairs or wl["pairs"]
+    A, S, Q, tgt = _score_grad_inputs(nq, 1)
+    budget = max(0.5, args.cpu_seconds / max(1, args.steps + args.warmup))
+    rates = []
+    for it in range(args.warmup + args.steps):
+        k, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < budget and k < nq:
+            i = nq + int(tgt[k])
+            osc.shape_tanimoto_grad(A[i], A[k], wl["alpha"])
+            osc.esp_tanimoto_grad(S[i], S[k], Q[i], Q[k], 1.216, wl["lam"] * LAM_SCALING)
+            k += 1
+        if it >= args.warmup:
+            rates.append(k / (time.perf_counter() - t0))
+    value = statistics.median(rates)
+    line = {"impl": "reference", "metric": "scored queries/s (vol + surface-ESP Tanimoto with "
+                                           "coordinate and charge gradients)",
+            "value": round(value, 3), "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1e3 * nq / value, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": {"workload": wl["desc"], "mode": "score_grad"},
+            "cpu_baseline": {"value": round(value, 3), "unit": "queries/s", "cores": 1,
+                             "kind": "port", "sample": f"{budget:.1f} s of queries per step"},
+            "e2e": {"value": round(value, 3), "unit": "queries/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return line
+
+
 def run_reference(args, wl):
     """The CPU implementation of the path (oracle port of the reference numba path)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
+    if wl["mode"] == "score_grad":
+        return _reference_score_grad(args, wl, world)
     from oracle import _lib as ol
     ol.build()
     cores = ol.max_threads()
@@ -758,6 +934,8 @@ def main(argv=None):
         return run_reference(args, wl)
     if wl["mode"] == "vol_and_surf_esp":
         return run_esp_combo(args, wl)
+    if wl["mode"] == "score_grad":
+        return run_score_grad(args, wl)
     return run_cuda(args, wl)
 
 
