@@ -30,7 +30,8 @@ from .modes import CANONICAL_MODES, canonical, seeds_for, steps_for
 Hit = namedtuple("Hit", ["score", "id", "transform"])
 
 _SURF_ALPHA_MODES = {"surf", "surf_esp"}
-_SCREEN_MODES = ("vol", "vol_esp", "surf", "surf_esp", "pharm", "vol_color", "vol_pharm")
+_SCREEN_MODES = ("vol", "vol_esp", "surf", "surf_esp", "vol_and_surf_esp", "pharm", "vol_color",
+                 "vol_pharm")
 
 
 def ALPHA(num_points):
@@ -69,6 +70,9 @@ def _supports(schema, mode) -> bool:
         return schema["surf"] and schema["surf_esp"]
     if mode in ("pharm", "vol_color", "vol_pharm"):
         return schema["pharm"]
+    if mode == "vol_and_surf_esp":
+        return (schema["surf"] and schema["surf_esp"] and schema["centers_w_H"]
+                and schema["radii"] and schema["charges"] and schema["with_H"])
     return False
 
 
@@ -91,8 +95,6 @@ class ProfileStore:
         if dtype not in ("float16", "float32"):
             raise ValueError("dtype must be 'float16' or 'float32'")
         schema = _schema_from_modes(modes)
-        if schema["with_H"]:
-            raise ValueError("vol_and_surf_esp stores are not written by this package")
         os.makedirs(path, exist_ok=True)
         mpath = os.path.join(path, cls.MANIFEST)
         if os.path.exists(mpath) and not overwrite:
@@ -110,15 +112,26 @@ class ProfileStore:
         return st
 
     def add_arrays(self, *, atom_pos, surf_pos=None, surf_esp=None, partial_charges=None,
-                   pharm_types=None, pharm_ancs=None, pharm_vecs=None, id=None) -> None:
+                   pharm_types=None, pharm_ancs=None, pharm_vecs=None, centers_w_H=None,
+                   radii=None, nonH_atoms_idx=None, id=None) -> None:
         """Buffer one molecule given as arrays (centred on its atom COM when the store is
-        pre-centred, as the reference's writer does)."""
+        pre-centred, as the reference's writer does).  Stores with hydrogens
+        (vol_and_surf_esp) take ``partial_charges``, ``radii`` and ``centers_w_H`` for all
+        atoms and ``nonH_atoms_idx`` (default: the first len(atom_pos) atoms are the heavy
+        ones)."""
         if self._rw != "w":
             raise RuntimeError("store is open for reading")
         rec = dict(atom_pos=np.asarray(atom_pos, np.float32), surf_pos=surf_pos,
                    surf_esp=surf_esp, partial_charges=partial_charges, pharm_types=pharm_types,
-                   pharm_ancs=pharm_ancs, pharm_vecs=pharm_vecs,
+                   pharm_ancs=pharm_ancs, pharm_vecs=pharm_vecs, centers_w_H=centers_w_H,
+                   radii=radii, nonH=nonH_atoms_idx,
                    id=self._n + len(self._buf) if id is None else id)
+        if self.manifest["schema"]["with_H"]:
+            if centers_w_H is None or radii is None or partial_charges is None:
+                raise ValueError("a store with hydrogens needs centers_w_H, radii and "
+                                 "partial_charges for every atom")
+            if rec["nonH"] is None:
+                rec["nonH"] = np.arange(len(rec["atom_pos"]), dtype=np.int64)
         if self.manifest["pre_centered"]:
             c = rec["atom_pos"].mean(0)
             rec["atom_pos"] = rec["atom_pos"] - c
@@ -126,6 +139,8 @@ class ProfileStore:
                 rec["surf_pos"] = np.asarray(surf_pos, np.float32) - c
             if pharm_ancs is not None:
                 rec["pharm_ancs"] = np.asarray(pharm_ancs, np.float32) - c
+            if centers_w_H is not None:
+                rec["centers_w_H"] = np.asarray(centers_w_H, np.float32) - c
         self._buf.append(rec)
         if len(self._buf) >= self.manifest["shard_size"]:
             self._flush()
@@ -159,7 +174,17 @@ class ProfileStore:
             out["surf_pos"] = np.stack([r["surf_pos"] for r in recs]).astype(dt)
         if sch["surf_esp"]:
             out["surf_esp"] = np.stack([r["surf_esp"] for r in recs]).astype(dt)
-        if sch["charges"]:
+        if sch["charges"] and sch["with_H"]:
+            # layout of the reference's writer (screen.py:470-481): all-atom arrays with their
+            # own offsets, heavy-atom indices into them
+            out["all_off"] = off([len(r["partial_charges"]) for r in recs])
+            out["charges"] = np.concatenate([r["partial_charges"] for r in recs]).astype(dt)
+            out["nonH"] = np.concatenate([r["nonH"] for r in recs]).astype(np.int64)
+            if sch["radii"]:
+                out["radii"] = np.concatenate([r["radii"] for r in recs]).astype(dt)
+            if sch["centers_w_H"]:
+                out["cwh"] = np.concatenate([r["centers_w_H"] for r in recs]).astype(dt)
+        elif sch["charges"]:
             out["charges"] = np.concatenate([r["partial_charges"] for r in recs]).astype(dt)
         if sch["pharm"]:
             out["pharm_off"] = off([len(r["pharm_types"]) for r in recs])
@@ -261,8 +286,17 @@ def _pharm_from_csr(types, ancs, vecs, off, device, with_vectors=True) -> PharmS
                     int(n.max()) if len(n) else 0)
 
 
-def shard_to_device(arrs: dict, mode: str, device):
-    """(fit CloudSet or None, fit PharmSet or None) of one shard for `mode`."""
+def shard_to_device(arrs: dict, mode: str, device, alpha: float = 0.81):
+    """(fit CloudSet or None, fit PharmSet or None, extra kwargs) of one shard for `mode`;
+    vol_and_surf_esp adds the atoms with hydrogens, their radii and the surfaces."""
+    if mode == "vol_and_surf_esp":
+        # shape centres: heavy atoms at alpha 0.81, else the surface (aligners.py:795-803)
+        surf = _cloud_from_dense(arrs["surf_pos"], device, arrs["surf_esp"])
+        cs = (_cloud_from_csr(arrs["atom_pos"], arrs["atom_off"], device) if alpha == 0.81
+              else _cloud_from_dense(arrs["surf_pos"], device))
+        atoms = _cloud_from_csr(arrs["cwh"], arrs["all_off"], device, arrs["charges"])
+        return cs, None, dict(fit_atoms=atoms, fit_radii=_dev(arrs["radii"], device),
+                              fit_surf=surf)
     if mode in ("vol", "vol_color", "vol_pharm"):
         cs = _cloud_from_csr(arrs["atom_pos"], arrs["atom_off"], device)
     elif mode == "vol_esp":
@@ -277,13 +311,25 @@ def shard_to_device(arrs: dict, mode: str, device):
     if mode in ("pharm", "vol_color", "vol_pharm"):
         ps = _pharm_from_csr(arrs["pharm_types"], arrs["pharm_ancs"], arrs["pharm_vecs"],
                              arrs["pharm_off"], device, with_vectors=(mode != "vol_color"))
-    return cs, ps
+    return cs, ps, {}
 
 
-def query_to_device(q, mode: str, device):
+def query_to_device(q, mode: str, device, alpha: float = 0.81):
     """One query molecule (attributes atom_pos / surf_pos / surf_esp / partial_charges /
-    pharm_types / pharm_ancs / pharm_vecs) as a one-molecule (CloudSet, PharmSet)."""
+    pharm_types / pharm_ancs / pharm_vecs, and centers_w_H / radii for vol_and_surf_esp) as a
+    one-molecule (CloudSet, PharmSet, extra kwargs)."""
     g = lambda name: getattr(q, name, None) if not isinstance(q, dict) else q.get(name)
+    if mode == "vol_and_surf_esp":
+        cwh = g("centers_w_H")
+        if cwh is None and g("mol") is not None:
+            cwh = g("mol").GetConformer().GetPositions()
+        cs = CloudSet.from_arrays([g("atom_pos") if alpha == 0.81 else g("surf_pos")],
+                                  device=device)
+        atoms = CloudSet.from_arrays([np.asarray(cwh, np.float32)], [g("partial_charges")],
+                                     device=device)
+        surf = CloudSet.from_arrays([g("surf_pos")], [g("surf_esp")], device=device)
+        radii = torch.as_tensor(np.asarray(g("radii"), np.float32), device=device)
+        return cs, None, dict(ref_atoms=atoms, ref_radii=radii, ref_surf=surf)
     cs = ps = None
     if mode in ("vol", "vol_color", "vol_pharm"):
         cs = CloudSet.from_arrays([g("atom_pos")], device=device)
@@ -297,7 +343,7 @@ def query_to_device(q, mode: str, device):
         ps = PharmSet.from_arrays([g("pharm_types")], [g("pharm_ancs")],
                                   None if mode == "vol_color" else [g("pharm_vecs")],
                                   device=device)
-    return cs, ps
+    return cs, ps, {}
 
 
 def _centred_query(q):
@@ -305,10 +351,14 @@ def _centred_query(q):
     get = (lambda n: q.get(n)) if isinstance(q, dict) else (lambda n: getattr(q, n, None))
     c = np.asarray(get("atom_pos"), np.float32).mean(0)
     out = {}
+    cwh = get("centers_w_H")
+    if cwh is None and get("mol") is not None:
+        cwh = get("mol").GetConformer().GetPositions()
+    out["centers_w_H"] = None if cwh is None else np.asarray(cwh, np.float32) - c
     for n in ("atom_pos", "surf_pos", "pharm_ancs"):
         v = get(n)
         out[n] = None if v is None else np.asarray(v, np.float32) - c
-    for n in ("surf_esp", "partial_charges", "pharm_types", "pharm_vecs"):
+    for n in ("surf_esp", "partial_charges", "pharm_types", "pharm_vecs", "radii"):
         out[n] = get(n)
     return out
 
@@ -347,6 +397,10 @@ def _batch_kwargs(mode, ak, alpha):
         kw["lam"] = ak["lam"]
     if mode in ("vol_color", "vol_pharm"):
         kw["color_weight"] = ak.get("color_weight", 0.5)
+    if mode == "vol_and_surf_esp":
+        kw.update(alpha=alpha, lam=ak.get("lam", 0.001),
+                  probe_radius=ak.get("probe_radius", 1.0),
+                  esp_weight=ak.get("esp_weight", 0.5), esp_stride=ak.get("esp_stride", 1))
     return kw
 
 
@@ -375,6 +429,8 @@ def screen_many(queries: Sequence, store: ProfileStore, mode: str = "surf_esp", 
     if mode == "vol_esp" and "lam" not in align_kwargs:
         raise ValueError("vol_esp requires an explicit lam=...")
     if alpha is None:
+        # vol_and_surf_esp takes alpha explicitly in the reference; 0.81 selects the heavy-atom
+        # shape centres
         alpha = ALPHA(store.num_surf_points) if mode in _SURF_ALPHA_MODES else 0.81
     device = torch.device(device or "cuda")
     center = (not store.pre_centered) if do_center is None else bool(do_center)
@@ -384,19 +440,20 @@ def screen_many(queries: Sequence, store: ProfileStore, mode: str = "surf_esp", 
     if scores_out is not None:
         so = [scores_out] if isinstance(scores_out, np.ndarray) and len(qs) == 1 else list(scores_out)
     heaps = [_TopK(top_k) for _ in qs]
-    qdev = [query_to_device(q, mode, device) for q in qs]
+    qdev = [query_to_device(q, mode, device, alpha) for q in qs]
     done = 0
     for si in range(store.num_shards):
         sh, arrs = store.read_shard(si)
         if center and not store.pre_centered:
             arrs = _center_shard(arrs, mode)
-        fit, fit_ph = shard_to_device(arrs, mode, device)
+        fit, fit_ph, fit_x = shard_to_device(arrs, mode, device, alpha)
         K = int(sh["n"])
         pr = torch.zeros(K, dtype=torch.int32, device=device)
         pf = torch.arange(K, dtype=torch.int32, device=device)
         ids = arrs["ids"]
-        for qi, (rc, rp) in enumerate(qdev):
-            sc, q, t = api.align_device(mode, rc, fit, rp, fit_ph, pr, pf, **kw)
+        for qi, (rc, rp, ref_x) in enumerate(qdev):
+            sc, q, t = api.align_device(mode, rc, fit, rp, fit_ph, pr, pf, **kw, **ref_x,
+                                        **fit_x)
             if so[qi] is not None:
                 so[qi][sh["start"]:sh["start"] + K] = sc.cpu().numpy()
             k = min(top_k, K)
@@ -434,6 +491,9 @@ def _center_shard(arrs, mode):
     if "pharm_ancs" in arrs:
         pn = np.diff(arrs["pharm_off"])
         arrs["pharm_ancs"] = arrs["pharm_ancs"].astype(np.float32) - c[np.repeat(np.arange(len(pn)), pn)]
+    if "cwh" in arrs:
+        an = np.diff(arrs["all_off"])
+        arrs["cwh"] = arrs["cwh"].astype(np.float32) - c[np.repeat(np.arange(len(an)), an)]
     return arrs
 
 

@@ -130,3 +130,34 @@ def test_object_api_matches_driver(cuda):
     np.testing.assert_allclose(scores, sc.cpu().numpy(), atol=1e-6)
     s2, _ = MoleculePairBatch(pairs).align_with_esp_combo(alpha=0.81, backend="cuda")
     np.testing.assert_allclose(s2, scores, atol=1e-6)
+
+
+def test_screen_matches_driver(tmp_path, cuda):
+    """screen() over a vol_and_surf_esp ProfileStore returns the driver's scores for every
+    library molecule (same seeds, steps and tile; float32 store, no centring)."""
+    from test_store import _combo_store
+    from fast_shepherd_score_b200.screen import screen
+    rng = np.random.default_rng(8)
+    mols = syn.esp_combo_molecules(12, rng, surf_lo=120, surf_hi=120)
+    st = _combo_store(str(tmp_path / "c.fss"), mols, shard_size=5)
+    q = dict(atom_pos=mols[0]["centers"], surf_pos=mols[0]["surf"],
+             surf_esp=mols[0]["surf_esp"], partial_charges=mols[0]["charges"],
+             radii=mols[0]["radii"], centers_w_H=mols[0]["atoms"])
+    out = np.zeros(len(mols), np.float32)
+    hits = screen(q, st, mode="vol_and_surf_esp", do_center=False, top_k=5, scores_out=out,
+                  num_repeats=8, max_num_steps=30, lr=0.1)
+    assert len(hits) == 5 and hits[0].id == 0 and hits[0].score > 0.9
+    pad = lambda xs: torch.nn.utils.rnn.pad_sequence([torch.as_tensor(x) for x in xs],
+                                                      batch_first=True).to(cuda)
+    n = lambda xs: torch.tensor([len(x) for x in xs], device=cuda)
+    get = lambda k: [m[k] for m in mols]
+    rep = lambda k: [mols[0][k]] * len(mols)
+    sc, _, _ = al.coarse_fine_esp_combo_align_many(
+        pad(rep("atoms")), pad(get("atoms")), pad(rep("centers")), pad(get("centers")),
+        pad(rep("surf")), pad(get("surf")), pad(rep("charges")), pad(get("charges")),
+        pad(rep("surf_esp")), pad(get("surf_esp")), pad(rep("radii")), pad(get("radii")),
+        alpha=0.81, lam=0.001, num_seeds=8, steps_fine=30, lr=0.1,
+        N_real_centers=n(rep("centers")), M_real_centers=n(get("centers")),
+        N_real_atoms_w_H_1=n(rep("atoms")), M_real_atoms_w_H_2=n(get("atoms")),
+        N_real_surf_1=n(rep("surf")), M_real_surf_2=n(get("surf")))
+    np.testing.assert_allclose(out, sc.cpu().numpy(), atol=1e-5)

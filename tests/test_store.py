@@ -85,3 +85,42 @@ def test_pre_centred_store_and_query(tmp_path):
     np.testing.assert_allclose(b["atom_pos"], a["atom_pos"], atol=1e-5)
     np.testing.assert_allclose(b["surf_pos"], a["surf_pos"], atol=1e-5)
     np.testing.assert_allclose(b["pharm_ancs"], a["pharm_ancs"], atol=1e-5)
+
+
+def _combo_store(path, mols, dtype="float32", pre_centered=False, shard_size=7):
+    with ProfileStore.create(path, num_surf_points=len(mols[0]["surf"]),
+                             modes=["vol_and_surf_esp"], dtype=dtype, shard_size=shard_size,
+                             pre_centered=pre_centered) as st:
+        for m in mols:
+            st.add_arrays(atom_pos=m["centers"], surf_pos=m["surf"], surf_esp=m["surf_esp"],
+                          partial_charges=m["charges"], radii=m["radii"],
+                          centers_w_H=m["atoms"])
+    return ProfileStore.open(path)
+
+
+def test_with_hydrogens_store_round_trip(tmp_path):
+    """vol_and_surf_esp stores keep all-atom charges, radii and positions with their own
+    offsets and the heavy-atom index (the reference writer's layout)."""
+    rng = np.random.default_rng(3)
+    mols = syn.esp_combo_molecules(16, rng, surf_lo=80, surf_hi=80)
+    st = _combo_store(str(tmp_path / "combo.fss"), mols)
+    assert st.supports("vol_and_surf_esp") and st.supports("surf_esp") and st.supports("vol")
+    assert not st.supports("pharm")
+    k = 0
+    for s in range(st.num_shards):
+        sh, a = st.read_shard(s)
+        for i in range(sh["n"]):
+            m = mols[k + i]
+            a0, a1 = a["all_off"][i], a["all_off"][i + 1]
+            np.testing.assert_array_equal(a["cwh"][a0:a1], m["atoms"])
+            np.testing.assert_array_equal(a["charges"][a0:a1], m["charges"])
+            np.testing.assert_array_equal(a["radii"][a0:a1], m["radii"])
+            h0, h1 = a["atom_off"][i], a["atom_off"][i + 1]
+            np.testing.assert_array_equal(a["atom_pos"][h0:h1], m["centers"])
+            np.testing.assert_array_equal(a["surf_esp"][i], m["surf_esp"])
+        k += sh["n"]
+    with pytest.raises(ValueError):
+        with ProfileStore.create(str(tmp_path / "bad.fss"), num_surf_points=80,
+                                 modes=["vol_and_surf_esp"]) as bad:
+            bad.add_arrays(atom_pos=mols[0]["centers"], surf_pos=mols[0]["surf"],
+                           surf_esp=mols[0]["surf_esp"])
