@@ -97,6 +97,15 @@ def candidates(mode: str, max_fit: int, n_starts: int):
             if 2 * base <= n_starts:
                 out.append({"lanes_per_pose": lpp, "chunks": 2 * base, "cta_per_sm": 0,
                             "kernel_variant": var})
+            # small molecules (cheap candidates): start blocks that fill whole warps, so no
+            # lanes shadow an idle start except in a pair's last block
+            if max_fit < 64:
+                for warps in (1, 2):
+                    ppc = warps * (32 // lpp)
+                    ch = -(-n_starts // ppc)
+                    if ch not in (base, 2 * base) and ch <= n_starts:
+                        out.append({"lanes_per_pose": lpp, "chunks": ch, "cta_per_sm": 0,
+                                    "kernel_variant": var})
     if mode in ("shape", "esp") and max_fit >= 16:
         base = _auto_chunks(32, n_starts)
         for ch, cps in ((0, 0), (0, 1), (2 * base, 0)):
