@@ -70,6 +70,10 @@ _SIGS = {
                       ctypes.c_int),
     "fss_score_bwd": ([_vp] * 6 + [_i32, _i32, _i32, _f32, _i32, _f32] + [_vp] * 5,
                       ctypes.c_int),
+    "fss_score_fwd_dense": ([_vp, _vp, _i32, _vp, _vp, _i32, _vp, _vp, _i32, _f32, _i32, _f32,
+                             _vp, _vp, _vp], ctypes.c_int),
+    "fss_score_bwd_dense": ([_vp, _vp, _i32, _vp, _vp, _i32, _vp, _vp, _i32, _f32, _i32, _f32]
+                            + [_vp] * 7, ctypes.c_int),
     "fss_probe_peak": ([_i32, _i32, _i32, _vp, ctypes.POINTER(ctypes.c_longlong), _vp],
                        ctypes.c_int),
 }

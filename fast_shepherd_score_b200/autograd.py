@@ -12,7 +12,9 @@ torch ops that pack them.
 * :func:`tanimoto_packed` -- P pairs of molecules in two packed sets (the general form; a
   fixed target shared by many queries is one molecule of the ref set).
 * :func:`get_overlap`, :func:`get_overlap_esp` -- the reference's signatures for one pair
-  ((N,3) vs (M,3)) or a matched batch ((B,N,3) vs (B,M,3)).
+  ((N,3) vs (M,3)) or a matched batch ((B,N,3) vs (B,M,3)); :class:`DenseTanimoto` runs them
+  on the padded tensors directly (``fss_score_fwd_dense`` / ``fss_score_bwd_dense``), with no
+  packing and gradients written straight into the input shapes.
 """
 from __future__ import annotations
 
@@ -85,13 +87,59 @@ def tanimoto_packed(ref_pts, ref_off, fit_pts, fit_off, pair_ref, pair_fit, *, a
     return (score, ov) if return_overlaps else score
 
 
-def _pack(x, c=None):
-    """(B, N, 3) [+ (B, N)] -> differentiable (B*N, 4) float4 rows and offsets."""
-    B, N, _ = x.shape
-    w = c.reshape(B, N, 1) if c is not None else torch.zeros(B, N, 1, dtype=x.dtype, device=x.device)
-    pts = torch.cat([x, w.to(x.dtype)], -1).reshape(B * N, 4).to(_f32)
-    off = torch.arange(0, (B + 1) * N, N, dtype=_i32, device=x.device)
-    return pts, off
+_IDX_CACHE: dict = {}
+
+
+def _pair_index(B, n_mol, device):
+    """Cached int32 molecule index of each pair: identity, or 0 for a broadcast molecule."""
+    key = (device, B, n_mol)
+    t = _IDX_CACHE.get(key)
+    if t is None:
+        t = (torch.arange(B, dtype=_i32, device=device) if n_mol == B
+             else torch.zeros(B, dtype=_i32, device=device))
+        _IDX_CACHE[key] = t
+    return t
+
+
+class DenseTanimoto(torch.autograd.Function):
+    """score_b = V_AB / (V_AA + V_BB - V_AB) for padded (B, N, 3) / (B, M, 3) batches (either
+    side may be a single molecule broadcast over the batch); optional (B, N) charges."""
+
+    @staticmethod
+    def forward(ctx, x1, x2, q1, q2, alpha, inv_lam):
+        esp = q1 is not None
+        B = max(x1.shape[0], x2.shape[0])
+        dev = x1.device
+        x1, x2 = x1.to(_f32).contiguous(), x2.to(_f32).contiguous()
+        q1 = q1.to(_f32).contiguous() if esp else None
+        q2 = q2.to(_f32).contiguous() if esp else None
+        pr, pf = _pair_index(B, x1.shape[0], dev), _pair_index(B, x2.shape[0], dev)
+        score = torch.empty(B, dtype=_f32, device=dev)
+        ov = torch.empty(B, 3, dtype=_f32, device=dev)
+        check(_lib.load().fss_score_fwd_dense(
+            ptr(x1), ptr(q1) if esp else None, x1.shape[1], ptr(x2),
+            ptr(q2) if esp else None, x2.shape[1], ptr(pr, _i32), ptr(pf, _i32), B,
+            float(alpha), int(esp), float(inv_lam), ptr(score), ptr(ov), stream_ptr(dev)),
+            "score_fwd_dense")
+        ctx.save_for_backward(x1, x2, q1, q2, pr, pf, ov)
+        ctx.cfg = (float(alpha), esp, float(inv_lam))
+        return score
+
+    @staticmethod
+    def backward(ctx, g_score):
+        x1, x2, q1, q2, pr, pf, ov = ctx.saved_tensors
+        alpha, esp, inv_lam = ctx.cfg
+        g1, g2 = torch.zeros_like(x1), torch.zeros_like(x2)
+        gq1 = torch.zeros_like(q1) if esp else None
+        gq2 = torch.zeros_like(q2) if esp else None
+        g = g_score.to(_f32).contiguous()
+        check(_lib.load().fss_score_bwd_dense(
+            ptr(x1), ptr(q1) if esp else None, x1.shape[1], ptr(x2),
+            ptr(q2) if esp else None, x2.shape[1], ptr(pr, _i32), ptr(pf, _i32),
+            int(pr.shape[0]), alpha, int(esp), inv_lam, ptr(ov), ptr(g), ptr(g1),
+            ptr(gq1) if esp else None, ptr(g2), ptr(gq2) if esp else None,
+            stream_ptr(x1.device)), "score_bwd_dense")
+        return g1, g2, gq1, gq2, None, None
 
 
 def _batched(c1, c2, q1=None, q2=None):
@@ -110,13 +158,9 @@ def _score(c1, c2, q1, q2, alpha, lam):
     c1, c2, q1, q2, B, single = _batched(c1, c2, q1, q2)
     if not (c1.is_cuda and c2.is_cuda):
         raise ValueError("fast_shepherd_score_b200 scores CUDA tensors only")
-    r, roff = _pack(c1, q1)
-    f, foff = _pack(c2, q2)
-    idx = torch.arange(B, dtype=_i32, device=c1.device)
-    pr = idx if c1.shape[0] == B else torch.zeros(B, dtype=_i32, device=c1.device)
-    pf = idx if c2.shape[0] == B else torch.zeros(B, dtype=_i32, device=c1.device)
-    s = tanimoto_packed(r, roff, f, foff, pr, pf, alpha=alpha, lam=lam,
-                        max_ref=c1.shape[1], max_fit=c2.shape[1])
+    if c1.shape[0] not in (1, B) or c2.shape[0] not in (1, B):
+        raise ValueError("batch sizes must match or be 1")
+    s = DenseTanimoto.apply(c1, c2, q1, q2, alpha, 1.0 / float(lam) if lam is not None else 0.0)
     s = s.to(c1.dtype) if c1.dtype != _f32 else s
     return s[0] if single else s
 

@@ -63,6 +63,17 @@ int score_bwd_launch(const float* ref_pts, const int32_t* ref_off, const float* 
                      int P, int maxN, int maxM, float alpha, int esp, float inv_lam,
                      const float* overlaps, const float* grad_score, float* grad_ref,
                      float* grad_fit, cudaStream_t st);
+int score_fwd_dense_launch(const float* ref_xyz, const float* ref_q, int ref_n,
+                           const float* fit_xyz, const float* fit_q, int fit_n,
+                           const int32_t* pair_ref, const int32_t* pair_fit, int P, float alpha,
+                           int esp, float inv_lam, float* score, float* overlaps,
+                           cudaStream_t st);
+int score_bwd_dense_launch(const float* ref_xyz, const float* ref_q, int ref_n,
+                           const float* fit_xyz, const float* fit_q, int fit_n,
+                           const int32_t* pair_ref, const int32_t* pair_fit, int P, float alpha,
+                           int esp, float inv_lam, const float* overlaps, const float* grad_score,
+                           float* grad_ref_xyz, float* grad_ref_q, float* grad_fit_xyz,
+                           float* grad_fit_q, cudaStream_t st);
 
 int probe_launch(int which, int iters, int blocks_per_sm, float* out, long long* ops,
                  cudaStream_t st);
@@ -168,6 +179,28 @@ int fss_score_bwd(const float* ref_pts, const int32_t* ref_off, const float* fit
   FSS_GUARD(fss::score_bwd_launch(ref_pts, ref_off, fit_pts, fit_off, pair_ref, pair_fit,
                                   n_pairs, max_ref_points, max_fit_points, alpha, esp, inv_lam,
                                   overlaps, grad_score, grad_ref, grad_fit, S(stream)));
+}
+
+int fss_score_fwd_dense(const float* ref_xyz, const float* ref_q, int32_t ref_points,
+                        const float* fit_xyz, const float* fit_q, int32_t fit_points,
+                        const int32_t* pair_ref, const int32_t* pair_fit, int32_t n_pairs,
+                        float alpha, int32_t esp, float inv_lam, float* score, float* overlaps,
+                        void* stream) {
+  FSS_GUARD(fss::score_fwd_dense_launch(ref_xyz, ref_q, ref_points, fit_xyz, fit_q, fit_points,
+                                        pair_ref, pair_fit, n_pairs, alpha, esp, inv_lam, score,
+                                        overlaps, S(stream)));
+}
+
+int fss_score_bwd_dense(const float* ref_xyz, const float* ref_q, int32_t ref_points,
+                        const float* fit_xyz, const float* fit_q, int32_t fit_points,
+                        const int32_t* pair_ref, const int32_t* pair_fit, int32_t n_pairs,
+                        float alpha, int32_t esp, float inv_lam, const float* overlaps,
+                        const float* grad_score, float* grad_ref_xyz, float* grad_ref_q,
+                        float* grad_fit_xyz, float* grad_fit_q, void* stream) {
+  FSS_GUARD(fss::score_bwd_dense_launch(ref_xyz, ref_q, ref_points, fit_xyz, fit_q, fit_points,
+                                        pair_ref, pair_fit, n_pairs, alpha, esp, inv_lam,
+                                        overlaps, grad_score, grad_ref_xyz, grad_ref_q,
+                                        grad_fit_xyz, grad_fit_q, S(stream)));
 }
 
 int fss_probe_peak(int32_t which, int32_t iters, int32_t blocks_per_sm, float* out,

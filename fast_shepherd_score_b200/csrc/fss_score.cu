@@ -65,16 +65,59 @@ __device__ __forceinline__ void point_grad(float4 x, const float4* __restrict__ 
   }
 }
 
-template <bool ESP>
+// Cloud sources: packed float4 clouds with prefix offsets, or the reference's dense padded
+// batches (molecule b = points [b*n, (b+1)*n) of an (B, n, 3) array plus optional (B, n)
+// charges, every point real).
+struct PackedSrc {
+  const float4* p;
+  const int* off;
+  __device__ __forceinline__ int begin(int mol) const { return off[mol]; }
+  __device__ __forceinline__ int size(int mol) const { return off[mol + 1] - off[mol]; }
+  __device__ __forceinline__ float4 load(int k) const { return p[k]; }
+};
+
+struct DenseSrc {
+  const float* xyz;
+  const float* q;
+  int n;
+  __device__ __forceinline__ int begin(int mol) const { return mol * n; }
+  __device__ __forceinline__ int size(int) const { return n; }
+  __device__ __forceinline__ float4 load(int k) const {
+    return make_float4(xyz[3 * (size_t)k], xyz[3 * (size_t)k + 1], xyz[3 * (size_t)k + 2],
+                       q ? q[k] : 0.f);
+  }
+};
+
+// Gradient sinks matching the sources: float4 rows (w = d/d charge), or separate (., 3)
+// coordinate and (.) charge arrays.  Atomic: a molecule may appear in several pairs.
+struct PackedSink {
+  float* g;
+  __device__ __forceinline__ void add(int k, float x, float y, float z, float c, bool esp) const {
+    float* o = g + 4 * (size_t)k;
+    atomicAdd(o + 0, x); atomicAdd(o + 1, y); atomicAdd(o + 2, z);
+    if (esp) atomicAdd(o + 3, c);
+  }
+};
+
+struct DenseSink {
+  float* gxyz;
+  float* gq;
+  __device__ __forceinline__ void add(int k, float x, float y, float z, float c, bool esp) const {
+    float* o = gxyz + 3 * (size_t)k;
+    atomicAdd(o + 0, x); atomicAdd(o + 1, y); atomicAdd(o + 2, z);
+    if (esp && gq) atomicAdd(gq + k, c);
+  }
+};
+
+template <bool ESP, class Src>
 __global__ void __launch_bounds__(kScoreThreads) score_fwd_kernel(
-    const float4* __restrict__ rp, const int* __restrict__ roff, const float4* __restrict__ fp,
-    const int* __restrict__ foff, const int* __restrict__ pr, const int* __restrict__ pf,
+    const Src ref, const Src fit, const int* __restrict__ pr, const int* __restrict__ pf,
     int maxN, int maxM, float nk, float ne, float Kc, float* score, float* ov) {
   extern __shared__ __align__(16) float4 smem[];
   __shared__ float red[32];
   const int p = blockIdx.x;
   const int ri = pr[p], fi = pf[p];
-  const int n = roff[ri + 1] - roff[ri], m = foff[fi + 1] - foff[fi];
+  const int n = ref.size(ri), m = fit.size(fi);
   if (n < 0 || m < 0 || n > maxN || m > maxM) {  // outside the staged tile: NaN, no access
     if (threadIdx.x == 0) {
       const float nan = __int_as_float(0x7fc00000);
@@ -82,12 +125,11 @@ __global__ void __launch_bounds__(kScoreThreads) score_fwd_kernel(
     }
     return;
   }
-  const float4* A = rp + roff[ri];
-  const float4* B = fp + foff[fi];
+  const int r0 = ref.begin(ri), f0 = fit.begin(fi);
   float4* sA = smem;
   float4* sB = smem + n;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) sA[i] = A[i];
-  for (int j = threadIdx.x; j < m; j += blockDim.x) sB[j] = B[j];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) sA[i] = ref.load(r0 + i);
+  for (int j = threadIdx.x; j < m; j += blockDim.x) sB[j] = fit.load(f0 + j);
   __syncthreads();
   float ab = 0.f, aa = 0.f, bb = 0.f;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -104,22 +146,21 @@ __global__ void __launch_bounds__(kScoreThreads) score_fwd_kernel(
   }
 }
 
-template <bool ESP>
+template <bool ESP, class Src, class Sink>
 __global__ void __launch_bounds__(kScoreThreads) score_bwd_kernel(
-    const float4* __restrict__ rp, const int* __restrict__ roff, const float4* __restrict__ fp,
-    const int* __restrict__ foff, const int* __restrict__ pr, const int* __restrict__ pf,
+    const Src ref, const Src fit, const int* __restrict__ pr, const int* __restrict__ pf,
     int maxN, int maxM, float nk, float ne, float aKc, float cKc, const float* __restrict__ ov,
-    const float* __restrict__ gs, float* gref, float* gfit) {
+    const float* __restrict__ gs, const Sink gref, const Sink gfit) {
   extern __shared__ __align__(16) float4 smem[];
   const int p = blockIdx.x;
   const int ri = pr[p], fi = pf[p];
-  const int r0 = roff[ri], f0 = foff[fi];
-  const int n = roff[ri + 1] - r0, m = foff[fi + 1] - f0;
+  const int n = ref.size(ri), m = fit.size(fi);
   if (n < 0 || m < 0 || n > maxN || m > maxM) return;
+  const int r0 = ref.begin(ri), f0 = fit.begin(fi);
   float4* sA = smem;
   float4* sB = smem + n;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) sA[i] = rp[r0 + i];
-  for (int j = threadIdx.x; j < m; j += blockDim.x) sB[j] = fp[f0 + j];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) sA[i] = ref.load(r0 + i);
+  for (int j = threadIdx.x; j < m; j += blockDim.x) sB[j] = fit.load(f0 + j);
   __syncthreads();
   const float vab = ov[3 * p], U = ov[3 * p + 1] + ov[3 * p + 2];
   const float D = U - vab;
@@ -131,22 +172,59 @@ __global__ void __launch_bounds__(kScoreThreads) score_bwd_kernel(
     float ax, ay, az, ac, sx, sy, sz, sc;
     point_grad<ESP>(sA[i], sB, m, nk, ne, ax, ay, az, ac);
     point_grad<ESP>(sA[i], sA, n, nk, ne, sx, sy, sz, sc);
-    float* o = gref + 4 * (size_t)(r0 + i);
-    atomicAdd(o + 0, -aKc * (dAB * ax + 2.f * dSelf * sx));
-    atomicAdd(o + 1, -aKc * (dAB * ay + 2.f * dSelf * sy));
-    atomicAdd(o + 2, -aKc * (dAB * az + 2.f * dSelf * sz));
-    if (ESP) atomicAdd(o + 3, -cKc * (dAB * ac + 2.f * dSelf * sc));
+    gref.add(r0 + i, -aKc * (dAB * ax + 2.f * dSelf * sx), -aKc * (dAB * ay + 2.f * dSelf * sy),
+             -aKc * (dAB * az + 2.f * dSelf * sz), -cKc * (dAB * ac + 2.f * dSelf * sc), ESP);
   }
   for (int j = threadIdx.x; j < m; j += blockDim.x) {
     float ax, ay, az, ac, sx, sy, sz, sc;
     point_grad<ESP>(sB[j], sA, n, nk, ne, ax, ay, az, ac);
     point_grad<ESP>(sB[j], sB, m, nk, ne, sx, sy, sz, sc);
-    float* o = gfit + 4 * (size_t)(f0 + j);
-    atomicAdd(o + 0, -aKc * (dAB * ax + 2.f * dSelf * sx));
-    atomicAdd(o + 1, -aKc * (dAB * ay + 2.f * dSelf * sy));
-    atomicAdd(o + 2, -aKc * (dAB * az + 2.f * dSelf * sz));
-    if (ESP) atomicAdd(o + 3, -cKc * (dAB * ac + 2.f * dSelf * sc));
+    gfit.add(f0 + j, -aKc * (dAB * ax + 2.f * dSelf * sx), -aKc * (dAB * ay + 2.f * dSelf * sy),
+             -aKc * (dAB * az + 2.f * dSelf * sz), -cKc * (dAB * ac + 2.f * dSelf * sc), ESP);
   }
+}
+
+struct ScoreConsts {
+  float nk, ne, Kc, aKc, cKc;
+};
+
+ScoreConsts score_consts(float alpha, int esp, float inv_lam) {
+  const double a = alpha;
+  const double Kd = std::pow(M_PI, 1.5) / std::pow(2.0 * a, 1.5);
+  ScoreConsts c;
+  c.nk = (float)(-0.5 * a * 1.4426950408889634);
+  c.ne = esp ? (float)(-(double)inv_lam * 1.4426950408889634) : 0.f;
+  c.Kc = (float)Kd;
+  c.aKc = (float)(a * Kd);
+  c.cKc = esp ? (float)(2.0 * (double)inv_lam * Kd) : 0.f;
+  return c;
+}
+
+template <class Src>
+int fwd_dispatch(const Src& R, const Src& F, const int32_t* pr, const int32_t* pf, int P,
+                 int maxN, int maxM, float alpha, int esp, float inv_lam, float* score,
+                 float* overlaps, cudaStream_t st) {
+  const ScoreConsts c = score_consts(alpha, esp, inv_lam);
+  const size_t smem = sizeof(float4) * ((size_t)maxN + maxM) + 16;
+  auto kern = esp ? score_fwd_kernel<true, Src> : score_fwd_kernel<false, Src>;
+  cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (ce != cudaSuccess) return set_error(FSS_ERR_CUDA, std::string("fss_score_fwd: ") + cudaGetErrorString(ce));
+  kern<<<P, kScoreThreads, smem, st>>>(R, F, pr, pf, maxN, maxM, c.nk, c.ne, c.Kc, score, overlaps);
+  return check_launch("fss_score_fwd");
+}
+
+template <class Src, class Sink>
+int bwd_dispatch(const Src& R, const Src& F, const int32_t* pr, const int32_t* pf, int P,
+                 int maxN, int maxM, float alpha, int esp, float inv_lam, const float* overlaps,
+                 const float* grad_score, const Sink& gR, const Sink& gF, cudaStream_t st) {
+  const ScoreConsts c = score_consts(alpha, esp, inv_lam);
+  const size_t smem = sizeof(float4) * ((size_t)maxN + maxM) + 16;
+  auto kern = esp ? score_bwd_kernel<true, Src, Sink> : score_bwd_kernel<false, Src, Sink>;
+  cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (ce != cudaSuccess) return set_error(FSS_ERR_CUDA, std::string("fss_score_bwd: ") + cudaGetErrorString(ce));
+  kern<<<P, kScoreThreads, smem, st>>>(R, F, pr, pf, maxN, maxM, c.nk, c.ne, c.aKc, c.cKc,
+                                       overlaps, grad_score, gR, gF);
+  return check_launch("fss_score_bwd");
 }
 
 }  // namespace
@@ -162,27 +240,10 @@ int score_fwd_launch(const float* ref_pts, const int32_t* ref_off, const float* 
   if (P == 0) return FSS_OK;
   if (!ref_pts || !ref_off || !fit_pts || !fit_off || !pair_ref || !pair_fit || !score || !overlaps)
     return set_error(FSS_ERR_INVALID, "fss_score_fwd: null pointer");
-  const double a = alpha;
-  const float nk = (float)(-0.5 * a * 1.4426950408889634);
-  const float ne = esp ? (float)(-(double)inv_lam * 1.4426950408889634) : 0.f;
-  const float Kc = (float)(std::pow(M_PI, 1.5) / std::pow(2.0 * a, 1.5));
-  const size_t smem = sizeof(float4) * ((size_t)maxN + maxM) + 16;
-  const float4* R = reinterpret_cast<const float4*>(ref_pts);
-  const float4* F = reinterpret_cast<const float4*>(fit_pts);
-  cudaError_t ce;
-  if (esp) {
-    ce = cudaFuncSetAttribute(score_fwd_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (ce == cudaSuccess)
-      score_fwd_kernel<true><<<P, kScoreThreads, smem, st>>>(R, ref_off, F, fit_off, pair_ref, pair_fit,
-                                                             maxN, maxM, nk, ne, Kc, score, overlaps);
-  } else {
-    ce = cudaFuncSetAttribute(score_fwd_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (ce == cudaSuccess)
-      score_fwd_kernel<false><<<P, kScoreThreads, smem, st>>>(R, ref_off, F, fit_off, pair_ref, pair_fit,
-                                                              maxN, maxM, nk, 0.f, Kc, score, overlaps);
-  }
-  if (ce != cudaSuccess) return set_error(FSS_ERR_CUDA, std::string("fss_score_fwd: ") + cudaGetErrorString(ce));
-  return check_launch("fss_score_fwd");
+  const PackedSrc R{reinterpret_cast<const float4*>(ref_pts), ref_off};
+  const PackedSrc F{reinterpret_cast<const float4*>(fit_pts), fit_off};
+  return fwd_dispatch(R, F, pair_ref, pair_fit, P, maxN, maxM, alpha, esp, inv_lam, score,
+                      overlaps, st);
 }
 
 int score_bwd_launch(const float* ref_pts, const int32_t* ref_off, const float* fit_pts,
@@ -198,31 +259,49 @@ int score_bwd_launch(const float* ref_pts, const int32_t* ref_off, const float* 
   if (!ref_pts || !ref_off || !fit_pts || !fit_off || !pair_ref || !pair_fit || !overlaps ||
       !grad_score || !grad_ref || !grad_fit)
     return set_error(FSS_ERR_INVALID, "fss_score_bwd: null pointer");
-  const double a = alpha;
-  const float nk = (float)(-0.5 * a * 1.4426950408889634);
-  const float ne = esp ? (float)(-(double)inv_lam * 1.4426950408889634) : 0.f;
-  const double Kd = std::pow(M_PI, 1.5) / std::pow(2.0 * a, 1.5);
-  const float aKc = (float)(a * Kd);
-  const float cKc = (float)(2.0 * (double)inv_lam * Kd);
-  const size_t smem = sizeof(float4) * ((size_t)maxN + maxM) + 16;
-  const float4* R = reinterpret_cast<const float4*>(ref_pts);
-  const float4* F = reinterpret_cast<const float4*>(fit_pts);
-  cudaError_t ce;
-  if (esp) {
-    ce = cudaFuncSetAttribute(score_bwd_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (ce == cudaSuccess)
-      score_bwd_kernel<true><<<P, kScoreThreads, smem, st>>>(R, ref_off, F, fit_off, pair_ref, pair_fit,
-                                                             maxN, maxM, nk, ne, aKc, cKc, overlaps,
-                                                             grad_score, grad_ref, grad_fit);
-  } else {
-    ce = cudaFuncSetAttribute(score_bwd_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (ce == cudaSuccess)
-      score_bwd_kernel<false><<<P, kScoreThreads, smem, st>>>(R, ref_off, F, fit_off, pair_ref, pair_fit,
-                                                              maxN, maxM, nk, 0.f, aKc, 0.f, overlaps,
-                                                              grad_score, grad_ref, grad_fit);
-  }
-  if (ce != cudaSuccess) return set_error(FSS_ERR_CUDA, std::string("fss_score_bwd: ") + cudaGetErrorString(ce));
-  return check_launch("fss_score_bwd");
+  const PackedSrc R{reinterpret_cast<const float4*>(ref_pts), ref_off};
+  const PackedSrc F{reinterpret_cast<const float4*>(fit_pts), fit_off};
+  return bwd_dispatch(R, F, pair_ref, pair_fit, P, maxN, maxM, alpha, esp, inv_lam, overlaps,
+                      grad_score, PackedSink{grad_ref}, PackedSink{grad_fit}, st);
+}
+
+int score_fwd_dense_launch(const float* ref_xyz, const float* ref_q, int ref_n,
+                           const float* fit_xyz, const float* fit_q, int fit_n,
+                           const int32_t* pair_ref, const int32_t* pair_fit, int P, float alpha,
+                           int esp, float inv_lam, float* score, float* overlaps,
+                           cudaStream_t st) {
+  if (P < 0 || ref_n < 0 || fit_n < 0 || !(alpha > 0.f))
+    return set_error(FSS_ERR_INVALID, "fss_score_fwd_dense: bad sizes or alpha");
+  if (ref_n > kMaxPoints || fit_n > kMaxPoints)
+    return set_error(FSS_ERR_UNSUPPORTED, "fss_score_fwd_dense: more than fss_max_points() points");
+  if (P == 0) return FSS_OK;
+  if (!ref_xyz || !fit_xyz || !pair_ref || !pair_fit || !score || !overlaps ||
+      (esp && (!ref_q || !fit_q)))
+    return set_error(FSS_ERR_INVALID, "fss_score_fwd_dense: null pointer");
+  return fwd_dispatch(DenseSrc{ref_xyz, esp ? ref_q : nullptr, ref_n},
+                      DenseSrc{fit_xyz, esp ? fit_q : nullptr, fit_n}, pair_ref, pair_fit, P,
+                      ref_n, fit_n, alpha, esp, inv_lam, score, overlaps, st);
+}
+
+int score_bwd_dense_launch(const float* ref_xyz, const float* ref_q, int ref_n,
+                           const float* fit_xyz, const float* fit_q, int fit_n,
+                           const int32_t* pair_ref, const int32_t* pair_fit, int P, float alpha,
+                           int esp, float inv_lam, const float* overlaps, const float* grad_score,
+                           float* grad_ref_xyz, float* grad_ref_q, float* grad_fit_xyz,
+                           float* grad_fit_q, cudaStream_t st) {
+  if (P < 0 || ref_n < 0 || fit_n < 0 || !(alpha > 0.f))
+    return set_error(FSS_ERR_INVALID, "fss_score_bwd_dense: bad sizes or alpha");
+  if (ref_n > kMaxPoints || fit_n > kMaxPoints)
+    return set_error(FSS_ERR_UNSUPPORTED, "fss_score_bwd_dense: more than fss_max_points() points");
+  if (P == 0) return FSS_OK;
+  if (!ref_xyz || !fit_xyz || !pair_ref || !pair_fit || !overlaps || !grad_score ||
+      !grad_ref_xyz || !grad_fit_xyz || (esp && (!ref_q || !fit_q)))
+    return set_error(FSS_ERR_INVALID, "fss_score_bwd_dense: null pointer");
+  return bwd_dispatch(DenseSrc{ref_xyz, esp ? ref_q : nullptr, ref_n},
+                      DenseSrc{fit_xyz, esp ? fit_q : nullptr, fit_n}, pair_ref, pair_fit, P,
+                      ref_n, fit_n, alpha, esp, inv_lam, overlaps, grad_score,
+                      DenseSink{grad_ref_xyz, grad_ref_q}, DenseSink{grad_fit_xyz, grad_fit_q},
+                      st);
 }
 
 }  // namespace fss

@@ -240,6 +240,25 @@ int fss_score_bwd(const float *ref_pts, const int32_t *ref_off, const float *fit
                   int32_t esp, float inv_lam, const float *overlaps, const float *grad_score,
                   float *grad_ref, float *grad_fit, void *stream);
 
+/* Dense-batch form of fss_score_fwd / fss_score_bwd for the reference's padded tensors: ref
+ * molecule b is ref_xyz[b, 0:ref_points, :] of a (B_ref, ref_points, 3) array (every point
+ * real) with charges ref_q[b, :] (B_ref, ref_points) when esp != 0 (NULL otherwise); likewise
+ * the fit side.  Same math as get_overlap / get_overlap_esp (score/gaussian_overlap.py:62-117,
+ * score/electrostatic_scoring.py:17-120) without packing.  Backward ADDS d(loss)/d(coords)
+ * into grad_*_xyz (same shapes as the inputs) and d(loss)/d(charges) into grad_*_q (may be
+ * NULL when esp == 0). */
+int fss_score_fwd_dense(const float *ref_xyz, const float *ref_q, int32_t ref_points,
+                        const float *fit_xyz, const float *fit_q, int32_t fit_points,
+                        const int32_t *pair_ref, const int32_t *pair_fit, int32_t n_pairs,
+                        float alpha, int32_t esp, float inv_lam, float *score, float *overlaps,
+                        void *stream);
+int fss_score_bwd_dense(const float *ref_xyz, const float *ref_q, int32_t ref_points,
+                        const float *fit_xyz, const float *fit_q, int32_t fit_points,
+                        const int32_t *pair_ref, const int32_t *pair_fit, int32_t n_pairs,
+                        float alpha, int32_t esp, float inv_lam, const float *overlaps,
+                        const float *grad_score, float *grad_ref_xyz, float *grad_ref_q,
+                        float *grad_fit_xyz, float *grad_fit_q, void *stream);
+
 /* ---------------------------------------------------------------------------------------
  * Roof probe (measurement support, no reference counterpart): launches a throughput kernel
  * of `which` = 0 (ex2 on the MUFU pipe) or 1 (FP32 FMA) with `blocks_per_sm` CTAs of 256
