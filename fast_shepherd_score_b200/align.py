@@ -83,7 +83,8 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
     (P*S,), (P*S,4), (P*S,3) tensors) receives every start's best score and pose.
     Self overlaps default to the kernels' own (:func:`kernels.self_overlap`).
     ``accumulate`` picks where the shape/ESP sums run: 0 automatic (autotuned), 1 FP32 lanes,
-    2 tensor cores (modes "shape" and "esp", 32 lanes per pose).  ``kernel_variant`` picks the
+    2 tensor-core value/gradient sums, 3 tensor-core exponents (2 and 3: modes "shape" and
+    "esp", 32 lanes per pose).  ``kernel_variant`` picks the
     FP32-lane loop's code variant: 0 automatic, 1 base, 2 wide register tile, 3 one-CTA/SM
     register budget (2 and 3 for "shape" and "esp").  Mode "pharm" only: ``similarity`` in
     ("tanimoto", "tversky", "tversky_ref", "tversky_fit") and ``pharm_extended`` 0 (cosine

@@ -4,8 +4,9 @@ Tunables of one launch (``fss_align_desc``):
   lanes_per_pose  4, 8, 16 or 32 lanes cooperate on one pose (so 32/lanes starts per warp)
   chunks          start blocks per pair (a CTA owns one pair and n_starts/chunks starts)
   cta_per_sm      persistent CTAs per SM (1 or 2; 2 hides latency, 1 leaves more L1)
-  accumulate      1 = value/gradient sums on the FP32 lanes, 2 = on the tensor cores
-                  (shape/ESP modes; 32 lanes per pose)
+  accumulate      1 = value/gradient sums on the FP32 lanes, 2 = sums on the tensor cores,
+                  3 = pairwise exponents on the tensor cores (2 and 3: shape/ESP modes,
+                  32 lanes per pose)
   kernel_variant  code variant of the FP32-lane loop (shape/ESP modes): 1 base, 2 wide
                   register tile, 3 one-CTA/SM register budget, 4 base tile unrolled 4x
 
@@ -108,10 +109,11 @@ def candidates(mode: str, max_fit: int, n_starts: int):
                                     "kernel_variant": var})
     if mode in ("shape", "esp") and max_fit >= 16:
         base = _auto_chunks(32, n_starts)
-        for ch, cps in ((0, 0), (0, 1), (2 * base, 0)):
-            if ch <= n_starts:
-                out.append({"lanes_per_pose": 32, "chunks": ch, "cta_per_sm": cps,
-                            "accumulate": 2})
+        for acc in (2, 3):
+            for ch, cps in ((0, 0), (0, 1), (2 * base, 0)):
+                if ch <= n_starts:
+                    out.append({"lanes_per_pose": 32, "chunks": ch, "cta_per_sm": cps,
+                                "accumulate": acc})
     return out
 
 
@@ -169,7 +171,8 @@ def tune(run, key: str, cands, repeats: int = 2) -> dict:
             t = min(ms)
         except (ValueError, RuntimeError):
             continue
-        tag = "tc" if c.get("accumulate") == 2 else f"v{c.get('kernel_variant', 0)}:"
+        acc = c.get("accumulate", 0)
+        tag = "tc" if acc == 2 else "tce" if acc == 3 else f"v{c.get('kernel_variant', 0)}:"
         timings[f"{tag}{c['lanes_per_pose']}x{c['cta_per_sm']}c{c['chunks']}"] = round(t, 4)
         if t < best_ms:
             best, best_ms = c, t

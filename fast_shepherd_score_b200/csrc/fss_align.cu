@@ -183,11 +183,13 @@ int align_launch(const fss_align_desc* d, cudaStream_t st) {
   if (d->n_pairs == 0) return FSS_OK;
 
   const bool tc_mode = d->mode == FSS_MODE_SHAPE || d->mode == FSS_MODE_ESP;
-  if (d->accumulate < 0 || d->accumulate > 2)
-    return set_error(FSS_ERR_INVALID, "fss_align: accumulate must be 0, 1 or 2");
-  if (d->accumulate == 2 && !tc_mode)
+  if (d->accumulate < 0 || d->accumulate > 3)
+    return set_error(FSS_ERR_INVALID, "fss_align: accumulate must be 0, 1, 2 or 3");
+  if (d->accumulate >= 2 && !tc_mode)
     return set_error(FSS_ERR_INVALID, "fss_align: tensor-core sums need mode SHAPE or ESP");
-  const bool tc = d->accumulate == 2;
+  // kernel accumulation path: 0 FP32 lanes, 1 tensor-core sums, 2 tensor-core exponents
+  const int acc = d->accumulate >= 2 ? d->accumulate - 1 : 0;
+  const bool tc = acc != 0;
   if (d->pharm_extended < 0 || d->pharm_extended > 2 ||
       (d->pharm_extended != 0 && d->mode != FSS_MODE_PHARM))
     return set_error(FSS_ERR_INVALID, "fss_align: pharm_extended must be 0, 1 or 2 (mode PHARM)");
@@ -261,7 +263,8 @@ int align_launch(const fss_align_desc* d, cudaStream_t st) {
 
   const size_t nb = ((size_t)maxN + 7) / 8;
   const size_t smem = sizeof(float) * kColdFields * (size_t)threads +
-      (tc ? sizeof(float4) * (kMmaP4PerBlock * nb + maxM) +
+      (acc == 2 ? sizeof(float2) * kTceF2PerBlock * nb + sizeof(float4) * maxM + 16
+       : tc ? sizeof(float4) * (kMmaP4PerBlock * nb + maxM) +
                sizeof(float2) * (kMmaC2PerBlock + kMmaQ2PerBlock) * nb + 16
          : sizeof(float4) * (2 * (size_t)maxN + maxM + 2 * (size_t)maxNp + 2 * (size_t)maxMp) +
                sizeof(float2) * (d->mode == FSS_MODE_ESP ? (size_t)maxN : 0) +
@@ -269,8 +272,8 @@ int align_launch(const fss_align_desc* d, cudaStream_t st) {
                sizeof(float2) * ((size_t)maxNa + maxMa) + 16);
   int rc;
   switch (d->mode) {
-    case FSS_MODE_SHAPE: rc = launch_align_shape(lpp, tc, var, p, threads, d->cta_per_sm, smem, st); break;
-    case FSS_MODE_ESP: rc = launch_align_esp(lpp, tc, var, p, threads, d->cta_per_sm, smem, st); break;
+    case FSS_MODE_SHAPE: rc = launch_align_shape(lpp, acc, var, p, threads, d->cta_per_sm, smem, st); break;
+    case FSS_MODE_ESP: rc = launch_align_esp(lpp, acc, var, p, threads, d->cta_per_sm, smem, st); break;
     case FSS_MODE_ESP_COMBO:
       rc = launch_align_combo(lpp, var, p, threads, d->cta_per_sm, smem, st);
       break;

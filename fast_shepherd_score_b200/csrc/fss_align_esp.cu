@@ -3,9 +3,10 @@
 
 namespace fss {
 
-int launch_align_esp(int lpp, bool tc, int var, const AlignParams& prm, int threads, int cps, size_t smem,
+int launch_align_esp(int lpp, int acc, int var, const AlignParams& prm, int threads, int cps, size_t smem,
          cudaStream_t st) {
-  if (tc) return launch_align<32, FSS_MODE_ESP, true, 0>(prm, threads, cps, smem, st);
+  if (acc == 1) return launch_align<32, FSS_MODE_ESP, 1, 0>(prm, threads, cps, smem, st);
+  if (acc == 2) return launch_align<32, FSS_MODE_ESP, 2, 0>(prm, threads, cps, smem, st);
   switch (var) {
     case 0: return dispatch_lanes<FSS_MODE_ESP, 0>(lpp, prm, threads, cps, smem, st);
     case 1: return dispatch_lanes<FSS_MODE_ESP, 1>(lpp, prm, threads, cps, smem, st);

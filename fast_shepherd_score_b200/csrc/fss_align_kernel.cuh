@@ -16,6 +16,7 @@
 
 #include "fss_internal.cuh"
 #include "fss_mma.cuh"
+#include "fss_tce.cuh"
 
 namespace fss {
 
@@ -68,19 +69,23 @@ struct AlignVariant<2> { static constexpr int kJB2 = 2, kUnroll = 4, kMinCtas = 
 template <>
 struct AlignVariant<3> { static constexpr int kJB2 = 2, kUnroll = 4, kMinCtas = 2; };
 
-// TC: shape/ESP sums on the tensor cores (fss_mma.cuh); requires LPP == 32 and a mode
+// ACC: where the shape/ESP sums run -- 0 FP32 lanes, 1 tensor-core value/gradient sums
+// (fss_mma.cuh), 2 tensor-core exponents (fss_tce.cuh); 1 and 2 need LPP == 32 and a mode
 // without a pharmacophore channel.  EXT: extended pharmacophore points (pharm_pose).
-template <int LPP, int MODE, bool TC, int VAR, int EXT = 0>
+template <int LPP, int MODE, int ACC, int VAR, int EXT = 0>
 __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
     align_kernel(const AlignParams p) {
   using V = AlignVariant<VAR>;
+  constexpr bool TC = ACC == 1;
+  constexpr bool TCE = ACC == 2;
   constexpr bool kCombo = MODE == FSS_MODE_ESP_COMBO;
   constexpr bool kShape = MODE == FSS_MODE_SHAPE || MODE == FSS_MODE_ESP ||
                           MODE == FSS_MODE_SHAPE_PHARM || MODE == FSS_MODE_SHAPE_COLOR || kCombo;
   constexpr bool kEsp = MODE == FSS_MODE_ESP;
   constexpr bool kPharm = MODE == FSS_MODE_PHARM || MODE == FSS_MODE_SHAPE_PHARM ||
                           MODE == FSS_MODE_SHAPE_COLOR;
-  static_assert(!TC || (LPP == 32 && !kPharm), "tensor-core sums: whole-warp shape/ESP poses");
+  static_assert(ACC == 0 || (LPP == 32 && !kPharm && (MODE == FSS_MODE_SHAPE || MODE == FSS_MODE_ESP)),
+                "tensor-core paths: whole-warp shape/ESP poses");
   extern __shared__ __align__(16) float4 smem[];
   // FP32 path: sP = 2 * maxN duplicated expanded reference (+ sQc).  Tensor-core path:
   // sP = 8 * nbMax block-interleaved reference, sCm/sQm after the fit cloud.
@@ -88,7 +93,8 @@ __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
   // parked optimiser state: kColdFields floats per thread (a multiple of 16 bytes per CTA)
   volatile float* sCold = reinterpret_cast<float*>(smem) + threadIdx.x;
   float4* sP = smem + kColdFields * blockDim.x / 4;
-  float4* sB = sP + (TC ? kMmaP4PerBlock * nbMax : 2 * p.maxN);
+  float4* sB = sP + (TC ? kMmaP4PerBlock * nbMax : TCE ? kTceF2PerBlock / 2 * nbMax
+                                                     : 2 * p.maxN);
   float4* sRA = sB + p.maxM;
   float4* sRV = sRA + p.maxNp;
   float4* sFA = sRV + p.maxNp;
@@ -152,6 +158,8 @@ __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
     if (kShape) {
       c = block_centroid(p.ref_pts + r0, N, red);
       if constexpr (TC) stage_ref_mma<kEsp>(p.ref_pts + r0, N, c, p.k, p.e, sP, sQm, sCm);
+      else if constexpr (TCE)
+        stage_ref_tce<kEsp>(p.ref_pts + r0, N, c, p.k, p.e, sP, nbMax);
       else stage_ref<kEsp>(p.ref_pts + r0, N, c, p.k, p.e, sP, sQc);
       stage_copy(p.fit_pts + f0, M, sB);
     }
@@ -213,6 +221,9 @@ __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
           if constexpr (TC)
             shape_pose_mma<kEsp>(sP, sQm, sCm, sB, N, M, lane, R, s.t[0], s.t[1], s.t[2], p.k,
                                  p.e, ms);
+          else if constexpr (TCE)
+            shape_pose_tce<kEsp>(tce_ref(sP, nbMax), sB, N, M, lane, R, s.t[0], s.t[1], s.t[2],
+                                 p.k, p.e, p.inv2k, ms);
           else
             shape_pose<LPP, kEsp, V::kJB2, V::kUnroll>(sP, sQc, sB, N, M, lane, R, s.t[0],
                                                        s.t[1], s.t[2], p.k, p.e, p.inv2k, ms);
@@ -268,10 +279,10 @@ __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
   }
 }
 
-template <int LPP, int MODE, bool TC, int VAR, int EXT = 0>
+template <int LPP, int MODE, int ACC, int VAR, int EXT = 0>
 int launch_align(const AlignParams& prm, int threads, int cta_per_sm, size_t smem,
                  cudaStream_t st) {
-  auto kern = align_kernel<LPP, MODE, TC, VAR, EXT>;
+  auto kern = align_kernel<LPP, MODE, ACC, VAR, EXT>;
   cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)smem);
   if (ce != cudaSuccess)
@@ -291,19 +302,19 @@ template <int MODE, int VAR, int EXT = 0>
 int dispatch_lanes(int lpp, const AlignParams& prm, int threads, int cps, size_t smem,
                    cudaStream_t st) {
   switch (lpp) {
-    case 4: return launch_align<4, MODE, false, VAR, EXT>(prm, threads, cps, smem, st);
-    case 8: return launch_align<8, MODE, false, VAR, EXT>(prm, threads, cps, smem, st);
-    case 16: return launch_align<16, MODE, false, VAR, EXT>(prm, threads, cps, smem, st);
-    case 32: return launch_align<32, MODE, false, VAR, EXT>(prm, threads, cps, smem, st);
+    case 4: return launch_align<4, MODE, 0, VAR, EXT>(prm, threads, cps, smem, st);
+    case 8: return launch_align<8, MODE, 0, VAR, EXT>(prm, threads, cps, smem, st);
+    case 16: return launch_align<16, MODE, 0, VAR, EXT>(prm, threads, cps, smem, st);
+    case 32: return launch_align<32, MODE, 0, VAR, EXT>(prm, threads, cps, smem, st);
     default: return set_error(FSS_ERR_INVALID, "fss_align: lanes_per_pose must be 4, 8, 16 or 32");
   }
 }
 
-// Per-mode launchers (one translation unit each).  var: 0..2 as AlignVariant; tc: tensor-core
-// sums (shape and ESP modes only).
-int launch_align_shape(int lpp, bool tc, int var, const AlignParams& prm, int threads, int cps,
+// Per-mode launchers (one translation unit each).  var: as AlignVariant; acc: 0 FP32 lanes,
+// 1 tensor-core sums, 2 tensor-core exponents (shape and ESP modes only).
+int launch_align_shape(int lpp, int acc, int var, const AlignParams& prm, int threads, int cps,
                        size_t smem, cudaStream_t st);
-int launch_align_esp(int lpp, bool tc, int var, const AlignParams& prm, int threads, int cps,
+int launch_align_esp(int lpp, int acc, int var, const AlignParams& prm, int threads, int cps,
                      size_t smem, cudaStream_t st);
 int launch_align_pharm(int mode, int lpp, int ext, const AlignParams& prm, int threads,
                        int cps, size_t smem, cudaStream_t st);

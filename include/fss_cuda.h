@@ -154,9 +154,10 @@ typedef struct fss_align_desc {
   int32_t lanes_per_pose;    /* 4, 8, 16 or 32 lanes cooperate on one pose */
   int32_t chunks;            /* start blocks per pair (CTA covers n_starts/chunks starts) */
   int32_t cta_per_sm;        /* persistent CTAs per SM */
-  int32_t accumulate;        /* where the value/gradient sums of the shape and ESP channels
-                              * run: 0 automatic, 1 FP32 lanes, 2 tensor cores (tf32 hi/lo
-                              * split MMA, one warp per pose; modes SHAPE and ESP) */
+  int32_t accumulate;        /* where the shape and ESP channels' pairwise work runs:
+                              * 0 automatic, 1 FP32 lanes, 2 value/gradient sums on the tensor
+                              * cores, 3 exponents on the tensor cores (both tf32 hi/lo split
+                              * MMA, one warp per pose; modes SHAPE and ESP) */
   int32_t kernel_variant;    /* code variant of the FP32-lane loop: 0 automatic, 1 base (4 fit
                               * points per lane, 2 CTAs/SM register budget), 2 wide (6 fit
                               * points per lane, deeper unroll), 3 roomy (4 fit points, one
