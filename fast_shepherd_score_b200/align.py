@@ -30,7 +30,7 @@ from typing import Optional
 import numpy as np
 import torch
 
-from . import _lib, autotune, kernels
+from . import _lib, autotune, kernels, legacy_seeds
 from ._lib import AlignDesc, check, ptr, stream_ptr
 from .layout import CloudSet, PharmSet, cost_order
 
@@ -305,6 +305,22 @@ def _default_counts(x, K, pad, dev):
     return torch.as_tensor(x, device=dev).to(torch.int64)
 
 
+def _trans_seeds(run, g_ref: CloudSet, g_fit: CloudSet, trans_centers, trans_centers_real,
+                 per_trans: int, topk: int, shift=None):
+    """Start poses of the translation-seeded path (the reference's trans_centers branch,
+    drivers/esp.py:228-262 and its twins): the legacy grid of every pair
+    (:mod:`legacy_seeds`), each pose scored once by the fused kernel (``run(seeds, 1)`` returns
+    the per-row scores of a one-step launch, i.e. the seed poses' own scores), and the top-k
+    poses per pair as (K,topk,4), (K,topk,3) seeds for the fine run."""
+    K = trans_centers.shape[0]
+    dev = trans_centers.device
+    n = _default_counts(trans_centers_real, K, trans_centers.shape[1], dev)
+    centres = CloudSet.from_padded(trans_centers.to(_f32), n)
+    pr, pf = _self_pairs(K, dev)
+    gq, gt, G = legacy_seeds.grid_packed(g_ref, g_fit, centres, pr, pf, per_trans, shift)
+    return legacy_seeds.select(run((gq, gt), 1), gq, gt, G, topk)
+
+
 def coarse_fine_align_many(A_batch, B_batch, VAA, VBB, *, alpha: float = 0.81,
                            num_seeds: int = 50, steps_fine: int = 100, lr: float = 0.075,
                            N_real=None, M_real=None, early_stop_patience: int = 2,
@@ -334,10 +350,11 @@ def coarse_fine_esp_align_many(A_batch, B_batch, CA_batch, CB_batch, VAA, VBB, *
                                M_real=None, early_stop_patience: int = 5,
                                early_stop_tol: float = 1e-5, seeds: Optional[tuple] = None,
                                **tile):
-    """Batched ESP alignment; ``lam`` is the kernel lambda (LAM_SCALING*lam for surfaces)."""
-    if trans_centers is not None:
-        raise NotImplementedError("trans_init (coarse translation grid) is not part of the "
-                                  "CUDA backend; use the reference backend for it")
+    """Batched ESP alignment; ``lam`` is the kernel lambda (LAM_SCALING*lam for surfaces).
+
+    ``trans_centers`` (K,P,3) with ``trans_centers_real`` selects the translation-seeded
+    starts (trans_init=True): the legacy grid of 5 + num_repeats_per_trans * P poses per pair,
+    scored once, its ``topk`` best refined."""
     K, npad, _ = A_batch.shape
     dev = A_batch.device
     N_real = _default_counts(N_real, K, npad, dev)
@@ -345,12 +362,19 @@ def coarse_fine_esp_align_many(A_batch, B_batch, CA_batch, CB_batch, VAA, VBB, *
     ref = CloudSet.from_padded(A_batch, N_real, CA_batch)
     fit = CloudSet.from_padded(B_batch, M_real, CB_batch)
     pr, pf = _self_pairs(K, dev)
-    if seeds is None:
+    VAA, VBB = VAA.to(_f32).contiguous(), VBB.to(_f32).contiguous()
+
+    def run(sd, steps):
+        return align_packed("esp", ref=ref, fit=fit, pair_ref=pr, pair_fit=pf, seed_q=sd[0],
+                            seed_t=sd[1], steps=steps, lr=lr, alpha=alpha, lam=lam,
+                            ref_self=VAA, fit_self=VBB, **tile)
+
+    if trans_centers is not None:
+        seeds = _trans_seeds(lambda sd, st: run(sd, st).rows[0], ref, fit, trans_centers,
+                             trans_centers_real, num_repeats_per_trans, topk)
+    elif seeds is None:
         seeds = kernels.seeds(ref, fit, pr, pf, num_seeds)
-    return align_packed("esp", ref=ref, fit=fit, pair_ref=pr, pair_fit=pf, seed_q=seeds[0],
-                        seed_t=seeds[1], steps=steps_fine, lr=lr, alpha=alpha, lam=lam,
-                        ref_self=VAA.to(_f32).contiguous(), fit_self=VBB.to(_f32).contiguous(),
-                        **tile)
+    return run(seeds, steps_fine)
 
 
 def _centroids(X, n):
@@ -391,8 +415,6 @@ def coarse_fine_pharm_align_many(anchors_1, anchors_2, vectors_1, vectors_2, typ
     the centred clouds.  VAA/VBB are recomputed by the kernel with the same extended-point
     convention as the cross overlap, as in the reference (pharm.py:732-748).
     """
-    if trans_centers is not None:
-        raise NotImplementedError("trans_init is not part of the CUDA backend")
     K, npad, _ = anchors_1.shape
     dev = anchors_1.device
     N_real = _default_counts(N_real, K, npad, dev)
@@ -406,13 +428,24 @@ def coarse_fine_pharm_align_many(anchors_1, anchors_2, vectors_1, vectors_2, typ
     ref_ph = PharmSet.from_padded(a1c, types_1, vectors_1, N_real)
     fit_ph = PharmSet.from_padded(a2c, types_2, vectors_2, M_real)
     pr, pf = _self_pairs(K, dev)
-    if seeds is None:
+
+    def run(sd, steps):
+        return align_packed("pharm", ref_ph=ref_ph, fit_ph=fit_ph, pair_ref=pr, pair_fit=pf,
+                            seed_q=sd[0], seed_t=sd[1], steps=steps, lr=lr,
+                            similarity=similarity,
+                            pharm_extended=extended_code(extended_points, only_extended),
+                            **tile)
+
+    if trans_centers is not None:
+        # centres are points of the original reference frame: shift them with the anchors
+        seeds = _trans_seeds(lambda sd, st: run(sd, st).rows[0],
+                             CloudSet.from_padded(a1c, N_real),
+                             CloudSet.from_padded(a2c, M_real), trans_centers.to(_f32),
+                             trans_centers_real, num_repeats_per_trans, topk, shift=c_ref)
+    elif seeds is None:
         seeds = kernels.seeds(CloudSet.from_padded(a1c, N_real),
                               CloudSet.from_padded(a2c, M_real), pr, pf, num_seeds)
-    sc, q, t = align_packed("pharm", ref_ph=ref_ph, fit_ph=fit_ph, pair_ref=pr, pair_fit=pf,
-                            seed_q=seeds[0], seed_t=seeds[1], steps=steps_fine, lr=lr,
-                            similarity=similarity,
-                            pharm_extended=extended_code(extended_points, only_extended), **tile)
+    sc, q, t = run(seeds, steps_fine)
     R = _quat_rot(q)
     t = t - torch.einsum('bij,bj->bi', R, c_fit) + c_ref
     return sc, q, t
@@ -440,8 +473,6 @@ def coarse_fine_esp_combo_align_many(centers_w_H_1, centers_w_H_2, centers_1, ce
     ``esp_stride`` = 1 scores every step as the reference's CUDA-graph loop does; 5 matches its
     eager loop.  VAA/VBB (shape self overlaps) are recomputed when not given.
     """
-    if trans_centers is not None:
-        raise NotImplementedError("trans_init is not part of the CUDA backend")
     K = centers_1.shape[0]
     dev = centers_1.device
     cnt = lambda n, x: _default_counts(n, K, x.shape[1], dev)
@@ -457,14 +488,22 @@ def coarse_fine_esp_combo_align_many(centers_w_H_1, centers_w_H_2, centers_1, ce
     rs = CloudSet.from_padded(points_1.to(_f32), NS, point_charges_1)
     fs = CloudSet.from_padded(points_2.to(_f32), MS, point_charges_2)
     pr, pf = _self_pairs(K, dev)
-    if seeds is None:
+
+    def run(sd, steps):
+        return align_packed("esp_combo", ref=ref, fit=fit, pair_ref=pr, pair_fit=pf,
+                            seed_q=sd[0], seed_t=sd[1], steps=steps, lr=lr, alpha=alpha,
+                            lam=lam, ref_self=VAA, fit_self=VBB, ref_atoms=ra, fit_atoms=fa,
+                            ref_radii=rrad, fit_radii=frad, ref_surf=rs, fit_surf=fs,
+                            probe_radius=probe_radius, esp_weight=esp_weight,
+                            esp_stride=esp_stride, **tile)
+
+    if trans_centers is not None:
+        # the legacy grid is built from the surface clouds (esp_combo.py:409-412)
+        seeds = _trans_seeds(lambda sd, st: run(sd, st).rows[0], rs, fs, trans_centers,
+                             trans_centers_real, num_repeats_per_trans, topk)
+    elif seeds is None:
         seeds = kernels.seeds(ref, fit, pr, pf, num_seeds)
-    return align_packed("esp_combo", ref=ref, fit=fit, pair_ref=pr, pair_fit=pf,
-                        seed_q=seeds[0], seed_t=seeds[1], steps=steps_fine, lr=lr, alpha=alpha,
-                        lam=lam, ref_self=VAA, fit_self=VBB, ref_atoms=ra, fit_atoms=fa,
-                        ref_radii=rrad, fit_radii=frad, ref_surf=rs, fit_surf=fs,
-                        probe_radius=probe_radius, esp_weight=esp_weight,
-                        esp_stride=esp_stride, **tile)
+    return run(seeds, steps_fine)
 
 
 def _packed_values(X, n_real):
@@ -491,8 +530,6 @@ def coarse_fine_vol_color_align_many(centers_1, centers_2, ptype_1, ptype_2, anc
     ``directional=False`` is the reference vol_color mode (directionless colour);
     ``directional=True`` weights same-type pairs by the vector cosine (needs vectors).
     """
-    if trans_centers is not None:
-        raise NotImplementedError("trans_init is not part of the CUDA backend")
     K = centers_1.shape[0]
     dev = centers_1.device
     Nc = _default_counts(N_real_centers, K, centers_1.shape[1], dev)
@@ -504,13 +541,20 @@ def coarse_fine_vol_color_align_many(centers_1, centers_2, ptype_1, ptype_2, anc
     ref_ph = PharmSet.from_padded(anchors_1, ptype_1, vectors_1 if directional else None, Np)
     fit_ph = PharmSet.from_padded(anchors_2, ptype_2, vectors_2 if directional else None, Mp)
     pr, pf = _self_pairs(K, dev)
-    if seeds is None:
+    VAA, VBB = VAA.to(_f32).contiguous(), VBB.to(_f32).contiguous()
+
+    def run(sd, steps):
+        return align_packed("shape_pharm" if directional else "shape_color", ref=ref, fit=fit,
+                            ref_ph=ref_ph, fit_ph=fit_ph, pair_ref=pr, pair_fit=pf,
+                            seed_q=sd[0], seed_t=sd[1], steps=steps, lr=lr, alpha=alpha,
+                            color_weight=color_weight, ref_self=VAA, fit_self=VBB, **tile)
+
+    if trans_centers is not None:
+        seeds = _trans_seeds(lambda sd, st: run(sd, st).rows[0], ref, fit, trans_centers,
+                             trans_centers_real, num_repeats_per_trans, topk)
+    elif seeds is None:
         seeds = kernels.seeds(ref, fit, pr, pf, num_seeds)
-    return align_packed("shape_pharm" if directional else "shape_color", ref=ref, fit=fit,
-                        ref_ph=ref_ph, fit_ph=fit_ph, pair_ref=pr, pair_fit=pf,
-                        seed_q=seeds[0], seed_t=seeds[1], steps=steps_fine, lr=lr, alpha=alpha,
-                        color_weight=color_weight, ref_self=VAA.to(_f32).contiguous(),
-                        fit_self=VBB.to(_f32).contiguous(), **tile)
+    return run(seeds, steps_fine)
 
 
 def coarse_fine_vol_pharm_align_many(centers_1, centers_2, ptype_1, ptype_2, anchors_1,

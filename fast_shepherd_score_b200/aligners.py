@@ -140,6 +140,17 @@ def _align(pairs, mode, ref, fit, ref_ph, fit_ph, r_idx, f_idx, **kw):
     return _write(pairs, mode, out)
 
 
+def _trans_kw(pairs, trans_init, attr, src, dev, r_idx, num_repeats_per_trans=10, topk=30):
+    """Keyword arguments of the translation-seeded starts (trans_init=True): the reference
+    molecules' translation centres (p.<attr>, built from ref_molec.<src> if absent) packed like
+    the reference clouds (shared when the reference is)."""
+    if not trans_init:
+        return {}
+    t = _ensure(pairs, attr, src, _f32, dev)
+    centres, _ = _cloud_set(t, device=dev, dedup=r_idx is not None)
+    return dict(trans_centres=centres, num_repeats_per_trans=num_repeats_per_trans, topk=topk)
+
+
 def _align_batch_vol(pairs, *, alpha: float = 0.81, steps_fine: int = 100,
                      num_repeats: Optional[int] = None, lr: float = 0.075):
     """Volumetric (heavy-atom) shape alignment; writes transform_vol_noH / sim_aligned_vol_noH."""
@@ -171,8 +182,6 @@ def _align_batch_surf_esp(pairs, *, alpha: float, lam: float, trans_init: bool =
     transform_surf_esp / sim_aligned_surf_esp."""
     if not pairs:
         return
-    if trans_init:
-        raise NotImplementedError("trans_init=True is not part of the CUDA backend")
     dev = _device_of(pairs)
     pts_r = _ensure(pairs, "_ref_surf_t", "surf_pos", _f32, dev)
     pts_f = _ensure(pairs, "_fit_surf_t", "surf_pos", _f32, dev)
@@ -180,8 +189,11 @@ def _align_batch_surf_esp(pairs, *, alpha: float, lam: float, trans_init: bool =
     esp_f = _ensure(pairs, "_fit_surf_esp_t", "surf_esp", _f32, dev)
     ref, ri = _cloud_set(pts_r, esp_r, device=dev)
     fit, fi = _cloud_set(pts_f, esp_f, device=dev)
+    # trans_init: translation centres are the reference atoms (aligners.py:408-412)
+    tk = _trans_kw(pairs, trans_init, "_ref_xyz_t", "atom_pos", dev, ri, num_repeats_per_trans,
+                   topk)
     return _align(pairs, "surf_esp", ref, fit, None, None, ri, fi, alpha=alpha, lam=lam,
-                  steps=steps_fine, lr=lr, num_seeds=num_repeats or seeds_for("surf_esp"))
+                  steps=steps_fine, lr=lr, num_seeds=num_repeats or seeds_for("surf_esp"), **tk)
 
 
 _align_batch_esp = _align_batch_surf_esp
@@ -195,8 +207,6 @@ def _align_batch_vol_esp(pairs, *, lam: float, alpha: float = 0.81, trans_init: 
     ``_*_xyz_esp_t`` when present, else atom positions and partial charges."""
     if not pairs:
         return
-    if trans_init:
-        raise NotImplementedError("trans_init=True is not part of the CUDA backend")
     dev = _device_of(pairs)
     for side in ("ref", "fit"):
         for p in pairs:
@@ -209,8 +219,10 @@ def _align_batch_vol_esp(pairs, *, lam: float, alpha: float = 0.81, trans_init: 
     ch_f = _ensure(pairs, "_fit_xyz_esp_t", "partial_charges", _f32, dev)
     ref, ri = _cloud_set(pts_r, ch_r, device=dev)
     fit, fi = _cloud_set(pts_f, ch_f, device=dev)
+    tk = _trans_kw(pairs, trans_init, "_ref_xyz_t", "atom_pos", dev, ri, num_repeats_per_trans,
+                   topk)
     return _align(pairs, "vol_esp", ref, fit, None, None, ri, fi, alpha=alpha, lam=lam,
-                  steps=steps_fine, lr=lr, num_seeds=num_repeats or seeds_for("vol_esp"))
+                  steps=steps_fine, lr=lr, num_seeds=num_repeats or seeds_for("vol_esp"), **tk)
 
 
 def _conformer_positions(mol):
@@ -231,8 +243,6 @@ def _align_batch_vol_and_surf_esp(pairs, *, alpha: float, lam: float = 0.001,
     sim_aligned_vol_and_surf_esp."""
     if not pairs:
         return
-    if trans_init:
-        raise NotImplementedError("trans_init=True is not part of the CUDA backend")
     dev = _device_of(pairs)
     sets = {}
     for side in ("ref", "fit"):
@@ -250,12 +260,15 @@ def _align_batch_vol_and_surf_esp(pairs, *, alpha: float, lam: float = 0.001,
         radii = torch.cat([r.reshape(-1).to(_f32) for r in (rad[:1] if dd else rad)]).to(dev)
         sets[side] = (centres, idx, atoms, radii, surfs)
     (ref, ri, ra, rr, rs), (fit, fi, fa, fr, fs) = sets["ref"], sets["fit"]
+    # trans_init: centres are the reference atoms (aligners.py:712-727, :816-822)
+    tk = _trans_kw(pairs, trans_init, "_ref_xyz_t", "atom_pos", dev, ri, num_repeats_per_trans,
+                   topk)
     return _align(pairs, "vol_and_surf_esp", ref, fit, None, None, ri, fi, alpha=alpha, lam=lam,
                   steps=steps_fine, lr=lr,
                   num_seeds=num_repeats or seeds_for("vol_and_surf_esp"),
                   ref_atoms=ra, fit_atoms=fa, ref_radii=rr, fit_radii=fr, ref_surf=rs,
                   fit_surf=fs, probe_radius=probe_radius, esp_weight=esp_weight,
-                  esp_stride=esp_stride)
+                  esp_stride=esp_stride, **tk)
 
 
 _align_batch_esp_combo = _align_batch_vol_and_surf_esp
@@ -280,13 +293,13 @@ def _align_batch_pharm(pairs, *, similarity: str = "tanimoto", extended_points: 
     """Directional pharmacophore alignment; writes transform_pharm / sim_aligned_pharm."""
     if not pairs:
         return
-    if trans_init:
-        raise NotImplementedError("trans_init=True is not part of the CUDA backend")
     dev = _device_of(pairs)
     rp, fp, ri, fi = _pharm_inputs(pairs, dev)
+    # trans_init: centres are the reference anchors (aligners.py:932, :966-967)
+    tk = _trans_kw(pairs, trans_init, "_ref_pharm_ancs_t", "pharm_ancs", dev, ri, 10, topk)
     return _align(pairs, "pharm", None, None, rp, fp, ri, fi, steps=steps_fine, lr=lr,
                   num_seeds=num_repeats or seeds_for("pharm"), similarity=similarity,
-                  extended_points=extended_points, only_extended=only_extended)
+                  extended_points=extended_points, only_extended=only_extended, **tk)
 
 
 def _align_batch_vol_color(pairs, *, alpha: float = 0.81, color_weight: float = 0.5,
@@ -295,23 +308,23 @@ def _align_batch_vol_color(pairs, *, alpha: float = 0.81, color_weight: float = 
                            steps_fine: int = 100, lr: float = 0.075):
     """Atom shape + directionless colour; writes transform_vol_color / sim_aligned_vol_color."""
     return _combo(pairs, "vol_color", alpha, color_weight, trans_init, num_repeats, steps_fine,
-                  lr)
+                  lr, num_repeats_per_trans, topk)
 
 
 def _align_batch_vol_pharm(pairs, *, alpha: float = 0.81, color_weight: float = 0.5,
                            trans_init: bool = False, num_repeats: int = 50,
+                           num_repeats_per_trans: int = 10, topk: int = 30,
                            steps_fine: int = 100, lr: float = 0.075, **_):
     """Atom shape + directional (cosine-weighted) pharmacophores with one shared pose;
     writes transform_vol_pharm / sim_aligned_vol_pharm."""
     return _combo(pairs, "vol_pharm", alpha, color_weight, trans_init, num_repeats, steps_fine,
-                  lr)
+                  lr, num_repeats_per_trans, topk)
 
 
-def _combo(pairs, mode, alpha, color_weight, trans_init, num_repeats, steps_fine, lr):
+def _combo(pairs, mode, alpha, color_weight, trans_init, num_repeats, steps_fine, lr,
+           num_repeats_per_trans=10, topk=30):
     if not pairs:
         return
-    if trans_init:
-        raise NotImplementedError("trans_init=True is not part of the CUDA backend")
     dev = _device_of(pairs)
     xr = _ensure(pairs, "_ref_xyz_t", "atom_pos", _f32, dev)
     xf = _ensure(pairs, "_fit_xyz_t", "atom_pos", _f32, dev)
@@ -329,5 +342,8 @@ def _combo(pairs, mode, alpha, color_weight, trans_init, num_repeats, steps_fine
     fit, fi = _cloud_set(xf, device=dev, dedup=df)
     rp, _ = _pharm_set(tr, ar, vr, dev, dedup=dr)
     fp, _ = _pharm_set(tf, af, vf, dev, dedup=df)
+    # trans_init: centres are the reference atoms (aligners.py:1064, :1109-1113)
+    tk = _trans_kw(pairs, trans_init, "_ref_xyz_t", "atom_pos", dev, ri, num_repeats_per_trans,
+                   topk)
     return _align(pairs, mode, ref, fit, rp, fp, ri, fi, alpha=alpha, color_weight=color_weight,
-                  steps=steps_fine, lr=lr, num_seeds=num_repeats or seeds_for(mode))
+                  steps=steps_fine, lr=lr, num_seeds=num_repeats or seeds_for(mode), **tk)

@@ -28,6 +28,7 @@ import torch
 
 from . import align as al
 from . import kernels as K
+from . import legacy_seeds
 from .layout import CloudSet, PharmSet, _offsets
 
 LAM_SCALING = al.LAM_SCALING
@@ -182,11 +183,40 @@ def align_device(mode, ref: Optional[CloudSet], fit: Optional[CloudSet],
                  ref_ph: Optional[PharmSet], fit_ph: Optional[PharmSet], pair_ref, pair_fit,
                  *, alpha=0.81, lam=0.3, color_weight=0.5, num_seeds=50, steps=200, lr=0.1,
                  seeds=None, ref_self=None, fit_self=None, ref_self_ph=None, fit_self_ph=None,
-                 similarity="tanimoto", extended_points=False, only_extended=False, **tile):
+                 similarity="tanimoto", extended_points=False, only_extended=False,
+                 trans_centres: Optional[CloudSet] = None, num_repeats_per_trans: int = 10,
+                 topk: int = 30, **tile):
     """Device-resident form of :func:`align_host` (all tensors already on the GPU).
-    ``similarity`` / ``extended_points`` / ``only_extended`` apply to mode "pharm"."""
+    ``similarity`` / ``extended_points`` / ``only_extended`` apply to mode "pharm".
+
+    ``trans_centres`` (a CloudSet indexed like the reference molecules) selects the
+    translation-seeded starts of the reference's ``trans_init=True``: per pair the legacy grid
+    (identity, 4 principal-axis poses, ``num_repeats_per_trans`` Fibonacci rotations per
+    centre) built from the clouds the reference seeds from (the surfaces for
+    vol_and_surf_esp, the centred anchors for pharm, else the aligned clouds), every pose
+    scored by a one-step launch, and the ``topk`` best refined for ``steps``."""
     if mode != "pharm" and (similarity != "tanimoto" or extended_points or only_extended):
         raise ValueError("similarity and extended points apply to mode 'pharm' only")
+    if trans_centres is not None:
+        if seeds is not None:
+            raise ValueError("seeds and trans_centres are exclusive")
+        kw = dict(alpha=alpha, lam=lam, color_weight=color_weight, lr=lr, ref_self=ref_self,
+                  fit_self=fit_self, ref_self_ph=ref_self_ph, fit_self_ph=fit_self_ph,
+                  similarity=similarity, extended_points=extended_points,
+                  only_extended=only_extended, **tile)
+        shift = None
+        if mode == "pharm":
+            rph, shift = _centred_pharm(ref_ph)
+            g_ref, g_fit = _as_cloud(rph), _as_cloud(_centred_pharm(fit_ph)[0])
+        elif mode in ESP_COMBO_MODES:
+            g_ref, g_fit = tile["ref_surf"], tile["fit_surf"]
+        else:
+            g_ref, g_fit = ref, fit
+        gq, gt, G = legacy_seeds.grid_packed(g_ref, g_fit, trans_centres, pair_ref, pair_fit,
+                                             num_repeats_per_trans, shift)
+        coarse = align_device(mode, ref, fit, ref_ph, fit_ph, pair_ref, pair_fit, steps=1,
+                              seeds=(gq, gt), **kw)
+        seeds = legacy_seeds.select(coarse.rows[0], gq, gt, G, topk)
     if mode in ESP_COMBO_MODES:
         # shape centres steer the pose; tile holds the ESP-comparison sets and parameters
         if seeds is None:

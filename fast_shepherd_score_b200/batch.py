@@ -74,8 +74,8 @@ class MoleculePairBatch:
         _resolve(backend)
         if not no_H:
             raise ValueError("backend='cuda' aligns heavy atoms (no_H=True)")
-        if trans_init:
-            raise NotImplementedError("trans_init=True is not part of the CUDA backend")
+        # trans_init is not forwarded to the vol fast path by the reference either
+        # (container/_batch.py:362-368): batched seeds are used
         sc = A._align_batch_vol(self.pairs, alpha=alpha, steps_fine=self._steps("vol", max_num_steps),
                                 num_repeats=self._seeds("vol", num_repeats), lr=lr)
         return self._finish("vol", sc, "_fit_xyz_t", return_aligned, verbose)
@@ -99,8 +99,7 @@ class MoleculePairBatch:
                         use_shmap: bool = False, verbose: bool = False,
                         backend: Optional[str] = None, return_aligned: bool = False):
         _resolve(backend)
-        if trans_init:
-            raise NotImplementedError("trans_init=True is not part of the CUDA backend")
+        # as for vol, the reference's surf fast path ignores trans_init (_batch.py:813-818)
         sc = A._align_batch_surf(self.pairs, alpha=alpha,
                                  steps_fine=self._steps("surf", max_num_steps),
                                  num_repeats=self._seeds("surf", num_repeats), lr=lr)
@@ -131,11 +130,9 @@ class MoleculePairBatch:
         score every step by default, as the reference's CUDA-graph loop; 5 matches its eager
         loop."""
         _resolve(backend)
-        if trans_init:
-            raise NotImplementedError("trans_init=True is not part of the CUDA backend")
         sc = A._align_batch_vol_and_surf_esp(
             self.pairs, alpha=alpha, lam=lam, probe_radius=probe_radius, esp_weight=esp_weight,
-            num_repeats=self._seeds("vol_and_surf_esp", num_repeats),
+            trans_init=trans_init, num_repeats=self._seeds("vol_and_surf_esp", num_repeats),
             steps_fine=self._steps("vol_and_surf_esp", max_num_steps), lr=lr,
             esp_stride=esp_stride)
         return self._finish("vol_and_surf_esp", sc, "_fit_surf_t", return_aligned, verbose)

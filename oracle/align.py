@@ -382,3 +382,31 @@ def align_esp_combo(C1, C2, CN, CM, A1, A2, Q1, Q2, R1, R2, AN, AM, S1, S2, PE1,
         int(steps), float(np.float32(lr)), L(best), L(bq), L(bt), _threads(nthreads))
     out = _pick(best, bq, bt, nb, S)
     return (out + ((best, bq, bt),)) if return_rows else out
+
+
+# --------------------------------------------------------------------------------------------
+# translation-seeded starts (trans_init=True): accel/drivers/esp.py:228-262 and its twins in
+# pharm.py:244-283, vol_color.py:253-291, esp_combo.py:407-460
+# --------------------------------------------------------------------------------------------
+def select_top(scores, G, topk):
+    """Indices (K, topk) of the best-scoring start poses per pair (``coarse_score.topk``),
+    rows at or past a pair's pose count G excluded."""
+    sc = np.array(scores, np.float64, copy=True)
+    Gm = sc.shape[1]
+    if topk > int(np.min(G)):
+        raise ValueError("topk exceeds a pair's pose count")
+    sc[np.arange(Gm)[None, :] >= np.asarray(G)[:, None]] = -np.inf
+    return np.argsort(-sc, axis=1, kind="stable")[:, :topk]
+
+
+def align_trans(align_fn, args, grid_q, grid_t, G, *, topk=30, steps=100, **kw):
+    """Coarse grid + top-k + fine: every grid pose scored once (the row scores of a one-step
+    run are the seeds' own scores), the ``topk`` best per pair refined for ``steps``.
+    ``align_fn`` is one of the align_* drivers above, called with ``args`` and ``kw``."""
+    grid_q, grid_t = _f32(grid_q), _f32(grid_t)
+    K, Gm = grid_q.shape[:2]
+    *_, (best, _, _) = align_fn(*args, seeds=(grid_q, grid_t), steps=1, return_rows=True, **kw)
+    idx = select_top(best.reshape(K, Gm), G, topk)
+    sq = np.take_along_axis(grid_q, idx[..., None], 1)
+    st = np.take_along_axis(grid_t, idx[..., None], 1)
+    return align_fn(*args, seeds=(sq, st), steps=steps, **kw)

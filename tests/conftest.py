@@ -17,7 +17,8 @@ def pytest_configure(config):
 def golden():
     import numpy as np
     d = os.path.join(ROOT, "tests", "golden")
-    return {k: np.load(os.path.join(d, f"{k}.npz")) for k in ("kernels", "seeds", "align", "scores", "pharm_ext", "esp_combo")}
+    return {k: np.load(os.path.join(d, f"{k}.npz")) for k in ("kernels", "seeds", "align", "scores", "pharm_ext", "esp_combo",
+                                                             "trans_init")}
 
 
 @pytest.fixture(scope="session")

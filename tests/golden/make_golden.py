@@ -85,6 +85,8 @@ def main():
         return make_pharm_ext()
     if args.only == "esp_combo":
         return make_esp_combo()
+    if args.only == "trans_init":
+        return make_trans_init()
     import torch
     torch.set_num_threads(max(1, os.cpu_count() or 1))
     from shepherd_score.accel.kernels import cpu as rk
@@ -271,6 +273,7 @@ def main():
     print("scores.npz")
     make_pharm_ext()
     make_esp_combo()
+    make_trans_init()
 
 
 def make_pharm_ext():
@@ -401,6 +404,154 @@ def make_esp_combo():
     out.update(al_score=sc.numpy(), al_q=bq.numpy(), al_t=bt.numpy())
     np.savez_compressed(os.path.join(HERE, "esp_combo.npz"), **out)
     print("esp_combo.npz")
+
+
+def make_trans_init():
+    """trans_init.npz: the legacy translation-seeded path (trans_init=True).  Per pair, the
+    reference's start grid (legacy_seeds_with_translations_torch: identity, 4 principal-axis
+    poses, 10 Fibonacci rotations per translation centre) and the coarse-grid + top-k + fine
+    alignment of the surf_esp, pharm, vol_color and vol_and_surf_esp drivers (one pair per call,
+    CPU path, early stop off), on their own seeded molecules; plus the 45-rotation table the
+    legacy path uses for num_repeats_per_trans=45."""
+    import torch
+    from shepherd_score.accel.kernels import cpu as rk
+    from shepherd_score.accel.drivers._common import legacy_seeds_with_translations_torch
+    from shepherd_score.accel.drivers.esp import coarse_fine_esp_align_many
+    from shepherd_score.accel.drivers.pharm import coarse_fine_pharm_align_many
+    from shepherd_score.accel.drivers.pharm_overlap import batch_pharm_self_overlap
+    from shepherd_score.accel.drivers.vol_color import coarse_fine_vol_color_align_many
+    from shepherd_score.accel.drivers.esp_combo import (coarse_fine_esp_combo_align_many,
+                                                        _self_overlap_chunks)
+    from shepherd_score.alignment._torch import _get_45_fibo
+    from shepherd_score.score.constants import LAM_SCALING
+
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a))
+    ES = 10 ** 9
+    rng = np.random.default_rng(91)
+    out = {"fibo45": _get_45_fibo().numpy()}
+    kw = dict(num_repeats_per_trans=10, topk=30, steps_fine=30, lr=0.1, early_stop_patience=ES)
+
+    def collect(tag, results):
+        out[f"{tag}_score"] = np.array([r[0] for r in results], np.float32)
+        out[f"{tag}_q"] = np.stack([r[1] for r in results]).astype(np.float32)
+        out[f"{tag}_t"] = np.stack([r[2] for r in results]).astype(np.float32)
+
+    # surf_esp: grid from the surfaces, translation centres = a few interior points
+    refs, fits = syn.esp_surface_pairs(4, seed=41, lo=40, hi=90)
+    fits[0] = (rotated_copy(rng, refs[0][0])[0], refs[0][1].copy())
+    ctr = [(0.5 * p[rng.choice(len(p), n, replace=False)]).astype(np.float32)
+           for (p, _), n in zip(refs, (5, 7, 6, 5))]
+    lam_s = 0.3 * LAM_SCALING
+    grids, res = [], []
+    for (pa, ca), (pb, cb), c in zip(refs, fits, ctr):
+        q, t = legacy_seeds_with_translations_torch(T(pa), T(pb), T(c), num_repeats_per_trans=10)
+        grids.append((q.detach().numpy(), t.detach().numpy()))
+        VAA = rk._batch_self_overlap_esp(T(pa[None]), T(ca[None]), T([len(pa)]), 0.81, lam_s)
+        VBB = rk._batch_self_overlap_esp(T(pb[None]), T(cb[None]), T([len(pb)]), 0.81, lam_s)
+        sc, bq, bt = coarse_fine_esp_align_many(
+            T(pa[None]), T(pb[None]), T(ca[None]), T(cb[None]), VAA, VBB, alpha=0.81,
+            lam=lam_s, trans_centers=T(c[None]), **kw)
+        res.append((float(sc[0]), bq[0].detach().numpy(), bt[0].detach().numpy()))
+    EA, EN = pad([p for p, _ in refs]); EB, EM = pad([p for p, _ in fits])
+    ECA, _ = pad([c for _, c in refs]); ECB, _ = pad([c for _, c in fits])
+    TC, TN = pad(ctr)
+    GQ, GN = pad([g[0] for g in grids]); GT, _ = pad([g[1] for g in grids])
+    out.update(esp_A=EA, esp_B=EB, esp_CA=ECA, esp_CB=ECB, esp_N=EN, esp_M=EM,
+               esp_lam=np.float64(lam_s), esp_TC=TC, esp_TN=TN, esp_GQ=GQ, esp_GT=GT,
+               esp_G=GN)
+    collect("esp", res)
+    q45, t45 = legacy_seeds_with_translations_torch(T(refs[1][0]), T(fits[1][0]), T(ctr[1][:2]),
+                                                    num_repeats_per_trans=45)
+    out.update(g45_q=q45.detach().numpy(), g45_t=t45.detach().numpy())
+
+    def grid_of(a, b, c):
+        q, t = legacy_seeds_with_translations_torch(T(a), T(b), T(c), num_repeats_per_trans=10)
+        return q.detach().numpy(), t.detach().numpy()
+
+    def store_grids(tag, grids):
+        GQ, GN = pad([g[0] for g in grids]); GT, _ = pad([g[1] for g in grids])
+        out.update({f"{tag}_GQ": GQ, f"{tag}_GT": GT, f"{tag}_G": GN})
+
+    # pharm (Tanimoto, directional): translation centres = the reference anchors; the driver
+    # builds the grid on per-cloud centred anchors with the centres shifted alike
+    prefs, pfits = syn.shape_pharm_pairs(4, seed=42, ph_lo=4, ph_hi=9, atom_hi=30)
+    res, grids = [], []
+    for r, f in zip(prefs, pfits):
+        ca = T(r["pharm_ancs"]).sum(0) / float(len(r["pharm_ancs"]))
+        cb = T(f["pharm_ancs"]).sum(0) / float(len(f["pharm_ancs"]))
+        grids.append(grid_of((T(r["pharm_ancs"]) - ca).numpy(), (T(f["pharm_ancs"]) - cb).numpy(),
+                             (T(r["pharm_ancs"]) - ca).numpy()))
+        # self overlaps as the public driver computes them (pharm.py:735-751): the coarse
+        # grid ranks poses by the similarity built from them
+        tr, tf = T(r["pharm_types"][None].astype(np.int64)), T(f["pharm_types"][None].astype(np.int64))
+        VAA = batch_pharm_self_overlap(T(r["pharm_ancs"][None]), T(r["pharm_vecs"][None]), tr,
+                                       extended_points=False, only_extended=False,
+                                       N_real=T([len(r["pharm_ancs"])]))
+        VBB = batch_pharm_self_overlap(T(f["pharm_ancs"][None]), T(f["pharm_vecs"][None]), tf,
+                                       extended_points=False, only_extended=False,
+                                       N_real=T([len(f["pharm_ancs"])]))
+        sc, bq, bt = coarse_fine_pharm_align_many(
+            T(r["pharm_ancs"][None]), T(f["pharm_ancs"][None]), T(r["pharm_vecs"][None]),
+            T(f["pharm_vecs"][None]), tr, tf, VAA, VBB,
+            trans_centers=T(r["pharm_ancs"][None]), **kw)
+        res.append((float(sc[0]), bq[0].detach().numpy(), bt[0].detach().numpy()))
+    PA, PN = pad([m["pharm_ancs"] for m in prefs]); PB, PM = pad([m["pharm_ancs"] for m in pfits])
+    PRV, _ = pad([m["pharm_vecs"] for m in prefs]); PFV, _ = pad([m["pharm_vecs"] for m in pfits])
+    PAt, _ = pad([m["pharm_types"] for m in prefs], fill=0, dtype=np.int64)
+    PBt, _ = pad([m["pharm_types"] for m in pfits], fill=0, dtype=np.int64)
+    out.update(pharm_A=PA, pharm_B=PB, pharm_RV=PRV, pharm_FV=PFV, pharm_At=PAt, pharm_Bt=PBt,
+               pharm_N=PN, pharm_M=PM)
+    collect("pharm", res)
+    store_grids("pharm", grids)
+
+    # vol_color: grid from the atom centres, translation centres = the reference atoms
+    res, grids = [], []
+    for r, f in zip(prefs, pfits):
+        grids.append(grid_of(r["atom_pos"], f["atom_pos"], r["atom_pos"]))
+        VAA = rk._batch_self_overlap(T(r["atom_pos"][None]), T([len(r["atom_pos"])]), 0.81)
+        VBB = rk._batch_self_overlap(T(f["atom_pos"][None]), T([len(f["atom_pos"])]), 0.81)
+        sc, bq, bt = coarse_fine_vol_color_align_many(
+            T(r["atom_pos"][None]), T(f["atom_pos"][None]),
+            T(r["pharm_types"][None].astype(np.int64)), T(f["pharm_types"][None].astype(np.int64)),
+            T(r["pharm_ancs"][None]), T(f["pharm_ancs"][None]), VAA, VBB, alpha=0.81,
+            color_weight=0.5, trans_centers=T(r["atom_pos"][None]), **kw)
+        res.append((float(sc[0]), bq[0].detach().numpy(), bt[0].detach().numpy()))
+    CA_, CN = pad([m["atom_pos"] for m in prefs]); CB_, CM = pad([m["atom_pos"] for m in pfits])
+    PAt8, _ = pad([m["pharm_types"] for m in prefs], fill=8, dtype=np.int64)
+    PBt8, _ = pad([m["pharm_types"] for m in pfits], fill=8, dtype=np.int64)
+    out.update(color_A=CA_, color_B=CB_, color_N=CN, color_M=CM, color_At=PAt8, color_Bt=PBt8)
+    collect("color", res)
+    store_grids("color", grids)
+
+    # vol_and_surf_esp: grid from the surfaces, translation centres = the reference centres
+    refs, fits = syn.esp_combo_pairs(3, seed=43, surf_lo=50, surf_hi=80)
+    res, grids = [], []
+    for r, f in zip(refs, fits):
+        grids.append(grid_of(r["surf"], f["surf"], r["centers"]))
+        one = lambda m, k: T(m[k][None])
+        cnt = lambda m, k: T([len(m[k])])
+        VAA = _self_overlap_chunks(one(r, "centers"), cnt(r, "centers"), 0.81)
+        VBB = _self_overlap_chunks(one(f, "centers"), cnt(f, "centers"), 0.81)
+        sc, bq, bt = coarse_fine_esp_combo_align_many(
+            one(r, "atoms"), one(f, "atoms"), one(r, "centers"), one(f, "centers"),
+            one(r, "surf"), one(f, "surf"), one(r, "charges"), one(f, "charges"),
+            one(r, "surf_esp"), one(f, "surf_esp"), one(r, "radii"), one(f, "radii"), VAA, VBB,
+            alpha=0.81, lam=0.001, probe_radius=1.0, esp_weight=0.5,
+            trans_centers=one(r, "centers"), **kw)
+        res.append((float(sc[0]), bq[0].detach().numpy(), bt[0].detach().numpy()))
+    arr = {}
+    for side, mols in (("1", refs), ("2", fits)):
+        arr["C" + side], arr["CN" + side] = pad([m["centers"] for m in mols])
+        arr["A" + side], arr["AN" + side] = pad([m["atoms"] for m in mols])
+        arr["Q" + side], _ = pad([m["charges"] for m in mols])
+        arr["R" + side], _ = pad([m["radii"] for m in mols])
+        arr["S" + side], arr["SN" + side] = pad([m["surf"] for m in mols])
+        arr["PE" + side], _ = pad([m["surf_esp"] for m in mols])
+    out.update({"combo_" + k: v for k, v in arr.items()})
+    collect("combo", res)
+    store_grids("combo", grids)
+    np.savez_compressed(os.path.join(HERE, "trans_init.npz"), **out)
+    print("trans_init.npz")
 
 
 if __name__ == "__main__":
