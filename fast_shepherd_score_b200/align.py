@@ -305,6 +305,15 @@ def _default_counts(x, K, pad, dev):
     return torch.as_tensor(x, device=dev).to(torch.int64)
 
 
+TILE_KEYS = ("lanes_per_pose", "chunks", "cta_per_sm", "accumulate", "kernel_variant")
+
+
+def coarse_tile(tile: dict) -> dict:
+    """Extra arguments of the one-step coarse-scoring launch: the library's built-in tile
+    unless the caller chose one (tuning a one-step launch costs far more than the launch)."""
+    return {} if any(tile.get(k) for k in TILE_KEYS) else {"accumulate": 1}
+
+
 def _trans_seeds(run, g_ref: CloudSet, g_fit: CloudSet, trans_centers, trans_centers_real,
                  per_trans: int, topk: int, shift=None):
     """Start poses of the translation-seeded path (the reference's trans_centers branch,
@@ -364,13 +373,14 @@ def coarse_fine_esp_align_many(A_batch, B_batch, CA_batch, CB_batch, VAA, VBB, *
     pr, pf = _self_pairs(K, dev)
     VAA, VBB = VAA.to(_f32).contiguous(), VBB.to(_f32).contiguous()
 
-    def run(sd, steps):
+    def run(sd, steps, **extra):
         return align_packed("esp", ref=ref, fit=fit, pair_ref=pr, pair_fit=pf, seed_q=sd[0],
                             seed_t=sd[1], steps=steps, lr=lr, alpha=alpha, lam=lam,
-                            ref_self=VAA, fit_self=VBB, **tile)
+                            ref_self=VAA, fit_self=VBB, **tile, **extra)
 
     if trans_centers is not None:
-        seeds = _trans_seeds(lambda sd, st: run(sd, st).rows[0], ref, fit, trans_centers,
+        coarse = lambda sd, st: run(sd, st, **coarse_tile(tile)).rows[0]
+        seeds = _trans_seeds(coarse, ref, fit, trans_centers,
                              trans_centers_real, num_repeats_per_trans, topk)
     elif seeds is None:
         seeds = kernels.seeds(ref, fit, pr, pf, num_seeds)
@@ -429,17 +439,17 @@ def coarse_fine_pharm_align_many(anchors_1, anchors_2, vectors_1, vectors_2, typ
     fit_ph = PharmSet.from_padded(a2c, types_2, vectors_2, M_real)
     pr, pf = _self_pairs(K, dev)
 
-    def run(sd, steps):
+    def run(sd, steps, **extra):
         return align_packed("pharm", ref_ph=ref_ph, fit_ph=fit_ph, pair_ref=pr, pair_fit=pf,
                             seed_q=sd[0], seed_t=sd[1], steps=steps, lr=lr,
                             similarity=similarity,
                             pharm_extended=extended_code(extended_points, only_extended),
-                            **tile)
+                            **tile, **extra)
 
     if trans_centers is not None:
         # centres are points of the original reference frame: shift them with the anchors
-        seeds = _trans_seeds(lambda sd, st: run(sd, st).rows[0],
-                             CloudSet.from_padded(a1c, N_real),
+        coarse = lambda sd, st: run(sd, st, **coarse_tile(tile)).rows[0]
+        seeds = _trans_seeds(coarse, CloudSet.from_padded(a1c, N_real),
                              CloudSet.from_padded(a2c, M_real), trans_centers.to(_f32),
                              trans_centers_real, num_repeats_per_trans, topk, shift=c_ref)
     elif seeds is None:
@@ -489,17 +499,18 @@ def coarse_fine_esp_combo_align_many(centers_w_H_1, centers_w_H_2, centers_1, ce
     fs = CloudSet.from_padded(points_2.to(_f32), MS, point_charges_2)
     pr, pf = _self_pairs(K, dev)
 
-    def run(sd, steps):
+    def run(sd, steps, **extra):
         return align_packed("esp_combo", ref=ref, fit=fit, pair_ref=pr, pair_fit=pf,
                             seed_q=sd[0], seed_t=sd[1], steps=steps, lr=lr, alpha=alpha,
                             lam=lam, ref_self=VAA, fit_self=VBB, ref_atoms=ra, fit_atoms=fa,
                             ref_radii=rrad, fit_radii=frad, ref_surf=rs, fit_surf=fs,
                             probe_radius=probe_radius, esp_weight=esp_weight,
-                            esp_stride=esp_stride, **tile)
+                            esp_stride=esp_stride, **tile, **extra)
 
     if trans_centers is not None:
         # the legacy grid is built from the surface clouds (esp_combo.py:409-412)
-        seeds = _trans_seeds(lambda sd, st: run(sd, st).rows[0], rs, fs, trans_centers,
+        coarse = lambda sd, st: run(sd, st, **coarse_tile(tile)).rows[0]
+        seeds = _trans_seeds(coarse, rs, fs, trans_centers,
                              trans_centers_real, num_repeats_per_trans, topk)
     elif seeds is None:
         seeds = kernels.seeds(ref, fit, pr, pf, num_seeds)
@@ -543,14 +554,16 @@ def coarse_fine_vol_color_align_many(centers_1, centers_2, ptype_1, ptype_2, anc
     pr, pf = _self_pairs(K, dev)
     VAA, VBB = VAA.to(_f32).contiguous(), VBB.to(_f32).contiguous()
 
-    def run(sd, steps):
+    def run(sd, steps, **extra):
         return align_packed("shape_pharm" if directional else "shape_color", ref=ref, fit=fit,
                             ref_ph=ref_ph, fit_ph=fit_ph, pair_ref=pr, pair_fit=pf,
                             seed_q=sd[0], seed_t=sd[1], steps=steps, lr=lr, alpha=alpha,
-                            color_weight=color_weight, ref_self=VAA, fit_self=VBB, **tile)
+                            color_weight=color_weight, ref_self=VAA, fit_self=VBB, **tile,
+                            **extra)
 
     if trans_centers is not None:
-        seeds = _trans_seeds(lambda sd, st: run(sd, st).rows[0], ref, fit, trans_centers,
+        coarse = lambda sd, st: run(sd, st, **coarse_tile(tile)).rows[0]
+        seeds = _trans_seeds(coarse, ref, fit, trans_centers,
                              trans_centers_real, num_repeats_per_trans, topk)
     elif seeds is None:
         seeds = kernels.seeds(ref, fit, pr, pf, num_seeds)

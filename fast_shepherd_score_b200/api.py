@@ -214,6 +214,7 @@ def align_device(mode, ref: Optional[CloudSet], fit: Optional[CloudSet],
             g_ref, g_fit = ref, fit
         gq, gt, G = legacy_seeds.grid_packed(g_ref, g_fit, trans_centres, pair_ref, pair_fit,
                                              num_repeats_per_trans, shift)
+        kw.update(al.coarse_tile(tile))
         coarse = align_device(mode, ref, fit, ref_ph, fit_ph, pair_ref, pair_fit, steps=1,
                               seeds=(gq, gt), **kw)
         seeds = legacy_seeds.select(coarse.rows[0], gq, gt, G, topk)

