@@ -98,15 +98,17 @@ def candidates(mode: str, max_fit: int, n_starts: int):
             if 2 * base <= n_starts:
                 out.append({"lanes_per_pose": lpp, "chunks": 2 * base, "cta_per_sm": 0,
                             "kernel_variant": var})
-            # small molecules (cheap candidates): start blocks that fill whole warps, so no
-            # lanes shadow an idle start except in a pair's last block
-            if max_fit < 64:
-                for warps in (1, 2):
-                    ppc = warps * (32 // lpp)
-                    ch = -(-n_starts // ppc)
-                    if ch not in (base, 2 * base) and ch <= n_starts:
-                        out.append({"lanes_per_pose": lpp, "chunks": ch, "cta_per_sm": 0,
-                                    "kernel_variant": var})
+            # start blocks that fill whole warps (no lanes shadow an idle start except in a
+            # pair's last block), in CTAs of 1, 2 or 4 warps: CTAs whose warps spread evenly
+            # over the SM's four schedulers.  A 5-warp CTA puts two warps on one scheduler,
+            # and its other warps then wait ~24 % of the time at the per-item barrier
+            # (measured on 200-400 point surfaces).
+            for warps in ((1, 2, 4) if max_fit < 64 else (2, 4)):
+                ppc = warps * (32 // lpp)
+                ch = -(-n_starts // ppc)
+                if ch not in (base, 2 * base) and ch <= n_starts:
+                    out.append({"lanes_per_pose": lpp, "chunks": ch, "cta_per_sm": 0,
+                                "kernel_variant": var})
     if mode in ("shape", "esp") and max_fit >= 16:
         base = _auto_chunks(32, n_starts)
         for acc in (2, 3):
