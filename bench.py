@@ -180,6 +180,31 @@ def flush_l2(buf):
 DRAM_BYTES_PER_PAIR = {"surf_esp": (3.318272e6 + 0.0) / 256}
 
 
+def hbm_peak_gbs():
+    """HBM copy bandwidth to compare the fused kernel's DRAM traffic with: the driver-measured
+    figure when the repository carries one, else the pool's earlier measurement (6650 GB/s)."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        v = d.get("hbm_gbs")
+        if isinstance(v, dict):
+            v = v.get("burst", v.get("value"))
+        return float(v), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def hbm_side(traffic_bytes, kernel_ms):
+    """The HBM view of a launch that is not HBM-bound: achieved DRAM GB/s and its fraction."""
+    if traffic_bytes is None:
+        return None
+    peak, src = hbm_peak_gbs()
+    gbs = traffic_bytes / (kernel_ms * 1e-3) / 1e9
+    return {"achieved": round(gbs, 2), "peak": peak, "unit": "GB/s",
+            "frac": round(gbs / peak, 6), "peak_source": src}
+
+
 def run_cuda(args, wl):
     import torch
     import torch.distributed as dist
@@ -329,7 +354,9 @@ def run_cuda(args, wl):
                      "peak_source": "measured by fss_probe_peak on this GPU: "
                                     f"ex2 {peak['ex2'] / 1e9:.0f} G/s, ffma "
                                     f"{peak['ffma'] / 1e9:.0f} G/s /{per_term_fp32} per term",
-                     "terms_per_launch": terms, "kernel_ms": round(kavg, 3)},
+                     "terms_per_launch": terms, "kernel_ms": round(kavg, 3),
+                     "hbm": hbm_side(DRAM_BYTES_PER_PAIR[mode] * n_pairs
+                                     if mode in DRAM_BYTES_PER_PAIR else None, kavg)},
         "clocks": clk,
     }
     if args.cpu_baseline and world == 1:
