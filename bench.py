@@ -240,7 +240,8 @@ def run_cuda(args, wl):
     tile = {}
     if args.tile:   # fixed tiling (no autotuning): lanes_per_pose,chunks,cta_per_sm,accumulate
         v = [int(x) for x in args.tile.split(",")]
-        tile = dict(zip(("lanes_per_pose", "chunks", "cta_per_sm", "accumulate"), v))
+        tile = dict(zip(("lanes_per_pose", "chunks", "cta_per_sm", "accumulate",
+                             "kernel_variant"), v))
 
     def step(record_kernel=False):
         if mode == "vol_pharm":
@@ -754,7 +755,8 @@ def run_esp_combo(args, wl):
     tile = {}
     if args.tile:
         v = [int(x) for x in args.tile.split(",")]
-        tile = dict(zip(("lanes_per_pose", "chunks", "cta_per_sm", "accumulate"), v))
+        tile = dict(zip(("lanes_per_pose", "chunks", "cta_per_sm", "accumulate",
+                             "kernel_variant"), v))
     kern = []
 
     def step(c1, c2, a1, a2, r1, r2, s1, s2, record=False):
@@ -954,7 +956,8 @@ def main(argv=None):
                     help="skip the screening-server leg (Poisson stream, p50/p99)")
     ap.add_argument("--server-seconds", type=float, default=20.0)
     ap.add_argument("--tile", default="", help="fixed tiling instead of the autotuner: "
-                    "lanes_per_pose,chunks,cta_per_sm,accumulate (e.g. 32,0,0,2)")
+                    "lanes_per_pose,chunks,cta_per_sm,accumulate[,kernel_variant] (e.g. 32,0,0,2 or "
+                    "16,7,0,0,4)")
     args = ap.parse_args(argv)
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":

@@ -169,8 +169,9 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
             order = cost_order(ref.counts[pr], fit.counts[pf], dev)
         else:
             order = cost_order(ref_ph.counts[pr], fit_ph.counts[pf], dev)
-    if (lanes_per_pose == 0 and chunks == 0 and cta_per_sm == 0 and accumulate == 0
-            and kernel_variant == 0 and autotune.enabled() and P >= 64 and steps > 0):
+    tuned = (lanes_per_pose == 0 and chunks == 0 and cta_per_sm == 0 and accumulate == 0
+             and kernel_variant == 0 and autotune.enabled() and P >= 64 and steps > 0)
+    if tuned:
         extra = (dict(ref_atoms=ref_atoms, fit_atoms=fit_atoms, ref_radii=ref_radii,
                       fit_radii=fit_radii, ref_surf=ref_surf, fit_surf=fit_surf,
                       probe_radius=probe_radius, esp_weight=esp_weight, esp_stride=esp_stride)
@@ -194,7 +195,7 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
     LAST_TILE.update(lanes_per_pose=int(lanes_per_pose), chunks=int(chunks),
                      cta_per_sm=int(cta_per_sm), accumulate=int(accumulate),
                      kernel_variant=int(kernel_variant),
-                     autotuned=autotune.enabled() and P >= 64)
+                     autotuned=tuned)
     d = AlignDesc()
     d.mode, d.n_pairs, d.n_starts, d.steps = m, P, S, int(steps)
     d.pair_ref, d.pair_fit = ptr(pair_ref, _i32), ptr(pair_fit, _i32)
