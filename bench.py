@@ -982,8 +982,17 @@ def main(argv=None):
     ap.add_argument("--tile", default="", help="fixed tiling instead of the autotuner: "
                     "lanes_per_pose,chunks,cta_per_sm,accumulate[,kernel_variant] (e.g. 32,0,0,2 or "
                     "16,7,0,0,4)")
+    ap.add_argument("--server-only", action="store_true",
+                    help="run only the screening-server leg on one GPU and print its JSON "
+                         "(library-streaming profiles)")
     args = ap.parse_args(argv)
     wl = WORKLOADS[args.workload]
+    if args.server_only:
+        import torch
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
+        print(json.dumps({"server": server_bench(dev, duration=args.server_seconds)}), flush=True)
+        return None
     if args.impl == "reference":
         return run_reference(args, wl)
     if wl["mode"] == "vol_and_surf_esp":
