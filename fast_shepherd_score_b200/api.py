@@ -32,6 +32,9 @@ from . import legacy_seeds
 from .layout import CloudSet, PharmSet, _offsets
 
 LAM_SCALING = al.LAM_SCALING
+# rows (pairs x grid poses) of one coarse-scoring launch of the translation-seeded path
+TRANS_GRID_ROWS = 1 << 22
+
 SHAPE_MODES = ("vol", "surf", "vol_esp", "surf_esp")
 PHARM_MODES = ("pharm",)
 COMBO_MODES = ("vol_color", "vol_pharm")
@@ -212,12 +215,26 @@ def align_device(mode, ref: Optional[CloudSet], fit: Optional[CloudSet],
             g_ref, g_fit = tile["ref_surf"], tile["fit_surf"]
         else:
             g_ref, g_fit = ref, fit
-        gq, gt, G = legacy_seeds.grid_packed(g_ref, g_fit, trans_centres, pair_ref, pair_fit,
-                                             num_repeats_per_trans, shift)
         kw.update(al.coarse_tile(tile))
-        coarse = align_device(mode, ref, fit, ref_ph, fit_ph, pair_ref, pair_fit, steps=1,
-                              seeds=(gq, gt), **kw)
-        seeds = legacy_seeds.select(coarse.rows[0], gq, gt, G, topk)
+        # the grid holds 5 + 10 x centres poses per pair: score it in pair chunks of at most
+        # TRANS_GRID_ROWS rows, so a library shard's grid never has to exist at once
+        P = int(pair_ref.shape[0])
+        g_max = 5 + num_repeats_per_trans * int(trans_centres.max_points)
+        step = max(1, TRANS_GRID_ROWS // max(g_max, 1))
+        sel_q, sel_t = [], []
+        for a in range(0, P, step):
+            pr, pf = pair_ref[a:a + step], pair_fit[a:a + step]
+            gq, gt, G = legacy_seeds.grid_packed(g_ref, g_fit, trans_centres, pr, pf,
+                                                 num_repeats_per_trans, shift)
+            coarse = align_device(mode, ref, fit, ref_ph, fit_ph, pr, pf, steps=1,
+                                  seeds=(gq, gt), **kw)
+            q_, t_ = legacy_seeds.select(coarse.rows[0], gq, gt, G, topk)
+            sel_q.append(q_)
+            sel_t.append(t_)
+        seeds = (torch.cat(sel_q), torch.cat(sel_t)) if sel_q else None
+        if seeds is None:
+            seeds = (torch.zeros(0, topk, 4, device=pair_ref.device),
+                     torch.zeros(0, topk, 3, device=pair_ref.device))
     if mode in ESP_COMBO_MODES:
         # shape centres steer the pose; tile holds the ESP-comparison sets and parameters
         if seeds is None:

@@ -346,6 +346,17 @@ def query_to_device(q, mode: str, device, alpha: float = 0.81):
     return cs, ps, {}
 
 
+def _query_centres(q, mode: str, device) -> CloudSet:
+    """The query's translation centres for trans_init: its heavy atoms, or its pharmacophore
+    anchors in mode pharm (the reference's aligners take them from the reference molecule)."""
+    g = lambda name: getattr(q, name, None) if not isinstance(q, dict) else q.get(name)
+    pts = g("pharm_ancs") if mode == "pharm" else g("atom_pos")
+    if pts is None:
+        raise ValueError("trans_init needs the query's "
+                         + ("pharm_ancs" if mode == "pharm" else "atom_pos"))
+    return CloudSet.from_arrays([np.asarray(pts, np.float32)], device=device)
+
+
 def _centred_query(q):
     """A copy of the query with every coordinate array shifted by its atom COM."""
     get = (lambda n: q.get(n)) if isinstance(q, dict) else (lambda n: getattr(q, n, None))
@@ -424,8 +435,6 @@ def screen_many(queries: Sequence, store: ProfileStore, mode: str = "surf_esp", 
                          f"not support {mode!r}")
     if align_kwargs.get("no_H") is False:
         raise ValueError("screen() aligns heavy atoms only; no_H=False is not supported")
-    if align_kwargs.get("trans_init"):
-        raise NotImplementedError("trans_init=True is not part of the CUDA backend")
     if mode == "vol_esp" and "lam" not in align_kwargs:
         raise ValueError("vol_esp requires an explicit lam=...")
     if alpha is None:
@@ -441,6 +450,13 @@ def screen_many(queries: Sequence, store: ProfileStore, mode: str = "surf_esp", 
         so = [scores_out] if isinstance(scores_out, np.ndarray) and len(qs) == 1 else list(scores_out)
     heaps = [_TopK(top_k) for _ in qs]
     qdev = [query_to_device(q, mode, device, alpha) for q in qs]
+    # trans_init: the legacy translation-seeded starts with the query's atoms (anchors for
+    # pharm) as translation centres, as the reference's per-pair screening path aligns
+    # MoleculePair(query, library molecule) (screen.py:1006-1008); vol and surf ignore it there
+    trans = bool(align_kwargs.get("trans_init")) and mode not in ("vol", "surf")
+    tks = [dict(trans_centres=_query_centres(q, mode, device),
+                num_repeats_per_trans=int(align_kwargs.get("num_repeats_per_trans", 10)),
+                topk=int(align_kwargs.get("topk", 30))) if trans else {} for q in qs]
     done = 0
     for si in range(store.num_shards):
         sh, arrs = store.read_shard(si)
@@ -453,7 +469,7 @@ def screen_many(queries: Sequence, store: ProfileStore, mode: str = "surf_esp", 
         ids = arrs["ids"]
         for qi, (rc, rp, ref_x) in enumerate(qdev):
             sc, q, t = api.align_device(mode, rc, fit, rp, fit_ph, pr, pf, **kw, **ref_x,
-                                        **fit_x)
+                                        **fit_x, **tks[qi])
             if so[qi] is not None:
                 so[qi][sh["start"]:sh["start"] + K] = sc.cpu().numpy()
             k = min(top_k, K)

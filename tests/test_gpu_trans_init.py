@@ -115,3 +115,41 @@ def test_object_api_trans_init(golden, cuda):
     sv, _ = MoleculePairBatch(pairs).align_with_vol(trans_init=True, max_num_steps=5,
                                                     backend="cuda")
     assert np.all(np.isfinite(sv))
+
+
+def test_screen_trans_init_matches_driver(tmp_path, cuda):
+    """screen(trans_init=True) takes the query's atoms as translation centres and gives the
+    driver's translation-seeded scores for every library molecule (float32 store, no
+    centring, one shard boundary inside the library).  The top-k of the coarse grid is
+    sensitive to rounding among near-equal poses, so both sides see the same coordinates."""
+    from fast_shepherd_score_b200.screen import ProfileStore, screen
+    from test_store import _mols
+    mols = _mols(9, seed=4)
+    path = str(tmp_path / "lib")
+    with ProfileStore.create(path, num_surf_points=64, modes=["surf_esp"], dtype="float32",
+                             shard_size=5, pre_centered=False) as st:
+        for m in mols:
+            st.add_arrays(**m)
+    store = ProfileStore.open(path)
+    q = mols[0]
+    out = np.zeros(len(mols), np.float32)
+    screen(q, store, "surf_esp", do_center=False, alpha=0.81, top_k=3, scores_out=out,
+           trans_init=True, max_num_steps=20, lr=0.1)
+    pad = lambda xs: torch.nn.utils.rnn.pad_sequence([torch.as_tensor(x) for x in xs],
+                                                      batch_first=True).to(cuda)
+    n = lambda xs: torch.tensor([len(x) for x in xs], device=cuda)
+    A = pad([q["surf_pos"]] * len(mols))
+    B = pad([m["surf_pos"] for m in mols])
+    CA = pad([q["surf_esp"]] * len(mols))
+    CB = pad([m["surf_esp"] for m in mols])
+    lam = 0.3 * al.LAM_SCALING
+    VAA = K.self_overlap(CloudSet.from_padded(A, n([q["surf_pos"]] * len(mols)), CA), 0.81,
+                         True, lam)
+    VBB = K.self_overlap(CloudSet.from_padded(B, n([m["surf_pos"] for m in mols]), CB), 0.81,
+                         True, lam)
+    sc, _, _ = al.coarse_fine_esp_align_many(
+        A, B, CA, CB, VAA, VBB, alpha=0.81, lam=lam, trans_centers=pad([q["atom_pos"]] * len(mols)),
+        steps_fine=20, lr=0.1, N_real=n([q["surf_pos"]] * len(mols)),
+        M_real=n([m["surf_pos"] for m in mols]))
+    np.testing.assert_allclose(out, sc.cpu().numpy(), atol=1e-5)
+    assert out[0] > 0.99
