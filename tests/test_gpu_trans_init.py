@@ -153,3 +153,38 @@ def test_screen_trans_init_matches_driver(tmp_path, cuda):
         M_real=n([m["surf_pos"] for m in mols]))
     np.testing.assert_allclose(out, sc.cpu().numpy(), atol=1e-5)
     assert out[0] > 0.99
+
+
+@pytest.mark.parametrize("mode", ["pharm", "vol_color"])
+def test_object_api_trans_init_pharm_modes(cuda, mode):
+    """align_with_pharm / align_with_vol_color(trans_init=True): the reference's centres
+    (anchors for pharm, atoms for vol_color) and the drivers' translation-seeded results."""
+    from test_gpu_api import _mols, _pairs
+    refs, fits = _mols(6, 21), _mols(6, 22)
+    pairs = _pairs(refs, fits, cuda)
+    b = MoleculePairBatch(pairs)
+    pad = lambda xs, dt=None: torch.nn.utils.rnn.pad_sequence(
+        [torch.as_tensor(np.asarray(x)) for x in xs], batch_first=True).to(cuda)
+    n = lambda xs: torch.tensor([len(x) for x in xs], device=cuda)
+    g = lambda ms, k: [m[k] for m in ms]
+    kw = dict(num_repeats_per_trans=10, topk=30, steps_fine=20, lr=0.1)
+    if mode == "pharm":
+        sc = b.align_with_pharm(trans_init=True, max_num_steps=20, backend="cuda")[0]
+        ref, _, _ = al.coarse_fine_pharm_align_many(
+            pad(g(refs, "pharm_ancs")), pad(g(fits, "pharm_ancs")), pad(g(refs, "pharm_vecs")),
+            pad(g(fits, "pharm_vecs")), pad(g(refs, "pharm_types")), pad(g(fits, "pharm_types")),
+            trans_centers=pad(g(refs, "pharm_ancs")), trans_centers_real=n(g(refs, "pharm_ancs")),
+            N_real=n(g(refs, "pharm_ancs")), M_real=n(g(fits, "pharm_ancs")), **kw)
+    else:
+        sc = b.align_with_vol_color(trans_init=True, max_num_steps=20, backend="cuda")[0]
+        A, B = pad(g(refs, "atom_pos")), pad(g(fits, "atom_pos"))
+        NA, NB = n(g(refs, "atom_pos")), n(g(fits, "atom_pos"))
+        VAA = K.self_overlap(CloudSet.from_padded(A, NA), 0.81)
+        VBB = K.self_overlap(CloudSet.from_padded(B, NB), 0.81)
+        tp = lambda ms: pad([np.asarray(t, np.int64) for t in g(ms, "pharm_types")])
+        ref, _, _ = al.coarse_fine_vol_color_align_many(
+            A, B, tp(refs), tp(fits), pad(g(refs, "pharm_ancs")), pad(g(fits, "pharm_ancs")),
+            VAA, VBB, alpha=0.81, color_weight=0.5, trans_centers=A, trans_centers_real=NA,
+            N_real_centers=NA, M_real_centers=NB, N_real_pharm=n(g(refs, "pharm_ancs")),
+            M_real_pharm=n(g(fits, "pharm_ancs")), **kw)
+    np.testing.assert_allclose(np.asarray(sc, np.float32), ref.cpu().numpy(), atol=1e-5)
