@@ -111,8 +111,9 @@ def candidates(mode: str, max_fit: int, n_starts: int):
                                 "kernel_variant": var})
     if mode in ("shape", "esp") and max_fit >= 16:
         base = _auto_chunks(32, n_starts)
+        ch4 = -(-n_starts // 4)     # one pose per warp: CTAs of 4 warps
         for acc in (2, 3):
-            for ch, cps in ((0, 0), (0, 1), (2 * base, 0)):
+            for ch, cps in ((0, 0), (0, 1), (2 * base, 0), (ch4, 0)):
                 if ch <= n_starts:
                     out.append({"lanes_per_pose": 32, "chunks": ch, "cta_per_sm": cps,
                                 "accumulate": acc})
