@@ -284,12 +284,20 @@ def align_device(mode, ref: Optional[CloudSet], fit: Optional[CloudSet],
 
 
 def _centred_pharm(ps: PharmSet):
-    """The set with every molecule's anchors centred on its own centroid (types kept)."""
-    n = torch.as_tensor(ps.counts, device=ps.anc.device)
-    mol = torch.repeat_interleave(torch.arange(len(ps.counts), device=ps.anc.device), n)
+    """The set with every molecule's anchors centred on its own centroid (types kept).  The
+    centroid is a padded per-molecule sum (the reference's masked sum, pharm.py:215-219), so
+    it is deterministic (an atomic scatter-add would make the last bits run-dependent)."""
+    dev = ps.anc.device
+    n = torch.as_tensor(ps.counts, device=dev)
+    mol = torch.repeat_interleave(torch.arange(len(ps.counts), device=dev), n)
     xyz = ps.anc[:, :3]
-    c = torch.zeros(len(ps.counts), 3, device=xyz.device, dtype=xyz.dtype)
-    c.index_add_(0, mol, xyz)
+    L = max(int(ps.max_points), 1)
+    ar = torch.arange(L, device=dev)[None, :]
+    off = torch.cumsum(n, 0) - n
+    mask = ar < n[:, None]
+    rows = torch.where(mask, off[:, None] + ar, torch.zeros_like(ar))
+    pts = xyz[rows] if xyz.shape[0] else torch.zeros(len(ps.counts), L, 3, device=dev)
+    c = torch.where(mask[..., None], pts, torch.zeros_like(pts)).sum(1)
     c = c / n.clamp(min=1).to(xyz.dtype)[:, None]
     anc = ps.anc.clone()
     anc[:, :3] = xyz - c[mol]

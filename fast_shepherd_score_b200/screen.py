@@ -415,50 +415,23 @@ def _batch_kwargs(mode, ak, alpha):
     return kw
 
 
-def screen_many(queries: Sequence, store: ProfileStore, mode: str = "surf_esp", *,
-                backend: Optional[str] = None, do_center: Optional[bool] = None,
-                top_k: int = 1000, ndev: Optional[int] = None, scores_out=None,
-                alpha: Optional[float] = None, progress: bool = False, device=None,
-                **align_kwargs) -> List[List[Hit]]:
-    """Screen a panel of queries against ``store``; one streaming pass over its shards."""
-    if backend not in (None, "cuda"):
-        raise ValueError(f"backend {backend!r} is provided by shepherd_score; this package "
-                         "implements backend='cuda'")
-    if ndev and ndev > 1:
-        raise ValueError("ndev>1: run one process per GPU over disjoint shard ranges "
-                         "(see fast_shepherd_score_b200.server.shard_ranges)")
-    mode = canonical(mode)
-    if mode not in _SCREEN_MODES:
-        raise ValueError(f"unknown mode {mode!r}; valid: {list(_SCREEN_MODES)}")
-    if not store.supports(mode):
-        raise ValueError(f"store at {store.path!r} was built for modes {store.modes} and does "
-                         f"not support {mode!r}")
-    if align_kwargs.get("no_H") is False:
-        raise ValueError("screen() aligns heavy atoms only; no_H=False is not supported")
-    if mode == "vol_esp" and "lam" not in align_kwargs:
-        raise ValueError("vol_esp requires an explicit lam=...")
-    if alpha is None:
-        # vol_and_surf_esp takes alpha explicitly in the reference; 0.81 selects the heavy-atom
-        # shape centres
-        alpha = ALPHA(store.num_surf_points) if mode in _SURF_ALPHA_MODES else 0.81
-    device = torch.device(device or "cuda")
-    center = (not store.pre_centered) if do_center is None else bool(do_center)
-    qs = [_centred_query(q) if (store.pre_centered or center) else q for q in queries]
-    kw = _batch_kwargs(mode, align_kwargs, alpha)
-    so = [None] * len(qs)
-    if scores_out is not None:
-        so = [scores_out] if isinstance(scores_out, np.ndarray) and len(qs) == 1 else list(scores_out)
+def _screen_shards(qs, store: ProfileStore, mode: str, shards, kw: dict, ak: dict, alpha,
+                   top_k: int, center: bool, device, so=None, progress: bool = False):
+    """Align the (already centred) queries ``qs`` against the store shards yielded by
+    ``shards`` on ``device``; returns one _TopK per query.  ``so``: per-query full score
+    arrays to fill (or None)."""
+    so = so or [None] * len(qs)
     heaps = [_TopK(top_k) for _ in qs]
     qdev = [query_to_device(q, mode, device, alpha) for q in qs]
     # trans_init: the legacy translation-seeded starts with the query's atoms (anchors for
     # pharm) as translation centres, as the reference's per-pair screening path aligns
     # MoleculePair(query, library molecule) (screen.py:1006-1008); vol and surf ignore it there
-    trans = bool(align_kwargs.get("trans_init")) and mode not in ("vol", "surf")
+    trans = bool(ak.get("trans_init")) and mode not in ("vol", "surf")
     tks = [dict(trans_centres=_query_centres(q, mode, device),
-                num_repeats_per_trans=int(align_kwargs.get("num_repeats_per_trans", 10)),
-                topk=int(align_kwargs.get("topk", 30))) if trans else {} for q in qs]
+                num_repeats_per_trans=int(ak.get("num_repeats_per_trans", 10)),
+                topk=int(ak.get("topk", 30))) if trans else {} for q in qs]
     done = 0
-    for si in range(store.num_shards):
+    for si in shards:
         sh, arrs = store.read_shard(si)
         if center and not store.pre_centered:
             arrs = _center_shard(arrs, mode)
@@ -477,13 +450,133 @@ def screen_many(queries: Sequence, store: ProfileStore, mode: str = "surf_esp", 
             keep = top_s > heaps[qi].threshold()
             top_s, top_i = top_s[keep], top_i[keep]
             T = api.se3_from_qt(q[top_i].cpu().numpy(), t[top_i].cpu().numpy())
-            for s, i, tf in zip(top_s.cpu().tolist(), top_i.cpu().tolist(), T):
-                heaps[qi].push(float(s), _id_to_py(ids[i]), tf)
+            for s_, i, tf in zip(top_s.cpu().tolist(), top_i.cpu().tolist(), T):
+                heaps[qi].push(float(s_), _id_to_py(ids[i]), tf)
         done += K
         if progress:
             print(f"[screen] {done}/{len(store)} library molecules aligned x {len(qs)} queries",
                   flush=True)
+    return heaps
+
+
+def _screen_worker(rank, store_path, qs, mode, kw, ak, alpha, top_k, center, shard_q, out_q):
+    """One GPU of a multi-GPU screen: pulls shard indices off ``shard_q`` until a None
+    sentinel, aligns them on cuda:rank and sends its per-query top-K lists to ``out_q``."""
+    try:
+        torch.cuda.set_device(rank)
+        store = ProfileStore.open(store_path)
+
+        def shards():
+            while True:
+                idx = shard_q.get()
+                if idx is None:
+                    return
+                yield idx
+        heaps = _screen_shards(qs, store, mode, shards(), kw, ak, alpha, top_k, center,
+                               torch.device("cuda", rank))
+        torch.cuda.synchronize()
+        out_q.put((rank, [h.heap for h in heaps]))
+    except Exception:                                   # relayed to the parent
+        import traceback
+        out_q.put((rank, "__ERR__", traceback.format_exc()))
+
+
+def _screen_multi_gpu(qs, store: ProfileStore, mode, ndev, kw, ak, alpha, top_k, center):
+    """Process-per-GPU screen (the structure of the reference's _screen_many_multigpu,
+    screen.py:1237-1297): ``ndev`` spawned workers stream disjoint shards from one queue, each
+    keeps its own top-K per query, and the parent merges them."""
+    import torch.multiprocessing as mp
+    ndev = max(1, min(int(ndev), torch.cuda.device_count()))
+    ctx = mp.get_context("spawn")
+    shard_q, out_q = ctx.Queue(), ctx.Queue()
+    for idx in range(store.num_shards):
+        shard_q.put(idx)
+    for _ in range(ndev):
+        shard_q.put(None)                               # one sentinel per worker
+    procs = [ctx.Process(target=_screen_worker,
+                         args=(r, store.path, qs, mode, kw, ak, alpha, top_k, center, shard_q,
+                               out_q)) for r in range(ndev)]
+    for p in procs:
+        p.start()
+    results, errs = {}, []
+    for _ in range(ndev):
+        msg = out_q.get()
+        if len(msg) == 3 and msg[1] == "__ERR__":
+            errs.append((msg[0], msg[2]))
+        else:
+            results[msg[0]] = msg[1]
+    for p in procs:
+        p.join()
+    if errs:
+        raise RuntimeError("multi-GPU screen failed on ranks " + str([r for r, _ in errs]) +
+                           ":\n" + "\n".join(f"[rank {r}]\n{tb}" for r, tb in errs))
+    heaps = [_TopK(top_k) for _ in qs]
+    for rank in sorted(results):
+        for qi, items in enumerate(results[rank]):
+            for score, _, id_, tf in items:
+                heaps[qi].push(score, id_, tf)
+    return heaps
+
+
+def screen_many(queries: Sequence, store: ProfileStore, mode: str = "surf_esp", *,
+                backend: Optional[str] = None, do_center: Optional[bool] = None,
+                top_k: int = 1000, ndev: Optional[int] = None, scores_out=None,
+                alpha: Optional[float] = None, progress: bool = False, device=None,
+                **align_kwargs) -> List[List[Hit]]:
+    """Screen a panel of queries against ``store``; one streaming pass over its shards.
+
+    ``ndev`` > 1 spreads the shards over that many GPUs (at most the visible ones), one
+    spawned process per GPU pulling shards from a shared queue; the per-GPU top-K lists are
+    merged on the host.  ``scores_out`` needs the single-process path (ndev 1 or None), as in
+    the reference (screen.py:1114-1124)."""
+    if backend not in (None, "cuda"):
+        raise ValueError(f"backend {backend!r} is provided by shepherd_score; this package "
+                         "implements backend='cuda'")
+    multi = bool(ndev and ndev > 1)
+    if multi and scores_out is not None:
+        raise ValueError("scores_out is not supported with ndev>1 (each GPU returns only its "
+                         "per-query top-K)")
+    mode = canonical(mode)
+    if mode not in _SCREEN_MODES:
+        raise ValueError(f"unknown mode {mode!r}; valid: {list(_SCREEN_MODES)}")
+    if not store.supports(mode):
+        raise ValueError(f"store at {store.path!r} was built for modes {store.modes} and does "
+                         f"not support {mode!r}")
+    if align_kwargs.get("no_H") is False:
+        raise ValueError("screen() aligns heavy atoms only; no_H=False is not supported")
+    if mode == "vol_esp" and "lam" not in align_kwargs:
+        raise ValueError("vol_esp requires an explicit lam=...")
+    if alpha is None:
+        # vol_and_surf_esp takes alpha explicitly in the reference; 0.81 selects the heavy-atom
+        # shape centres
+        alpha = ALPHA(store.num_surf_points) if mode in _SURF_ALPHA_MODES else 0.81
+    center = (not store.pre_centered) if do_center is None else bool(do_center)
+    qs = [_centred_query(q) if (store.pre_centered or center) else q for q in queries]
+    kw = _batch_kwargs(mode, align_kwargs, alpha)
+    if multi:
+        qs = [_plain_query(q) for q in qs]
+        heaps = _screen_multi_gpu(qs, store, mode, ndev, kw, dict(align_kwargs), alpha, top_k,
+                                  center)
+        return [h.sorted() for h in heaps]
+    device = torch.device(device or "cuda")
+    so = None
+    if scores_out is not None:
+        so = [scores_out] if isinstance(scores_out, np.ndarray) and len(qs) == 1 else list(scores_out)
+    heaps = _screen_shards(qs, store, mode, range(store.num_shards), kw, align_kwargs, alpha,
+                           top_k, center, device, so, progress)
     return [h.sorted() for h in heaps]
+
+
+def _plain_query(q):
+    """The query as a dict of numpy arrays (picklable for the spawned GPU workers)."""
+    if isinstance(q, dict):
+        return {k: (None if v is None else np.asarray(v)) for k, v in q.items()}
+    names = ("atom_pos", "surf_pos", "surf_esp", "partial_charges", "pharm_types",
+             "pharm_ancs", "pharm_vecs", "radii", "centers_w_H")
+    out = {n: getattr(q, n, None) for n in names}
+    if out["centers_w_H"] is None and getattr(q, "mol", None) is not None:
+        out["centers_w_H"] = q.mol.GetConformer().GetPositions()
+    return {k: (None if v is None else np.asarray(v)) for k, v in out.items()}
 
 
 def screen(query, store: ProfileStore, mode: str = "surf_esp", **kw) -> List[Hit]:
