@@ -35,16 +35,28 @@ __device__ __forceinline__ float3 block_sum3(float3 v, float* red) {
   return s;
 }
 
-// Centroid of n packed points (block cooperative).
+// Centroid of n packed points; every thread of the block gets it.  The sum has a fixed order
+// (lane-strided partial sums of warp 0, then a butterfly), so the centroid -- and the rounding
+// of everything staged relative to it -- does not depend on the CTA size of the launch.
 __device__ __forceinline__ float3 block_centroid(const float4* __restrict__ g, int n, float* red) {
   float3 s = make_float3(0.f, 0.f, 0.f);
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const float4 p = g[i];
-    s.x += p.x; s.y += p.y; s.z += p.z;
+  if (threadIdx.x < 32) {
+    for (int i = threadIdx.x; i < n; i += 32) {
+      const float4 p = g[i];
+      s.x += p.x; s.y += p.y; s.z += p.z;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
+      s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
+      s.z += __shfl_xor_sync(0xffffffffu, s.z, o);
+    }
   }
-  s = block_sum3(s, red);
+  __syncthreads();  // earlier readers of red are done
+  if (threadIdx.x == 0) { red[0] = s.x; red[1] = s.y; red[2] = s.z; }
+  __syncthreads();
   const float inv = 1.f / (float)(n > 0 ? n : 1);
-  return make_float3(s.x * inv, s.y * inv, s.z * inv);
+  return make_float3(red[0] * inv, red[1] * inv, red[2] * inv);
 }
 
 // Stage a reference cloud (centred on c) in the expanded, duplicated form
