@@ -475,7 +475,12 @@ __device__ __forceinline__ bool shape_chunk_packed(const float4* __restrict__ sP
     cj[v] = f2(cs[0], cs[1]);
     sg[v] = f2(0.f, 0.f); sx[v] = f2(0.f, 0.f); sy[v] = f2(0.f, 0.f); sz[v] = f2(0.f, 0.f);
   }
-  if (__any_sync(0xffffffffu, big)) return false;
+  // vote of this pose's lanes only (stride = lanes per pose, a power of two <= 32): a pose's
+  // arithmetic path must not depend on the other poses that share its warp
+  const unsigned vote = __ballot_sync(0xffffffffu, big);
+  const unsigned own = stride >= 32 ? 0xffffffffu
+                                    : ((1u << stride) - 1u) << ((threadIdx.x & 31) & ~(stride - 1));
+  if (vote & own) return false;
 #pragma unroll UNR
   for (int i = 0; i < N; ++i) {
     const float4 a = sPd[2 * i], c = sPd[2 * i + 1];

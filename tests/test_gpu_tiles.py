@@ -1,6 +1,7 @@
-"""Results do not depend on the CTA size: start blocks of 2, 4 or 10 poses (1, 2 or 5 warps of
-16-lane poses) pair the same starts in each warp, and the staged frame's centroid is a
-fixed-order sum, so every start row is bit-identical across these tiles."""
+"""Results do not depend on the CTA size or on which starts share a warp: the staged frame's
+centroid is a fixed-order sum and the factored/plain exponent guard is voted by each pose's
+own lanes, so start blocks of 2, 3, 4, 8 or 10 poses (16-lane poses: 1 to 5 warps, with an
+idle half-warp in the odd blocks) give bit-identical start rows."""
 import numpy as np
 import pytest
 import torch
@@ -20,11 +21,14 @@ def test_rows_independent_of_cta_size(cuda, mode):
     fit = CloudSet.from_arrays([p for p, _ in fits], [c for _, c in fits], device=cuda)
     idx = torch.arange(16, dtype=torch.int32, device=cuda)
     sq, st = K.seeds(ref, fit, idx, idx, 50)
+    # every third start begins 11 A off, so its first steps take the unfactored exponent
+    # while its warp-mates stay factored
+    st[:, ::3] += torch.tensor([11.0, 0.0, 0.0], device=cuda)
     kw = dict(ref=ref, fit=fit, pair_ref=idx, pair_fit=idx, seed_q=sq, seed_t=st, steps=30,
               lr=0.1, lam=0.3 * al.LAM_SCALING if mode == "esp" else None, lanes_per_pose=16,
               kernel_variant=4)
     rows = [tuple(x.cpu().numpy() for x in al.align_packed(mode, chunks=c, **kw).rows)
-            for c in (25, 13, 5)]
+            for c in (25, 17, 13, 7, 5)]
     for other in rows[1:]:
         for a, b in zip(rows[0], other):
             np.testing.assert_array_equal(a, b)
