@@ -52,10 +52,15 @@ def _axis_angle_quat(v_from: np.ndarray, v_to: np.ndarray) -> np.ndarray:
     same = np.all(np.abs(v_from - v_to) <= 1e-8 + 1e-5 * np.abs(v_to), axis=1)
     cr = np.cross(v_from, v_to)
     cn = nrm(cr)
-    axis = np.where(same[:, None], np.array([1.0, 0.0, 0.0]),
-                    cr / np.where(cn > 0, cn, 1.0))
+    # antiparallel directions have no common normal (the reference's axis would be 0/0):
+    # turn half way round an axis perpendicular to v_from instead
+    perp = np.cross(v_from, np.where(np.abs(u[:, :1]) < 0.9, np.array([1.0, 0.0, 0.0]),
+                                     np.array([0.0, 1.0, 0.0])))
+    cr = np.where(cn > 0, cr, perp)
+    cn = nrm(cr)
+    axis = np.where(same[:, None], np.array([1.0, 0.0, 0.0]), cr / np.where(cn > 0, cn, 1.0))
     sq = (axis * axis).sum(1, keepdims=True)
-    axis = np.where(np.abs(1.0 - sq) > 1e-12, axis / np.sqrt(sq), axis)
+    axis = np.where(np.abs(1.0 - sq) > 1e-12, axis / np.sqrt(np.where(sq > 0, sq, 1.0)), axis)
     h = angle / 2.0
     return np.concatenate([np.cos(h)[:, None], axis * np.sin(h)[:, None]], 1)
 
@@ -137,9 +142,11 @@ def grid_padded(R: torch.Tensor, nr, Fp: torch.Tensor, nf, C: torch.Tensor, nc,
     if P and (int(nr.min()) < 1 or int(nf.min()) < 1):
         raise ValueError("translation-seeded starts need non-empty clouds")
     R, Fp = R.to(torch.float32), Fp.to(torch.float32)
-    C = C.to(torch.float32).reshape(P, -1, 3)
+    C = C.to(torch.float32).reshape(P, C.shape[-2] if C.dim() == 3 else -1, 3)
     G = 5 + per_trans * ncn
     Gm = int(G.max()) if P else 5
+    if P == 0:
+        return torch.zeros(0, Gm, 4, device=dev), torch.zeros(0, Gm, 3, device=dev), G
     com_ref = R.sum(1) / nr.to(torch.float32)[:, None]
     com_fit = Fp.sum(1) / nf.to(torch.float32)[:, None]
     q = torch.zeros(P, Gm, 4, device=dev)

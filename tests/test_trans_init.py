@@ -124,3 +124,18 @@ def test_oracle_trans_path_matches_reference(golden, tag):
     sc, _, _ = oa.align_trans(fn, args, g[f"{tag}_GQ"], g[f"{tag}_GT"], g[f"{tag}_G"], topk=30,
                               steps=30, lr=0.1, **kw)
     np.testing.assert_allclose(sc, g[f"{tag}_score"], atol=2e-3)
+
+
+def test_degenerate_clouds_give_finite_grids():
+    """One-point and collinear clouds (equal or antiparallel principal axes; the reference's
+    axis-angle step divides 0 by 0 there) still give unit quaternions and finite
+    translations, and an empty batch gives empty grids."""
+    one = np.ones((1, 3), np.float32)
+    line = np.stack([np.linspace(-2, 2, 5)] * 3, 1).astype(np.float32)
+    for ref, fit in ((one, one * 0), (line, line[::-1] * 1.5), (line, one)):
+        q, t = L.pair_grid(ref, fit, ref[:2], 10)
+        assert torch.isfinite(q).all() and torch.isfinite(t).all()
+        np.testing.assert_allclose(q.norm(dim=1).numpy(), 1.0, atol=1e-6)
+    q, t, G = L.grid_padded(torch.zeros(0, 4, 3), [], torch.zeros(0, 5, 3), [],
+                            torch.zeros(0, 2, 3), [], 10)
+    assert q.shape == (0, 5, 4) and t.shape == (0, 5, 3) and len(G) == 0
