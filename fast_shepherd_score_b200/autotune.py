@@ -1,7 +1,9 @@
 """Autotuner for the fused alignment kernel's tiling.
 
 Tunables of one launch (``fss_align_desc``):
-  lanes_per_pose  4, 8, 16 or 32 lanes cooperate on one pose (so 32/lanes starts per warp)
+  lanes_per_pose  1, 2, 4, 8, 16 or 32 lanes cooperate on one pose (so 32/lanes starts per
+                  warp; 1 and 2 are tried for small molecules: no per-step lane reduction,
+                  but few warps unless the batch is large)
   chunks          start blocks per pair (a CTA owns one pair and n_starts/chunks starts)
   cta_per_sm      persistent CTAs per SM (1 or 2; 2 hides latency, 1 leaves more L1)
   accumulate      1 = value/gradient sums on the FP32 lanes, 2 = sums on the tensor cores,
@@ -30,7 +32,7 @@ import torch
 _LOCK = threading.Lock()
 _MEM: dict = {}
 _LOADED = False
-LANES = (4, 8, 16, 32)
+LANES = (1, 2, 4, 8, 16, 32)
 
 
 def _cache_path() -> str:
@@ -87,6 +89,8 @@ def candidates(mode: str, max_fit: int, n_starts: int):
     for lpp in LANES:
         if mode != "pharm" and lpp > 4 and lpp // 2 >= max(max_fit, 1):
             continue  # more lanes than fit points: idle lanes
+        if lpp < 4 and max_fit >= 64:
+            continue  # a pose per 1-2 lanes pays off only for small molecules in large batches
         if mode == "pharm" and lpp > 8:
             continue
         for var in variants:

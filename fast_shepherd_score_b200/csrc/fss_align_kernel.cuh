@@ -302,11 +302,13 @@ template <int MODE, int VAR, int EXT = 0>
 int dispatch_lanes(int lpp, const AlignParams& prm, int threads, int cps, size_t smem,
                    cudaStream_t st) {
   switch (lpp) {
+    case 1: return launch_align<1, MODE, 0, VAR, EXT>(prm, threads, cps, smem, st);
+    case 2: return launch_align<2, MODE, 0, VAR, EXT>(prm, threads, cps, smem, st);
     case 4: return launch_align<4, MODE, 0, VAR, EXT>(prm, threads, cps, smem, st);
     case 8: return launch_align<8, MODE, 0, VAR, EXT>(prm, threads, cps, smem, st);
     case 16: return launch_align<16, MODE, 0, VAR, EXT>(prm, threads, cps, smem, st);
     case 32: return launch_align<32, MODE, 0, VAR, EXT>(prm, threads, cps, smem, st);
-    default: return set_error(FSS_ERR_INVALID, "fss_align: lanes_per_pose must be 4, 8, 16 or 32");
+    default: return set_error(FSS_ERR_INVALID, "fss_align: lanes_per_pose must be 1, 2, 4, 8, 16 or 32");
   }
 }
 

@@ -151,7 +151,7 @@ typedef struct fss_align_desc {
    * exceeding them is skipped and flagged in scratch[1]) */
   int32_t max_ref_points, max_fit_points, max_ref_features, max_fit_features;
   /* tiling: 0 = choose automatically */
-  int32_t lanes_per_pose;    /* 4, 8, 16 or 32 lanes cooperate on one pose */
+  int32_t lanes_per_pose;    /* 1, 2, 4, 8, 16 or 32 lanes cooperate on one pose */
   int32_t chunks;            /* start blocks per pair (CTA covers n_starts/chunks starts) */
   int32_t cta_per_sm;        /* persistent CTAs per SM */
   int32_t accumulate;        /* where the shape and ESP channels' pairwise work runs:

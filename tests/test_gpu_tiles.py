@@ -32,3 +32,36 @@ def test_rows_independent_of_cta_size(cuda, mode):
     for other in rows[1:]:
         for a, b in zip(rows[0], other):
             np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("mode", ["shape", "esp", "shape_pharm", "pharm"])
+def test_one_and_two_lanes_per_pose(cuda, mode):
+    """Poses on 1 or 2 lanes (no lane reduction) agree with 4-lane poses: step-1 rows (the
+    seeds' own scores) to fp32 rounding, then best scores within the alignment tolerance."""
+    from fast_shepherd_score_b200.layout import PharmSet
+    refs, fits = syn.shape_pharm_pairs(10, seed=42)
+    g = lambda ms, k: [m[k] for m in ms]
+    rng = np.random.default_rng(3)
+    ch = lambda ms: [(0.2 * rng.standard_normal(len(m["atom_pos"]))).astype(np.float32)
+                     for m in ms]
+    esp = mode == "esp"
+    ref = CloudSet.from_arrays(g(refs, "atom_pos"), ch(refs) if esp else None, device=cuda)
+    fit = CloudSet.from_arrays(g(fits, "atom_pos"), ch(fits) if esp else None, device=cuda)
+    ps = lambda ms: PharmSet.from_arrays(g(ms, "pharm_types"), g(ms, "pharm_ancs"),
+                                         g(ms, "pharm_vecs"), device=cuda)
+    idx = torch.arange(10, dtype=torch.int32, device=cuda)
+    sq, st = K.seeds(ref, fit, idx, idx, 20)
+    kw = dict(pair_ref=idx, pair_fit=idx, seed_q=sq, seed_t=st, lr=0.1,
+              lam=0.3 if esp else None)
+    if mode != "pharm":
+        kw.update(ref=ref, fit=fit)
+    if mode in ("pharm", "shape_pharm"):
+        kw.update(ref_ph=ps(refs), fit_ph=ps(fits))
+    run = lambda lpp, steps: al.align_packed(mode, steps=steps, lanes_per_pose=lpp, **kw)
+    base1 = run(4, 1).rows[0].cpu().numpy()
+    base = run(4, 40)[0].cpu().numpy()
+    for lpp in (1, 2):
+        np.testing.assert_allclose(run(lpp, 1).rows[0].cpu().numpy(), base1, rtol=2e-5,
+                                   atol=1e-6)
+        sc = run(lpp, 40)[0].cpu().numpy()
+        assert np.mean(np.abs(sc - base) <= 1e-4) >= 0.75 and np.max(base - sc) <= 1e-3
