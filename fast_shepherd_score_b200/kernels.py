@@ -202,6 +202,21 @@ def _fibo_host(n: int) -> np.ndarray:
     return np.concatenate([np.cos(half), axes * np.sin(half)], 1).astype(np.float32)
 
 
+_FIBO_DEV: dict = {}
+
+
+def _fibo_device(n: int, dev) -> torch.Tensor:
+    """The Fibonacci quaternions on `dev`, copied once per (device, n): a fresh pageable copy
+    per call would synchronise the stream with the work already queued on it."""
+    dev = torch.device(dev)
+    key = (dev.type, dev.index, n)
+    t = _FIBO_DEV.get(key)
+    if t is None:
+        t = torch.from_numpy(_fibo_host(n)).to(dev)
+        _FIBO_DEV[key] = t
+    return t
+
+
 def seeds(ref: CloudSet, fit: CloudSet, pair_ref, pair_fit, num_seeds: int):
     """(P,S,4) quaternions and (P,S,3) translations: batched_seeds_torch (_common.py:281-441)."""
     dev = ref.device
@@ -211,7 +226,7 @@ def seeds(ref: CloudSet, fit: CloudSet, pair_ref, pair_fit, num_seeds: int):
         raise ValueError("num_seeds above 64 is not supported by the seed kernel")
     n_struct = min(max(S - 5, 0), 6)
     n_fibo = max(S - 5 - n_struct, 0)
-    fibo = torch.from_numpy(_fibo_host(n_fibo)).to(dev) if n_fibo else None
+    fibo = _fibo_device(n_fibo, dev) if n_fibo else None
     sq = torch.empty(P, S, 4, dtype=_f32, device=dev)
     st = torch.empty(P, S, 3, dtype=_f32, device=dev)
     check(_lib.load().fss_seeds(ptr(ref.pts, _f32), ptr(ref.off, _i32), ptr(fit.pts, _f32),
