@@ -210,7 +210,7 @@ def run_cuda(args, wl):
     import torch.distributed as dist
     from fast_shepherd_score_b200 import _lib, api, kernels as K
     from fast_shepherd_score_b200 import align as al
-    from fast_shepherd_score_b200.layout import cost_order
+    from fast_shepherd_score_b200.layout import cost_order_device
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -229,7 +229,8 @@ def run_cuda(args, wl):
     rc, rp = ref_h.to_device(dev)
     fc, fp = fit_h.to_device(dev)
     idx = torch.arange(n_pairs, dtype=torch.int32, device=dev)
-    order = cost_order(ref_h.counts, fit_h.counts, dev)
+    cs_r, cs_f = (rc, fc) if rc is not None else (rp, fp)
+    order = cost_order_device(cs_r.off, cs_f.off, idx, idx)
     esp = mode == "surf_esp"
     kl = api._kernel_lam(mode, wl["lam"]) if esp else None
     P, S = n_pairs, wl["starts"]

@@ -32,7 +32,7 @@ import torch
 
 from . import _lib, autotune, kernels, legacy_seeds
 from ._lib import AlignDesc, check, ptr, stream_ptr
-from .layout import CloudSet, PharmSet, cost_order
+from .layout import CloudSet, PharmSet, cost_order_device
 
 _f32, _i32 = torch.float32, torch.int32
 # Tversky weights of the reference (accel/drivers/pharm.py:40)
@@ -163,12 +163,8 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
             if fit_self_ph is None:
                 fit_self_ph = kernels.pharm_self_overlap(fit_ph, directional)
     if order is None and P > 1:
-        pr = pair_ref.cpu().numpy()
-        pf = pair_fit.cpu().numpy()
-        if shape:
-            order = cost_order(ref.counts[pr], fit.counts[pf], dev)
-        else:
-            order = cost_order(ref_ph.counts[pr], fit_ph.counts[pf], dev)
+        cr, cf = (ref, fit) if shape else (ref_ph, fit_ph)
+        order = cost_order_device(cr.off, cf.off, pair_ref, pair_fit)
     tuned = (lanes_per_pose == 0 and chunks == 0 and cta_per_sm == 0 and accumulate == 0
              and kernel_variant == 0 and autotune.enabled() and P >= 64 and steps > 0)
     if tuned:

@@ -149,8 +149,11 @@ def _np(x):
     return x
 
 
-def cost_order(n_ref: np.ndarray, n_fit: np.ndarray, device) -> torch.Tensor:
-    """Pair processing order for the persistent kernel: costliest (N*M) first (LPT)."""
-    cost = np.asarray(n_ref, np.int64) * np.asarray(n_fit, np.int64)
-    order = np.argsort(-cost, kind="stable").astype(np.int32)
-    return torch.from_numpy(order).to(device)
+def cost_order_device(ref_off: torch.Tensor, fit_off: torch.Tensor, pair_ref: torch.Tensor,
+                      pair_fit: torch.Tensor) -> torch.Tensor:
+    """cost_order computed where the pairs live (no device-to-host copy, no stream sync): the
+    per-molecule counts come from the packed sets' offsets."""
+    n_ref = (ref_off[1:] - ref_off[:-1]).to(torch.int64)
+    n_fit = (fit_off[1:] - fit_off[:-1]).to(torch.int64)
+    cost = n_ref[pair_ref.long()] * n_fit[pair_fit.long()]
+    return torch.argsort(-cost, stable=True).to(torch.int32)
