@@ -65,3 +65,25 @@ def test_one_and_two_lanes_per_pose(cuda, mode):
                                    atol=1e-6)
         sc = run(lpp, 40)[0].cpu().numpy()
         assert np.mean(np.abs(sc - base) <= 1e-4) >= 0.75 and np.max(base - sc) <= 1e-3
+
+
+def test_one_and_two_lanes_per_pose_esp_combo(cuda):
+    """vol_and_surf_esp with 1 or 2 lanes per pose: step-1 rows (shape Tanimoto + ESP
+    comparison of the seed poses) agree with 16-lane poses to fp32 rounding."""
+    refs, fits = syn.esp_combo_pairs(6, seed=44)
+    g = lambda ms, k: [m[k] for m in ms]
+    cs = lambda ms, k, v=None: CloudSet.from_arrays(g(ms, k), g(ms, v) if v else None,
+                                                    device=cuda)
+    rad = lambda ms: torch.as_tensor(np.concatenate(g(ms, "radii")).astype(np.float32),
+                                     device=cuda)
+    idx = torch.arange(6, dtype=torch.int32, device=cuda)
+    ref, fit = cs(refs, "centers"), cs(fits, "centers")
+    sq, st = K.seeds(ref, fit, idx, idx, 8)
+    kw = dict(ref=ref, fit=fit, pair_ref=idx, pair_fit=idx, seed_q=sq, seed_t=st, steps=1,
+              lr=0.1, lam=0.001, ref_atoms=cs(refs, "atoms", "charges"),
+              fit_atoms=cs(fits, "atoms", "charges"), ref_radii=rad(refs), fit_radii=rad(fits),
+              ref_surf=cs(refs, "surf", "surf_esp"), fit_surf=cs(fits, "surf", "surf_esp"))
+    base = al.align_packed("esp_combo", lanes_per_pose=16, **kw).rows[0].cpu().numpy()
+    for lpp in (1, 2):
+        got = al.align_packed("esp_combo", lanes_per_pose=lpp, **kw).rows[0].cpu().numpy()
+        np.testing.assert_allclose(got, base, rtol=5e-5, atol=1e-6)
