@@ -55,8 +55,11 @@ class PackedTanimoto(torch.autograd.Function):
     def backward(ctx, g_score, g_ov):
         ref_pts, fit_pts, ref_off, fit_off, pair_ref, pair_fit, ov = ctx.saved_tensors
         max_ref, max_fit, alpha, esp, inv_lam = ctx.cfg
-        gr = torch.zeros_like(ref_pts)
-        gf = torch.zeros_like(fit_pts)
+        need_r, need_f = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
+        if not (need_r or need_f):
+            return (None,) * 11
+        gr = torch.zeros_like(ref_pts) if need_r else None
+        gf = torch.zeros_like(fit_pts) if need_f else None
         g = g_score.to(_f32).contiguous()
         check(_lib.load().fss_score_bwd(ptr(ref_pts, _f32), ptr(ref_off, _i32), ptr(fit_pts, _f32),
                                         ptr(fit_off, _i32), ptr(pair_ref, _i32),
@@ -129,17 +132,24 @@ class DenseTanimoto(torch.autograd.Function):
     def backward(ctx, g_score):
         x1, x2, q1, q2, pr, pf, ov = ctx.saved_tensors
         alpha, esp, inv_lam = ctx.cfg
-        g1, g2 = torch.zeros_like(x1), torch.zeros_like(x2)
-        gq1 = torch.zeros_like(q1) if esp else None
-        gq2 = torch.zeros_like(q2) if esp else None
+        need = ctx.needs_input_grad
+        # a side nobody differentiates (e.g. a shared target) gets no adjoint pass at all
+        side1, side2 = need[0] or (esp and need[2]), need[1] or (esp and need[3])
+        if not (side1 or side2):
+            return None, None, None, None, None, None
+        g1 = torch.zeros_like(x1) if side1 else None
+        g2 = torch.zeros_like(x2) if side2 else None
+        gq1 = torch.zeros_like(q1) if esp and side1 else None
+        gq2 = torch.zeros_like(q2) if esp and side2 else None
         g = g_score.to(_f32).contiguous()
         check(_lib.load().fss_score_bwd_dense(
             ptr(x1), ptr(q1) if esp else None, x1.shape[1], ptr(x2),
             ptr(q2) if esp else None, x2.shape[1], ptr(pr, _i32), ptr(pf, _i32),
-            int(pr.shape[0]), alpha, int(esp), inv_lam, ptr(ov), ptr(g), ptr(g1),
-            ptr(gq1) if esp else None, ptr(g2), ptr(gq2) if esp else None,
+            int(pr.shape[0]), alpha, int(esp), inv_lam, ptr(ov), ptr(g),
+            ptr(g1), ptr(gq1), ptr(g2), ptr(gq2),
             stream_ptr(x1.device)), "score_bwd_dense")
-        return g1, g2, gq1, gq2, None, None
+        return (g1 if need[0] else None, g2 if need[1] else None,
+                gq1 if esp and need[2] else None, gq2 if esp and need[3] else None, None, None)
 
 
 def _batched(c1, c2, q1=None, q2=None):

@@ -12,6 +12,7 @@
 // so coordinate gradients keep full fp32 accuracy.  One CTA per pair, both clouds staged in
 // shared memory; gradients are accumulated with atomics because a molecule may appear in
 // several pairs (a fixed target scored against many queries).
+#include <algorithm>
 #include <cmath>
 
 #include "fss_internal.cuh"
@@ -19,7 +20,15 @@
 namespace fss {
 namespace {
 
-constexpr int kScoreThreads = 128;
+constexpr int kScoreMaxThreads = 256;
+
+// Threads per pair: about two points of the larger cloud per thread (load balance of the
+// thread-strided point loops), whole warps, 64..256.
+int score_threads(int maxN, int maxM) {
+  const int half = (std::max(maxN, maxM) + 1) / 2;
+  const int t = ((half + 31) / 32) * 32;
+  return std::min(kScoreMaxThreads, std::max(64, t));
+}
 
 __device__ __forceinline__ float block_sum(float v, float* red) {
 #pragma unroll
@@ -33,36 +42,65 @@ __device__ __forceinline__ float block_sum(float v, float* red) {
   return s;
 }
 
-// sum_j g(x, y_j) for one point x against a staged cloud (value only)
+// sum_j g(x, y_j) for one point x against a staged cloud (value only).  Four independent
+// partial sums (j mod 4) keep four ex2 in flight per thread instead of one serial chain;
+// they are combined in a fixed order, so the result does not depend on the launch shape.
 template <bool ESP>
 __device__ __forceinline__ float point_sum(float4 x, const float4* __restrict__ Y, int m,
                                            float nk, float ne) {
-  float s = 0.f;
-  for (int j = 0; j < m; ++j) {
+  float s[4] = {0.f, 0.f, 0.f, 0.f};
+  int j = 0;
+  for (; j + 4 <= m; j += 4) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const float4 y = Y[j + u];
+      const float dx = x.x - y.x, dy = x.y - y.y, dz = x.z - y.z;
+      float E = nk * (dx * dx + dy * dy + dz * dz);
+      if (ESP) { const float dc = x.w - y.w; E = fmaf(ne * dc, dc, E); }
+      s[u] += ex2(E);
+    }
+  }
+  for (int u = 0; j < m; ++j, ++u) {
     const float4 y = Y[j];
     const float dx = x.x - y.x, dy = x.y - y.y, dz = x.z - y.z;
     float E = nk * (dx * dx + dy * dy + dz * dz);
     if (ESP) { const float dc = x.w - y.w; E = fmaf(ne * dc, dc, E); }
-    s += ex2(E);
+    s[u] += ex2(E);
   }
-  return s;
+  return (s[0] + s[1]) + (s[2] + s[3]);
 }
 
-// gradient pieces for one point x: sum_j g (x - y_j) and sum_j g (c_x - c_j)
+// gradient pieces for one point x: sum_j g (x - y_j) and sum_j g (c_x - c_j), with two
+// independent partial sums (j mod 2) per component
 template <bool ESP>
 __device__ __forceinline__ void point_grad(float4 x, const float4* __restrict__ Y, int m, float nk,
                                            float ne, float& gx, float& gy, float& gz, float& gc) {
-  gx = gy = gz = gc = 0.f;
-  for (int j = 0; j < m; ++j) {
+  float ax[2] = {0.f, 0.f}, ay[2] = {0.f, 0.f}, az[2] = {0.f, 0.f}, ac[2] = {0.f, 0.f};
+  int j = 0;
+  for (; j + 2 <= m; j += 2) {
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const float4 y = Y[j + u];
+      const float dx = x.x - y.x, dy = x.y - y.y, dz = x.z - y.z;
+      float E = nk * (dx * dx + dy * dy + dz * dz);
+      float dc = 0.f;
+      if (ESP) { dc = x.w - y.w; E = fmaf(ne * dc, dc, E); }
+      const float g = ex2(E);
+      ax[u] = fmaf(g, dx, ax[u]); ay[u] = fmaf(g, dy, ay[u]); az[u] = fmaf(g, dz, az[u]);
+      if (ESP) ac[u] = fmaf(g, dc, ac[u]);
+    }
+  }
+  if (j < m) {
     const float4 y = Y[j];
     const float dx = x.x - y.x, dy = x.y - y.y, dz = x.z - y.z;
     float E = nk * (dx * dx + dy * dy + dz * dz);
     float dc = 0.f;
     if (ESP) { dc = x.w - y.w; E = fmaf(ne * dc, dc, E); }
     const float g = ex2(E);
-    gx = fmaf(g, dx, gx); gy = fmaf(g, dy, gy); gz = fmaf(g, dz, gz);
-    if (ESP) gc = fmaf(g, dc, gc);
+    ax[0] = fmaf(g, dx, ax[0]); ay[0] = fmaf(g, dy, ay[0]); az[0] = fmaf(g, dz, az[0]);
+    if (ESP) ac[0] = fmaf(g, dc, ac[0]);
   }
+  gx = ax[0] + ax[1]; gy = ay[0] + ay[1]; gz = az[0] + az[1]; gc = ac[0] + ac[1];
 }
 
 // Cloud sources: packed float4 clouds with prefix offsets, or the reference's dense padded
@@ -89,9 +127,11 @@ struct DenseSrc {
 };
 
 // Gradient sinks matching the sources: float4 rows (w = d/d charge), or separate (., 3)
-// coordinate and (.) charge arrays.  Atomic: a molecule may appear in several pairs.
+// coordinate and (.) charge arrays.  Atomic: a molecule may appear in several pairs.  A null
+// sink (on() false) marks a side whose gradient is not wanted: its adjoint loop is skipped.
 struct PackedSink {
   float* g;
+  __device__ __forceinline__ bool on() const { return g != nullptr; }
   __device__ __forceinline__ void add(int k, float x, float y, float z, float c, bool esp) const {
     float* o = g + 4 * (size_t)k;
     atomicAdd(o + 0, x); atomicAdd(o + 1, y); atomicAdd(o + 2, z);
@@ -102,6 +142,7 @@ struct PackedSink {
 struct DenseSink {
   float* gxyz;
   float* gq;
+  __device__ __forceinline__ bool on() const { return gxyz != nullptr; }
   __device__ __forceinline__ void add(int k, float x, float y, float z, float c, bool esp) const {
     float* o = gxyz + 3 * (size_t)k;
     atomicAdd(o + 0, x); atomicAdd(o + 1, y); atomicAdd(o + 2, z);
@@ -110,7 +151,7 @@ struct DenseSink {
 };
 
 template <bool ESP, class Src>
-__global__ void __launch_bounds__(kScoreThreads) score_fwd_kernel(
+__global__ void __launch_bounds__(kScoreMaxThreads) score_fwd_kernel(
     const Src ref, const Src fit, const int* __restrict__ pr, const int* __restrict__ pf,
     int maxN, int maxM, float nk, float ne, float Kc, float* score, float* ov) {
   extern __shared__ __align__(16) float4 smem[];
@@ -147,7 +188,7 @@ __global__ void __launch_bounds__(kScoreThreads) score_fwd_kernel(
 }
 
 template <bool ESP, class Src, class Sink>
-__global__ void __launch_bounds__(kScoreThreads) score_bwd_kernel(
+__global__ void __launch_bounds__(kScoreMaxThreads) score_bwd_kernel(
     const Src ref, const Src fit, const int* __restrict__ pr, const int* __restrict__ pf,
     int maxN, int maxM, float nk, float ne, float aKc, float cKc, const float* __restrict__ ov,
     const float* __restrict__ gs, const Sink gref, const Sink gfit) {
@@ -168,14 +209,14 @@ __global__ void __launch_bounds__(kScoreThreads) score_bwd_kernel(
   const float dAB = g * U / (D * D);        // d loss / d V_AB
   const float dSelf = -g * vab / (D * D);   // d loss / d V_AA (= d / d V_BB)
   // d V_XY / d x = -alpha K sum g (x - y); self terms count twice
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  for (int i = gref.on() ? threadIdx.x : n; i < n; i += blockDim.x) {
     float ax, ay, az, ac, sx, sy, sz, sc;
     point_grad<ESP>(sA[i], sB, m, nk, ne, ax, ay, az, ac);
     point_grad<ESP>(sA[i], sA, n, nk, ne, sx, sy, sz, sc);
     gref.add(r0 + i, -aKc * (dAB * ax + 2.f * dSelf * sx), -aKc * (dAB * ay + 2.f * dSelf * sy),
              -aKc * (dAB * az + 2.f * dSelf * sz), -cKc * (dAB * ac + 2.f * dSelf * sc), ESP);
   }
-  for (int j = threadIdx.x; j < m; j += blockDim.x) {
+  for (int j = gfit.on() ? threadIdx.x : m; j < m; j += blockDim.x) {
     float ax, ay, az, ac, sx, sy, sz, sc;
     point_grad<ESP>(sB[j], sA, n, nk, ne, ax, ay, az, ac);
     point_grad<ESP>(sB[j], sB, m, nk, ne, sx, sy, sz, sc);
@@ -209,7 +250,8 @@ int fwd_dispatch(const Src& R, const Src& F, const int32_t* pr, const int32_t* p
   auto kern = esp ? score_fwd_kernel<true, Src> : score_fwd_kernel<false, Src>;
   cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (ce != cudaSuccess) return set_error(FSS_ERR_CUDA, std::string("fss_score_fwd: ") + cudaGetErrorString(ce));
-  kern<<<P, kScoreThreads, smem, st>>>(R, F, pr, pf, maxN, maxM, c.nk, c.ne, c.Kc, score, overlaps);
+  kern<<<P, score_threads(maxN, maxM), smem, st>>>(R, F, pr, pf, maxN, maxM, c.nk, c.ne, c.Kc,
+                                                   score, overlaps);
   return check_launch("fss_score_fwd");
 }
 
@@ -222,8 +264,8 @@ int bwd_dispatch(const Src& R, const Src& F, const int32_t* pr, const int32_t* p
   auto kern = esp ? score_bwd_kernel<true, Src, Sink> : score_bwd_kernel<false, Src, Sink>;
   cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (ce != cudaSuccess) return set_error(FSS_ERR_CUDA, std::string("fss_score_bwd: ") + cudaGetErrorString(ce));
-  kern<<<P, kScoreThreads, smem, st>>>(R, F, pr, pf, maxN, maxM, c.nk, c.ne, c.aKc, c.cKc,
-                                       overlaps, grad_score, gR, gF);
+  kern<<<P, score_threads(maxN, maxM), smem, st>>>(R, F, pr, pf, maxN, maxM, c.nk, c.ne, c.aKc,
+                                                   c.cKc, overlaps, grad_score, gR, gF);
   return check_launch("fss_score_bwd");
 }
 
@@ -257,7 +299,7 @@ int score_bwd_launch(const float* ref_pts, const int32_t* ref_off, const float* 
     return set_error(FSS_ERR_UNSUPPORTED, "fss_score_bwd: more than fss_max_points() points");
   if (P == 0) return FSS_OK;
   if (!ref_pts || !ref_off || !fit_pts || !fit_off || !pair_ref || !pair_fit || !overlaps ||
-      !grad_score || !grad_ref || !grad_fit)
+      !grad_score || (!grad_ref && !grad_fit))
     return set_error(FSS_ERR_INVALID, "fss_score_bwd: null pointer");
   const PackedSrc R{reinterpret_cast<const float4*>(ref_pts), ref_off};
   const PackedSrc F{reinterpret_cast<const float4*>(fit_pts), fit_off};
@@ -295,7 +337,7 @@ int score_bwd_dense_launch(const float* ref_xyz, const float* ref_q, int ref_n,
     return set_error(FSS_ERR_UNSUPPORTED, "fss_score_bwd_dense: more than fss_max_points() points");
   if (P == 0) return FSS_OK;
   if (!ref_xyz || !fit_xyz || !pair_ref || !pair_fit || !overlaps || !grad_score ||
-      !grad_ref_xyz || !grad_fit_xyz || (esp && (!ref_q || !fit_q)))
+      (!grad_ref_xyz && !grad_fit_xyz) || (esp && (!ref_q || !fit_q)))
     return set_error(FSS_ERR_INVALID, "fss_score_bwd_dense: null pointer");
   return bwd_dispatch(DenseSrc{ref_xyz, esp ? ref_q : nullptr, ref_n},
                       DenseSrc{fit_xyz, esp ? fit_q : nullptr, fit_n}, pair_ref, pair_fit, P,

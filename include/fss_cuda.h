@@ -227,7 +227,8 @@ int fss_pick_best(const float *row_score, const float *row_q, const float *row_t
  * clouds: score_p = V_AB / (V_AA + V_BB - V_AB).  Forward writes score (P) and the three
  * overlaps (P,3) = (V_AB, V_AA, V_BB).  Backward takes d(loss)/d(score) (P) and ADDS
  * d(loss)/d(coords) into grad_ref / grad_fit (float4 arrays aligned with the inputs,
- * w = d/d(charge); zero them first -- molecules shared by several pairs accumulate).
+ * w = d/d(charge); zero them first -- molecules shared by several pairs accumulate).  Either
+ * grad_ref or grad_fit (not both) may be NULL: that side's adjoint is then not computed.
  * esp != 0 adds the charge factor exp(-(c_i-c_j)^2 * inv_lam).  max_*_points bound the
  * molecules' sizes (a larger pair gets a NaN score and no gradient).
  * ------------------------------------------------------------------------------------- */
@@ -247,7 +248,7 @@ int fss_score_bwd(const float *ref_pts, const int32_t *ref_off, const float *fit
  * the fit side.  Same math as get_overlap / get_overlap_esp (score/gaussian_overlap.py:62-117,
  * score/electrostatic_scoring.py:17-120) without packing.  Backward ADDS d(loss)/d(coords)
  * into grad_*_xyz (same shapes as the inputs) and d(loss)/d(charges) into grad_*_q (may be
- * NULL when esp == 0). */
+ * NULL when esp == 0).  A NULL grad_ref_xyz or grad_fit_xyz (not both) skips that side. */
 int fss_score_fwd_dense(const float *ref_xyz, const float *ref_q, int32_t ref_points,
                         const float *fit_xyz, const float *fit_q, int32_t fit_points,
                         const int32_t *pair_ref, const int32_t *pair_fit, int32_t n_pairs,

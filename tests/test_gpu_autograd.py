@@ -132,3 +132,30 @@ def test_shared_target_accumulates(cuda):
                            torch.arange(3, dtype=torch.int32, device=cuda))
     s.sum().backward()
     torch.testing.assert_close(rp.grad[:, :3], g_sum, rtol=1e-5, atol=1e-7)
+
+
+@pytest.mark.parametrize("esp", [False, True])
+def test_one_sided_backward_matches_two_sided(cuda, esp):
+    """Only the side that requires grad gets an adjoint pass; its gradient is the one the
+    two-sided backward gives, and the other side's .grad stays None."""
+    rng = np.random.default_rng(8)
+    surf = syn.sphere_clouds(rng, [40] * 7)
+    X = torch.tensor(np.stack([p for p, _ in surf]), device=cuda)
+    C = torch.tensor(np.stack([c for _, c in surf]), device=cuda)
+    t, tc = X[6:7].expand(6, -1, -1), C[6:7].expand(6, -1)
+
+    def run(grad_target):
+        q, qc = X[:6].clone().requires_grad_(True), C[:6].clone().requires_grad_(True)
+        tt, ttc = t.clone().requires_grad_(grad_target), tc.clone().requires_grad_(grad_target)
+        s = (AG.get_overlap_esp(tt, q, ttc, qc, alpha=1.216, lam=0.3) if esp
+             else AG.get_overlap(tt, q, alpha=1.216))
+        s.sum().backward()
+        return s.detach(), q.grad, qc.grad, tt.grad
+
+    s1, g1, gc1, gt1 = run(False)
+    s2, g2, gc2, gt2 = run(True)
+    assert gt1 is None and gt2 is not None
+    torch.testing.assert_close(s1, s2, rtol=0, atol=0)
+    torch.testing.assert_close(g1, g2, rtol=0, atol=0)
+    if esp:
+        torch.testing.assert_close(gc1, gc2, rtol=0, atol=0)
