@@ -74,6 +74,10 @@ _SIGS = {
                              _vp, _vp, _vp], ctypes.c_int),
     "fss_score_bwd_dense": ([_vp, _vp, _i32, _vp, _vp, _i32, _vp, _vp, _i32, _f32, _i32, _f32]
                             + [_vp] * 7, ctypes.c_int),
+    "fss_score_fwd_moments_dense": ([_vp, _vp, _i32, _vp, _vp, _i32, _vp, _vp, _i32, _f32,
+                                     _i32, _f32] + [_vp] * 5, ctypes.c_int),
+    "fss_score_bwd_moments_dense": ([_vp, _vp, _i32, _i32, _i32, _f32, _i32, _f32]
+                                    + [_vp] * 9, ctypes.c_int),
     "fss_probe_peak": ([_i32, _i32, _i32, _vp, ctypes.POINTER(ctypes.c_longlong), _vp],
                        ctypes.c_int),
 }

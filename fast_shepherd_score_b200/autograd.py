@@ -13,8 +13,10 @@ torch ops that pack them.
   fixed target shared by many queries is one molecule of the ref set).
 * :func:`get_overlap`, :func:`get_overlap_esp` -- the reference's signatures for one pair
   ((N,3) vs (M,3)) or a matched batch ((B,N,3) vs (B,M,3)); :class:`DenseTanimoto` runs them
-  on the padded tensors directly (``fss_score_fwd_dense`` / ``fss_score_bwd_dense``), with no
-  packing and gradients written straight into the input shapes.
+  on the padded tensors directly, with no packing and gradients written straight into the
+  input shapes: ``fss_score_fwd_dense`` without grad, ``fss_score_fwd_moments_dense`` (value
+  plus per-point adjoint moments in one pass) and the elementwise
+  ``fss_score_bwd_moments_dense`` with grad.
 """
 from __future__ import annotations
 
@@ -106,10 +108,15 @@ def _pair_index(B, n_mol, device):
 
 class DenseTanimoto(torch.autograd.Function):
     """score_b = V_AB / (V_AA + V_BB - V_AB) for padded (B, N, 3) / (B, M, 3) batches (either
-    side may be a single molecule broadcast over the batch); optional (B, N) charges."""
+    side may be a single molecule broadcast over the batch); optional (B, N) charges.
+
+    With grad mode on, the forward also writes the adjoint moments of every side that needs a
+    gradient (``fss_score_fwd_moments_dense``), so the backward is one elementwise launch and
+    the Gaussians are evaluated once per step; a side nobody differentiates (e.g. a shared
+    target) gets no moments and no adjoint at all."""
 
     @staticmethod
-    def forward(ctx, x1, x2, q1, q2, alpha, inv_lam):
+    def forward(ctx, x1, x2, q1, q2, alpha, inv_lam, grad_on):
         esp = q1 is not None
         B = max(x1.shape[0], x2.shape[0])
         dev = x1.device
@@ -119,37 +126,42 @@ class DenseTanimoto(torch.autograd.Function):
         pr, pf = _pair_index(B, x1.shape[0], dev), _pair_index(B, x2.shape[0], dev)
         score = torch.empty(B, dtype=_f32, device=dev)
         ov = torch.empty(B, 3, dtype=_f32, device=dev)
-        check(_lib.load().fss_score_fwd_dense(
-            ptr(x1), ptr(q1) if esp else None, x1.shape[1], ptr(x2),
-            ptr(q2) if esp else None, x2.shape[1], ptr(pr, _i32), ptr(pf, _i32), B,
-            float(alpha), int(esp), float(inv_lam), ptr(score), ptr(ov), stream_ptr(dev)),
-            "score_fwd_dense")
-        ctx.save_for_backward(x1, x2, q1, q2, pr, pf, ov)
-        ctx.cfg = (float(alpha), esp, float(inv_lam))
+        need = ctx.needs_input_grad
+        side1 = bool(grad_on and (need[0] or (esp and need[2])))
+        side2 = bool(grad_on and (need[1] or (esp and need[3])))
+        lib = _lib.load()
+        args = (ptr(x1), ptr(q1), x1.shape[1], ptr(x2), ptr(q2), x2.shape[1], ptr(pr, _i32),
+                ptr(pf, _i32), B, float(alpha), int(esp), float(inv_lam), ptr(score), ptr(ov))
+        m1 = torch.empty(B, x1.shape[1], 8, dtype=_f32, device=dev) if side1 else None
+        m2 = torch.empty(B, x2.shape[1], 8, dtype=_f32, device=dev) if side2 else None
+        if side1 or side2:
+            check(lib.fss_score_fwd_moments_dense(*args, ptr(m1), ptr(m2), stream_ptr(dev)),
+                  "score_fwd_moments_dense")
+        else:
+            check(lib.fss_score_fwd_dense(*args, stream_ptr(dev)), "score_fwd_dense")
+        ctx.save_for_backward(pr, pf, ov, m1, m2)
+        ctx.cfg = (float(alpha), esp, float(inv_lam), x1.shape, x2.shape, dev)
         return score
 
     @staticmethod
     def backward(ctx, g_score):
-        x1, x2, q1, q2, pr, pf, ov = ctx.saved_tensors
-        alpha, esp, inv_lam = ctx.cfg
+        pr, pf, ov, m1, m2 = ctx.saved_tensors
+        alpha, esp, inv_lam, shape1, shape2, dev = ctx.cfg
         need = ctx.needs_input_grad
-        # a side nobody differentiates (e.g. a shared target) gets no adjoint pass at all
-        side1, side2 = need[0] or (esp and need[2]), need[1] or (esp and need[3])
-        if not (side1 or side2):
-            return None, None, None, None, None, None
-        g1 = torch.zeros_like(x1) if side1 else None
-        g2 = torch.zeros_like(x2) if side2 else None
-        gq1 = torch.zeros_like(q1) if esp and side1 else None
-        gq2 = torch.zeros_like(q2) if esp and side2 else None
+        if m1 is None and m2 is None:
+            return None, None, None, None, None, None, None
+        g1 = torch.zeros(shape1, dtype=_f32, device=dev) if m1 is not None else None
+        g2 = torch.zeros(shape2, dtype=_f32, device=dev) if m2 is not None else None
+        gq1 = torch.zeros(shape1[:2], dtype=_f32, device=dev) if esp and g1 is not None else None
+        gq2 = torch.zeros(shape2[:2], dtype=_f32, device=dev) if esp and g2 is not None else None
         g = g_score.to(_f32).contiguous()
-        check(_lib.load().fss_score_bwd_dense(
-            ptr(x1), ptr(q1) if esp else None, x1.shape[1], ptr(x2),
-            ptr(q2) if esp else None, x2.shape[1], ptr(pr, _i32), ptr(pf, _i32),
-            int(pr.shape[0]), alpha, int(esp), inv_lam, ptr(ov), ptr(g),
-            ptr(g1), ptr(gq1), ptr(g2), ptr(gq2),
-            stream_ptr(x1.device)), "score_bwd_dense")
+        check(_lib.load().fss_score_bwd_moments_dense(
+            ptr(pr, _i32), ptr(pf, _i32), int(pr.shape[0]), shape1[1], shape2[1], alpha,
+            int(esp), inv_lam, ptr(ov), ptr(g), ptr(m1), ptr(m2), ptr(g1), ptr(gq1), ptr(g2),
+            ptr(gq2), stream_ptr(dev)), "score_bwd_moments_dense")
         return (g1 if need[0] else None, g2 if need[1] else None,
-                gq1 if esp and need[2] else None, gq2 if esp and need[3] else None, None, None)
+                gq1 if esp and need[2] else None, gq2 if esp and need[3] else None,
+                None, None, None)
 
 
 def _batched(c1, c2, q1=None, q2=None):
@@ -170,7 +182,8 @@ def _score(c1, c2, q1, q2, alpha, lam):
         raise ValueError("fast_shepherd_score_b200 scores CUDA tensors only")
     if c1.shape[0] not in (1, B) or c2.shape[0] not in (1, B):
         raise ValueError("batch sizes must match or be 1")
-    s = DenseTanimoto.apply(c1, c2, q1, q2, alpha, 1.0 / float(lam) if lam is not None else 0.0)
+    s = DenseTanimoto.apply(c1, c2, q1, q2, alpha, 1.0 / float(lam) if lam is not None else 0.0,
+                            torch.is_grad_enabled())
     s = s.to(c1.dtype) if c1.dtype != _f32 else s
     return s[0] if single else s
 

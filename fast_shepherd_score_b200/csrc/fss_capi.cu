@@ -75,6 +75,18 @@ int score_bwd_dense_launch(const float* ref_xyz, const float* ref_q, int ref_n,
                            float* grad_ref_xyz, float* grad_ref_q, float* grad_fit_xyz,
                            float* grad_fit_q, cudaStream_t st);
 
+int score_fwd_mom_dense_launch(const float* ref_xyz, const float* ref_q, int ref_n,
+                               const float* fit_xyz, const float* fit_q, int fit_n,
+                               const int32_t* pair_ref, const int32_t* pair_fit, int P,
+                               float alpha, int esp, float inv_lam, float* score, float* overlaps,
+                               float* ref_mom, float* fit_mom, cudaStream_t st);
+int score_bwd_mom_dense_launch(const int32_t* pair_ref, const int32_t* pair_fit, int P,
+                               int ref_n, int fit_n, float alpha, int esp, float inv_lam,
+                               const float* overlaps, const float* grad_score,
+                               const float* ref_mom, const float* fit_mom, float* grad_ref_xyz,
+                               float* grad_ref_q, float* grad_fit_xyz, float* grad_fit_q,
+                               cudaStream_t st);
+
 int probe_launch(int which, int iters, int blocks_per_sm, float* out, long long* ops,
                  cudaStream_t st);
 int align_static_launch(const fss_align_desc* d, cudaStream_t st);
@@ -201,6 +213,31 @@ int fss_score_bwd_dense(const float* ref_xyz, const float* ref_q, int32_t ref_po
                                         pair_ref, pair_fit, n_pairs, alpha, esp, inv_lam,
                                         overlaps, grad_score, grad_ref_xyz, grad_ref_q,
                                         grad_fit_xyz, grad_fit_q, S(stream)));
+}
+
+int fss_score_fwd_moments_dense(const float* ref_xyz, const float* ref_q, int32_t ref_points,
+                                const float* fit_xyz, const float* fit_q, int32_t fit_points,
+                                const int32_t* pair_ref, const int32_t* pair_fit,
+                                int32_t n_pairs, float alpha, int32_t esp, float inv_lam,
+                                float* score, float* overlaps, float* ref_moments,
+                                float* fit_moments, void* stream) {
+  FSS_GUARD(fss::score_fwd_mom_dense_launch(ref_xyz, ref_q, ref_points, fit_xyz, fit_q,
+                                            fit_points, pair_ref, pair_fit, n_pairs, alpha, esp,
+                                            inv_lam, score, overlaps, ref_moments, fit_moments,
+                                            S(stream)));
+}
+
+int fss_score_bwd_moments_dense(const int32_t* pair_ref, const int32_t* pair_fit,
+                                int32_t n_pairs, int32_t ref_points, int32_t fit_points,
+                                float alpha, int32_t esp, float inv_lam, const float* overlaps,
+                                const float* grad_score, const float* ref_moments,
+                                const float* fit_moments, float* grad_ref_xyz,
+                                float* grad_ref_q, float* grad_fit_xyz, float* grad_fit_q,
+                                void* stream) {
+  FSS_GUARD(fss::score_bwd_mom_dense_launch(pair_ref, pair_fit, n_pairs, ref_points, fit_points,
+                                            alpha, esp, inv_lam, overlaps, grad_score,
+                                            ref_moments, fit_moments, grad_ref_xyz, grad_ref_q,
+                                            grad_fit_xyz, grad_fit_q, S(stream)));
 }
 
 int fss_probe_peak(int32_t which, int32_t iters, int32_t blocks_per_sm, float* out,

@@ -30,15 +30,21 @@ int score_threads(int maxN, int maxM) {
   return std::min(kScoreMaxThreads, std::max(64, t));
 }
 
-__device__ __forceinline__ float block_sum(float v, float* red) {
+// Block-wide sums of three values (fixed order: warp butterfly, then warps in index order).
+__device__ __forceinline__ float3 block_sum3(float a, float b, float c, float3* red) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+  }
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) red[w] = make_float3(a, b, c);
   __syncthreads();
-  if (l == 0) red[w] = v;
-  __syncthreads();
-  float s = 0.f;
-  for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += red[i];
+  float3 s = make_float3(0.f, 0.f, 0.f);
+  for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+    s.x += red[i].x; s.y += red[i].y; s.z += red[i].z;
+  }
   return s;
 }
 
@@ -70,12 +76,33 @@ __device__ __forceinline__ float point_sum(float4 x, const float4* __restrict__ 
   return (s[0] + s[1]) + (s[2] + s[3]);
 }
 
-// gradient pieces for one point x: sum_j g (x - y_j) and sum_j g (c_x - c_j), with two
-// independent partial sums (j mod 2) per component
+// Strict upper triangle of a self overlap, sum_{i<j} g(x_i, x_j), for the rows owned by
+// thread slot `t` (0..blockDim-1).  Rows are taken in balanced pairs (r, n-1-r), n-1 terms
+// per pair; the middle row of an odd cloud goes to slot n/2, which owns no pair.  The full
+// self overlap is n (the diagonal, exactly ex2(0) = 1 per point) plus twice the block total
+// of these sums.  The two clouds of a pair use slots counted from opposite ends of the block,
+// so when their n/2 row pairs fill less than the block they land on different warps.
 template <bool ESP>
-__device__ __forceinline__ void point_grad(float4 x, const float4* __restrict__ Y, int m, float nk,
-                                           float ne, float& gx, float& gy, float& gz, float& gc) {
+__device__ __forceinline__ float self_upper(const float4* __restrict__ X, int n, int t, float nk,
+                                            float ne) {
+  float s = 0.f;
+  for (int r = t; r < n / 2; r += blockDim.x)
+    s += point_sum<ESP>(X[r], X + r + 1, n - 1 - r, nk, ne) +
+         point_sum<ESP>(X[n - 1 - r], X + n - r, r, nk, ne);
+  if ((n & 1) && t == (n / 2) % blockDim.x)
+    s += point_sum<ESP>(X[n / 2], X + n / 2 + 1, n / 2, nk, ne);
+  return s;
+}
+
+// gradient pieces for one point x: sum_j g (x - y_j) and sum_j g (c_x - c_j), with two
+// independent partial sums (j mod 2) per component; returns sum_j g (callers that only need
+// the moments let the compiler drop that accumulator)
+template <bool ESP>
+__device__ __forceinline__ float point_grad(float4 x, const float4* __restrict__ Y, int m,
+                                            float nk, float ne, float& gx, float& gy, float& gz,
+                                            float& gc) {
   float ax[2] = {0.f, 0.f}, ay[2] = {0.f, 0.f}, az[2] = {0.f, 0.f}, ac[2] = {0.f, 0.f};
+  float as[2] = {0.f, 0.f};
   int j = 0;
   for (; j + 2 <= m; j += 2) {
 #pragma unroll
@@ -86,6 +113,7 @@ __device__ __forceinline__ void point_grad(float4 x, const float4* __restrict__ 
       float dc = 0.f;
       if (ESP) { dc = x.w - y.w; E = fmaf(ne * dc, dc, E); }
       const float g = ex2(E);
+      as[u] += g;
       ax[u] = fmaf(g, dx, ax[u]); ay[u] = fmaf(g, dy, ay[u]); az[u] = fmaf(g, dz, az[u]);
       if (ESP) ac[u] = fmaf(g, dc, ac[u]);
     }
@@ -97,10 +125,12 @@ __device__ __forceinline__ void point_grad(float4 x, const float4* __restrict__ 
     float dc = 0.f;
     if (ESP) { dc = x.w - y.w; E = fmaf(ne * dc, dc, E); }
     const float g = ex2(E);
+    as[0] += g;
     ax[0] = fmaf(g, dx, ax[0]); ay[0] = fmaf(g, dy, ay[0]); az[0] = fmaf(g, dz, az[0]);
     if (ESP) ac[0] = fmaf(g, dc, ac[0]);
   }
   gx = ax[0] + ax[1]; gy = ay[0] + ay[1]; gz = az[0] + az[1]; gc = ac[0] + ac[1];
+  return as[0] + as[1];
 }
 
 // Cloud sources: packed float4 clouds with prefix offsets, or the reference's dense padded
@@ -155,7 +185,7 @@ __global__ void __launch_bounds__(kScoreMaxThreads) score_fwd_kernel(
     const Src ref, const Src fit, const int* __restrict__ pr, const int* __restrict__ pf,
     int maxN, int maxM, float nk, float ne, float Kc, float* score, float* ov) {
   extern __shared__ __align__(16) float4 smem[];
-  __shared__ float red[32];
+  __shared__ float3 red[kScoreMaxThreads / 32];
   const int p = blockIdx.x;
   const int ri = pr[p], fi = pf[p];
   const int n = ref.size(ri), m = fit.size(fi);
@@ -172,15 +202,13 @@ __global__ void __launch_bounds__(kScoreMaxThreads) score_fwd_kernel(
   for (int i = threadIdx.x; i < n; i += blockDim.x) sA[i] = ref.load(r0 + i);
   for (int j = threadIdx.x; j < m; j += blockDim.x) sB[j] = fit.load(f0 + j);
   __syncthreads();
-  float ab = 0.f, aa = 0.f, bb = 0.f;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    ab += point_sum<ESP>(sA[i], sB, m, nk, ne);
-    aa += point_sum<ESP>(sA[i], sA, n, nk, ne);
-  }
-  for (int j = threadIdx.x; j < m; j += blockDim.x) bb += point_sum<ESP>(sB[j], sB, m, nk, ne);
-  ab = block_sum(ab, red) * Kc;
-  aa = block_sum(aa, red) * Kc;
-  bb = block_sum(bb, red) * Kc;
+  float ab = 0.f;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) ab += point_sum<ESP>(sA[i], sB, m, nk, ne);
+  const float3 t = block_sum3(ab, self_upper<ESP>(sA, n, threadIdx.x, nk, ne),
+                              self_upper<ESP>(sB, m, blockDim.x - 1 - threadIdx.x, nk, ne), red);
+  ab = t.x * Kc;
+  const float aa = fmaf(2.f, t.y, (float)n) * Kc;
+  const float bb = fmaf(2.f, t.z, (float)m) * Kc;
   if (threadIdx.x == 0) {
     ov[3 * p] = ab; ov[3 * p + 1] = aa; ov[3 * p + 2] = bb;
     score[p] = ab / (aa + bb - ab);
@@ -222,6 +250,94 @@ __global__ void __launch_bounds__(kScoreMaxThreads) score_bwd_kernel(
     point_grad<ESP>(sB[j], sB, m, nk, ne, sx, sy, sz, sc);
     gfit.add(f0 + j, -aKc * (dAB * ax + 2.f * dSelf * sx), -aKc * (dAB * ay + 2.f * dSelf * sy),
              -aKc * (dAB * az + 2.f * dSelf * sz), -cKc * (dAB * ac + 2.f * dSelf * sc), ESP);
+  }
+}
+
+// Forward with adjoint moments.  For a side whose moments are wanted (MR: ref, MF: fit) every
+// point k of pair p gets two float4 rows, mom[2(p*size + k)] = sum over the other cloud of
+// g (x_k - y) and mom[2(p*size + k) + 1] = the same over its own cloud (w = the charge
+// differences), computed by the same point_grad as score_bwd_kernel.  The pair's overlaps
+// come out of the same passes (V_AB from the fit rows when MF, V_XX from the full rows of a
+// side with moments, the upper triangle otherwise), so the backward is one elementwise step
+// and the Gaussians are evaluated once per step instead of twice.
+template <bool ESP, bool MR, bool MF>
+__global__ void __launch_bounds__(kScoreMaxThreads) score_fwd_mom_kernel(
+    const DenseSrc ref, const DenseSrc fit, const int* __restrict__ pr,
+    const int* __restrict__ pf, float nk, float ne, float Kc, float* score, float* ov,
+    float4* __restrict__ momR, float4* __restrict__ momF) {
+  extern __shared__ __align__(16) float4 smem[];
+  __shared__ float3 red[kScoreMaxThreads / 32];
+  const int p = blockIdx.x;
+  const int n = ref.n, m = fit.n;
+  const int r0 = ref.begin(pr[p]), f0 = fit.begin(pf[p]);
+  float4* sA = smem;
+  float4* sB = smem + n;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) sA[i] = ref.load(r0 + i);
+  for (int j = threadIdx.x; j < m; j += blockDim.x) sB[j] = fit.load(f0 + j);
+  __syncthreads();
+  float ab = 0.f, aa = 0.f, bb = 0.f;
+  if (MF) {
+    for (int j = threadIdx.x; j < m; j += blockDim.x) {
+      float4 c, o;
+      ab += point_grad<ESP>(sB[j], sA, n, nk, ne, c.x, c.y, c.z, c.w);
+      bb += point_grad<ESP>(sB[j], sB, m, nk, ne, o.x, o.y, o.z, o.w);
+      float4* d = momF + 2 * ((size_t)p * m + j);
+      d[0] = c; d[1] = o;
+    }
+  } else {
+    bb = self_upper<ESP>(sB, m, blockDim.x - 1 - threadIdx.x, nk, ne);
+  }
+  if (MR) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      float4 c, o;
+      const float x = point_grad<ESP>(sA[i], sB, m, nk, ne, c.x, c.y, c.z, c.w);
+      if (!MF) ab += x;
+      aa += point_grad<ESP>(sA[i], sA, n, nk, ne, o.x, o.y, o.z, o.w);
+      float4* d = momR + 2 * ((size_t)p * n + i);
+      d[0] = c; d[1] = o;
+    }
+  } else {
+    aa = self_upper<ESP>(sA, n, threadIdx.x, nk, ne);
+  }
+  const float3 t = block_sum3(ab, aa, bb, red);
+  const float vab = t.x * Kc;
+  const float vaa = (MR ? t.y : fmaf(2.f, t.y, (float)n)) * Kc;
+  const float vbb = (MF ? t.z : fmaf(2.f, t.z, (float)m)) * Kc;
+  if (threadIdx.x == 0) {
+    ov[3 * p] = vab; ov[3 * p + 1] = vaa; ov[3 * p + 2] = vbb;
+    score[p] = vab / (vaa + vbb - vab);
+  }
+}
+
+// Backward from the moments: one thread per (pair, point) of each side with moments; the
+// same chain rule and the same expressions as score_bwd_kernel, added atomically into the
+// molecule's row (a broadcast molecule is shared by every pair).
+__global__ void score_bwd_mom_kernel(const int* __restrict__ pr, const int* __restrict__ pf,
+                                     int P, int n, int m, float aKc, float cKc, int esp,
+                                     const float* __restrict__ ov, const float* __restrict__ gs,
+                                     const float4* __restrict__ momR,
+                                     const float4* __restrict__ momF, const DenseSink gR,
+                                     const DenseSink gF) {
+  const long long nR = momR ? (long long)P * n : 0;
+  const long long nT = nR + (momF ? (long long)P * m : 0);
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nT;
+       t += (long long)gridDim.x * blockDim.x) {
+    const bool isR = t < nR;
+    const long long u = isR ? t : t - nR;
+    const int cnt = isR ? n : m;
+    const int p = (int)(u / cnt), k = (int)(u - (long long)p * cnt);
+    const float vab = ov[3 * p], U = ov[3 * p + 1] + ov[3 * p + 2];
+    const float D = U - vab;
+    const float g = gs[p];
+    const float dAB = g * U / (D * D);
+    const float dSelf = -g * vab / (D * D);
+    const float4* mom = (isR ? momR : momF) + 2 * u;
+    const float4 c = mom[0], o = mom[1];
+    const int row = (isR ? pr[p] : pf[p]) * cnt + k;
+    (isR ? gR : gF).add(row, -aKc * (dAB * c.x + 2.f * dSelf * o.x),
+                        -aKc * (dAB * c.y + 2.f * dSelf * o.y),
+                        -aKc * (dAB * c.z + 2.f * dSelf * o.z),
+                        -cKc * (dAB * c.w + 2.f * dSelf * o.w), esp != 0);
   }
 }
 
@@ -344,6 +460,67 @@ int score_bwd_dense_launch(const float* ref_xyz, const float* ref_q, int ref_n,
                       ref_n, fit_n, alpha, esp, inv_lam, overlaps, grad_score,
                       DenseSink{grad_ref_xyz, grad_ref_q}, DenseSink{grad_fit_xyz, grad_fit_q},
                       st);
+}
+
+
+int score_fwd_mom_dense_launch(const float* ref_xyz, const float* ref_q, int ref_n,
+                               const float* fit_xyz, const float* fit_q, int fit_n,
+                               const int32_t* pair_ref, const int32_t* pair_fit, int P,
+                               float alpha, int esp, float inv_lam, float* score, float* overlaps,
+                               float* ref_mom, float* fit_mom, cudaStream_t st) {
+  if (P < 0 || ref_n < 0 || fit_n < 0 || !(alpha > 0.f))
+    return set_error(FSS_ERR_INVALID, "fss_score_fwd_moments_dense: bad sizes or alpha");
+  if (ref_n > kMaxPoints || fit_n > kMaxPoints)
+    return set_error(FSS_ERR_UNSUPPORTED,
+                     "fss_score_fwd_moments_dense: more than fss_max_points() points");
+  if (P == 0) return FSS_OK;
+  if (!ref_xyz || !fit_xyz || !pair_ref || !pair_fit || !score || !overlaps ||
+      (!ref_mom && !fit_mom) || (esp && (!ref_q || !fit_q)))
+    return set_error(FSS_ERR_INVALID, "fss_score_fwd_moments_dense: null pointer");
+  const ScoreConsts c = score_consts(alpha, esp, inv_lam);
+  const size_t smem = sizeof(float4) * ((size_t)ref_n + fit_n) + 16;
+  using K = void (*)(const DenseSrc, const DenseSrc, const int*, const int*, float, float, float,
+                     float*, float*, float4*, float4*);
+  const K table[2][3] = {
+      {score_fwd_mom_kernel<false, true, false>, score_fwd_mom_kernel<false, false, true>,
+       score_fwd_mom_kernel<false, true, true>},
+      {score_fwd_mom_kernel<true, true, false>, score_fwd_mom_kernel<true, false, true>,
+       score_fwd_mom_kernel<true, true, true>}};
+  const K kern = table[esp ? 1 : 0][ref_mom ? (fit_mom ? 2 : 0) : 1];
+  cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (ce != cudaSuccess)
+    return set_error(FSS_ERR_CUDA, std::string("fss_score_fwd_moments_dense: ") + cudaGetErrorString(ce));
+  kern<<<P, score_threads(ref_n, fit_n), smem, st>>>(
+      DenseSrc{ref_xyz, esp ? ref_q : nullptr, ref_n}, DenseSrc{fit_xyz, esp ? fit_q : nullptr, fit_n},
+      pair_ref, pair_fit, c.nk, c.ne, c.Kc, score, overlaps, reinterpret_cast<float4*>(ref_mom),
+      reinterpret_cast<float4*>(fit_mom));
+  return check_launch("fss_score_fwd_moments_dense");
+}
+
+int score_bwd_mom_dense_launch(const int32_t* pair_ref, const int32_t* pair_fit, int P,
+                               int ref_n, int fit_n, float alpha, int esp, float inv_lam,
+                               const float* overlaps, const float* grad_score,
+                               const float* ref_mom, const float* fit_mom, float* grad_ref_xyz,
+                               float* grad_ref_q, float* grad_fit_xyz, float* grad_fit_q,
+                               cudaStream_t st) {
+  if (P < 0 || ref_n < 0 || fit_n < 0 || !(alpha > 0.f))
+    return set_error(FSS_ERR_INVALID, "fss_score_bwd_moments_dense: bad sizes or alpha");
+  if (P == 0) return FSS_OK;
+  // a side takes part when both its moments and its gradient are given
+  if (!grad_ref_xyz) ref_mom = nullptr;
+  if (!grad_fit_xyz) fit_mom = nullptr;
+  if (!pair_ref || !pair_fit || !overlaps || !grad_score || (!ref_mom && !fit_mom))
+    return set_error(FSS_ERR_INVALID, "fss_score_bwd_moments_dense: null pointer");
+  const ScoreConsts c = score_consts(alpha, esp, inv_lam);
+  const long long total = (ref_mom ? (long long)P * ref_n : 0) + (fit_mom ? (long long)P * fit_n : 0);
+  if (total == 0) return FSS_OK;
+  const long long want = (total + 255) / 256;
+  const int grid = (int)std::min<long long>(want, (long long)num_sms() * 8);
+  score_bwd_mom_kernel<<<grid, 256, 0, st>>>(
+      pair_ref, pair_fit, P, ref_n, fit_n, c.aKc, c.cKc, esp, overlaps, grad_score,
+      reinterpret_cast<const float4*>(ref_mom), reinterpret_cast<const float4*>(fit_mom),
+      DenseSink{grad_ref_xyz, grad_ref_q}, DenseSink{grad_fit_xyz, grad_fit_q});
+  return check_launch("fss_score_bwd_moments_dense");
 }
 
 }  // namespace fss

@@ -261,6 +261,34 @@ int fss_score_bwd_dense(const float *ref_xyz, const float *ref_q, int32_t ref_po
                         const float *grad_score, float *grad_ref_xyz, float *grad_ref_q,
                         float *grad_fit_xyz, float *grad_fit_q, void *stream);
 
+/* Forward with adjoint moments (no counterpart in the reference, which differentiates
+ * get_overlap / get_overlap_esp by torch autograd): as fss_score_fwd_dense, and in the same
+ * pass, for each side whose moments pointer is non-NULL (at least one), writes per pair p and
+ * point k of that side two float4 rows (x, y, z, charge):
+ *   moments[8 (p * points + k) + 0..3] = sum over the other cloud's points y of g (x_k - y)
+ *   moments[8 (p * points + k) + 4..7] = sum over the own cloud's points y of g (x_k - y)
+ * (charge component g (c_k - c_y)); ref_moments is (n_pairs, ref_points, 8) floats,
+ * fit_moments (n_pairs, fit_points, 8).  fss_score_bwd_moments_dense then turns them into the
+ * gradients without a second pass over the pairs.  The overlaps may differ from
+ * fss_score_fwd_dense's in the last bits (other summation order). */
+int fss_score_fwd_moments_dense(const float *ref_xyz, const float *ref_q, int32_t ref_points,
+                                const float *fit_xyz, const float *fit_q, int32_t fit_points,
+                                const int32_t *pair_ref, const int32_t *pair_fit,
+                                int32_t n_pairs, float alpha, int32_t esp, float inv_lam,
+                                float *score, float *overlaps, float *ref_moments,
+                                float *fit_moments, void *stream);
+/* ADDS into grad_* what fss_score_bwd_dense adds, from the forward's overlaps and moments, for
+ * each side whose moments and grad_*_xyz are both non-NULL (grad_*_q may be NULL when
+ * esp == 0).  Same expressions as fss_score_bwd_dense, so equal moments and overlaps give
+ * bit-identical gradients. */
+int fss_score_bwd_moments_dense(const int32_t *pair_ref, const int32_t *pair_fit,
+                                int32_t n_pairs, int32_t ref_points, int32_t fit_points,
+                                float alpha, int32_t esp, float inv_lam, const float *overlaps,
+                                const float *grad_score, const float *ref_moments,
+                                const float *fit_moments, float *grad_ref_xyz,
+                                float *grad_ref_q, float *grad_fit_xyz, float *grad_fit_q,
+                                void *stream);
+
 /* ---------------------------------------------------------------------------------------
  * Roof probe (measurement support, no reference counterpart): launches a throughput kernel
  * of `which` = 0 (ex2 on the MUFU pipe) or 1 (FP32 FMA) with `blocks_per_sm` CTAs of 256
