@@ -21,6 +21,10 @@ namespace fss {
 namespace {
 
 constexpr int kScoreMaxThreads = 256;
+// The moments kernel: at most 5 warps per CTA and <= 56 registers, so 7 CTAs (one pair
+// each) stay resident per SM -- 1036 pairs per wave on 148 SMs.
+constexpr int kMomMaxThreads = 160;
+constexpr int kMomMinBlocks = 7;
 
 // Threads per pair: about two points of the larger cloud per thread (load balance of the
 // thread-strided point loops), whole warps, 64..256.
@@ -31,6 +35,14 @@ int score_threads(int maxN, int maxM) {
 }
 
 // Block-wide sums of three values (fixed order: warp butterfly, then warps in index order).
+// Threads per pair of the moments kernel: its rows go two to a thread (f32x2 lanes), so about
+// one thread per two points of the larger cloud, whole warps, 64..kMomMaxThreads.
+int mom_threads(int maxN, int maxM) {
+  const int half = (std::max(maxN, maxM) + 1) / 2;
+  const int t = ((half + 31) / 32) * 32;
+  return std::min(kMomMaxThreads, std::max(64, t));
+}
+
 __device__ __forceinline__ float3 block_sum3(float a, float b, float c, float3* red) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -253,51 +265,136 @@ __global__ void __launch_bounds__(kScoreMaxThreads) score_bwd_kernel(
   }
 }
 
+// Negated, duplicated staging of a cloud for the packed rows below: point k occupies two
+// float4, (-x, -x, -y, -y) and (-z, -z, -c', -c') with c' = c * cs, so one 16-byte shared
+// load yields the f32x2 operands "minus this point" for two rows at once.
+__device__ __forceinline__ void stage_neg2(float4* __restrict__ d, float4 p, float cs) {
+  const float c = p.w * cs;
+  d[0] = make_float4(-p.x, -p.x, -p.y, -p.y);
+  d[1] = make_float4(-p.z, -p.z, -c, -c);
+}
+
+// Adjoint moments of two rows at once (f32x2 lanes: lane x = row 0, lane y = row 1) against
+// a cloud staged by stage_neg2: returns sum_k g per lane and sets (mx, my, mz, mc) =
+// sum_k g (x - o_k, ..., c' - o_k').  The charges are pre-scaled by cs = sqrt(ne / nk), so
+// the exponent nk (|x - o|^2 + (c' - o')^2) equals nk |x - o|^2 + ne (c - o_c)^2 with one
+// packed FFMA for the charge term instead of a multiply and an FFMA; the packed FADD2 /
+// FMUL2 / FFMA2 instructions cut the kernel's issued instructions by a quarter against
+// point_grad's scalar loop (the FMA sub-pipes still execute every lane-op: a packed op
+// occupies both halves of the pipe, so the FP32 pipe cycles per term do not change).  One
+// running sum per lane (the two lanes already give each instruction two independent terms,
+// and a second partial sum would push the kernel past 56 registers).
+template <bool ESP>
+__device__ __forceinline__ float2 rows2_grad(float2 X, float2 Y, float2 Z, float2 C,
+                                             const float4* __restrict__ O, int cnt, float2 nk2,
+                                             float2& mx, float2& my, float2& mz, float2& mc) {
+  const float2 z2 = make_float2(0.f, 0.f);
+  float2 s = z2, ax = z2, ay = z2, az = z2, ac = z2;
+#pragma unroll 4
+  for (int k = 0; k < cnt; ++k) {
+    const float4 a = O[2 * k], b = O[2 * k + 1];
+    const float2 dx = __fadd2_rn(X, make_float2(a.x, a.y));
+    const float2 dy = __fadd2_rn(Y, make_float2(a.z, a.w));
+    const float2 dz = __fadd2_rn(Z, make_float2(b.x, b.y));
+    float2 d2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+    float2 dc = z2;
+    if (ESP) {
+      dc = __fadd2_rn(C, make_float2(b.z, b.w));
+      d2 = __ffma2_rn(dc, dc, d2);
+    }
+    const float2 E = __fmul2_rn(d2, nk2);
+    const float2 g = make_float2(ex2(E.x), ex2(E.y));
+    s = __fadd2_rn(s, g);
+    ax = __ffma2_rn(g, dx, ax);
+    ay = __ffma2_rn(g, dy, ay);
+    az = __ffma2_rn(g, dz, az);
+    if (ESP) ac = __ffma2_rn(g, dc, ac);
+  }
+  mx = ax; my = ay; mz = az; mc = ac;
+  return s;
+}
+
+// Rows of one cloud X (plain staging) with moments against the other cloud and itself (both
+// staged by stage_neg2), two rows per thread: row t and row t + ceil(cnt/2) (the second lane
+// repeats row t, and is discarded, for the middle row of an odd cloud).  Adds the rows'
+// cross and self Gaussian sums to *cross / *self and writes the moment rows of pair p.
+template <bool ESP>
+__device__ __forceinline__ void moment_rows(const float4* __restrict__ X, int cnt,
+                                            const float4* __restrict__ Oother, int n_other,
+                                            const float4* __restrict__ Oself, float cs, float ics,
+                                            float2 nk2, float4* __restrict__ mom, float& cross,
+                                            float& self) {
+  const int h = (cnt + 1) / 2;
+  for (int t = threadIdx.x; t < h; t += blockDim.x) {
+    const int r0 = t, r1 = t + h < cnt ? t + h : t;
+    const float4 p0 = X[r0], p1 = X[r1];
+    const float2 px = make_float2(p0.x, p1.x), py = make_float2(p0.y, p1.y),
+                 pz = make_float2(p0.z, p1.z), pc = make_float2(p0.w * cs, p1.w * cs);
+    float2 mx, my, mz, mc;
+    // cross rows first, stored before the self rows so their moments hold no registers
+    const float2 sc = rows2_grad<ESP>(px, py, pz, pc, Oother, n_other, nk2, mx, my, mz, mc);
+    cross += sc.x;
+    mom[2 * r0] = make_float4(mx.x, my.x, mz.x, mc.x * ics);
+    if (r1 != r0) {
+      cross += sc.y;
+      mom[2 * r1] = make_float4(mx.y, my.y, mz.y, mc.y * ics);
+    }
+    const float2 ss = rows2_grad<ESP>(px, py, pz, pc, Oself, cnt, nk2, mx, my, mz, mc);
+    self += ss.x;
+    mom[2 * r0 + 1] = make_float4(mx.x, my.x, mz.x, mc.x * ics);
+    if (r1 != r0) {
+      self += ss.y;
+      mom[2 * r1 + 1] = make_float4(mx.y, my.y, mz.y, mc.y * ics);
+    }
+  }
+}
+
 // Forward with adjoint moments.  For a side whose moments are wanted (MR: ref, MF: fit) every
 // point k of pair p gets two float4 rows, mom[2(p*size + k)] = sum over the other cloud of
 // g (x_k - y) and mom[2(p*size + k) + 1] = the same over its own cloud (w = the charge
-// differences), computed by the same point_grad as score_bwd_kernel.  The pair's overlaps
-// come out of the same passes (V_AB from the fit rows when MF, V_XX from the full rows of a
-// side with moments, the upper triangle otherwise), so the backward is one elementwise step
-// and the Gaussians are evaluated once per step instead of twice.
+// differences).  The pair's overlaps come out of the same passes (V_AB from the fit rows when
+// MF, V_XX from the full rows of a side with moments, the upper triangle otherwise), so the
+// backward is one elementwise step and the Gaussians are evaluated once per step instead of
+// twice.  Shared memory: both clouds plain (n + m float4) and negated/duplicated (2(n + m)).
 template <bool ESP, bool MR, bool MF>
-__global__ void __launch_bounds__(kScoreMaxThreads) score_fwd_mom_kernel(
+__global__ void __launch_bounds__(kMomMaxThreads, kMomMinBlocks) score_fwd_mom_kernel(
     const DenseSrc ref, const DenseSrc fit, const int* __restrict__ pr,
-    const int* __restrict__ pf, float nk, float ne, float Kc, float* score, float* ov,
-    float4* __restrict__ momR, float4* __restrict__ momF) {
+    const int* __restrict__ pf, float nk, float ne, float Kc, float cs, float ics, float* score,
+    float* ov, float4* __restrict__ momR, float4* __restrict__ momF) {
   extern __shared__ __align__(16) float4 smem[];
   __shared__ float3 red[kScoreMaxThreads / 32];
   const int p = blockIdx.x;
   const int n = ref.n, m = fit.n;
   const int r0 = ref.begin(pr[p]), f0 = fit.begin(pf[p]);
   float4* sA = smem;
-  float4* sB = smem + n;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) sA[i] = ref.load(r0 + i);
-  for (int j = threadIdx.x; j < m; j += blockDim.x) sB[j] = fit.load(f0 + j);
+  float4* sB = sA + n;
+  float4* dA = sB + m;
+  float4* dB = dA + 2 * n;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const float4 v = ref.load(r0 + i);
+    sA[i] = v;
+    stage_neg2(dA + 2 * i, v, cs);
+  }
+  for (int j = threadIdx.x; j < m; j += blockDim.x) {
+    const float4 v = fit.load(f0 + j);
+    sB[j] = v;
+    stage_neg2(dB + 2 * j, v, cs);
+  }
   __syncthreads();
+  const float2 nk2 = make_float2(nk, nk);
   float ab = 0.f, aa = 0.f, bb = 0.f;
   if (MF) {
-    for (int j = threadIdx.x; j < m; j += blockDim.x) {
-      float4 c, o;
-      ab += point_grad<ESP>(sB[j], sA, n, nk, ne, c.x, c.y, c.z, c.w);
-      bb += point_grad<ESP>(sB[j], sB, m, nk, ne, o.x, o.y, o.z, o.w);
-      float4* d = momF + 2 * ((size_t)p * m + j);
-      d[0] = c; d[1] = o;
-    }
+    moment_rows<ESP>(sB, m, dA, n, dB, cs, ics, nk2, momF + 2 * (size_t)p * m, ab, bb);
   } else {
     bb = self_upper<ESP>(sB, m, blockDim.x - 1 - threadIdx.x, nk, ne);
   }
   if (MR) {
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      float4 c, o;
-      const float x = point_grad<ESP>(sA[i], sB, m, nk, ne, c.x, c.y, c.z, c.w);
-      if (!MF) ab += x;
-      aa += point_grad<ESP>(sA[i], sA, n, nk, ne, o.x, o.y, o.z, o.w);
-      float4* d = momR + 2 * ((size_t)p * n + i);
-      d[0] = c; d[1] = o;
-    }
+    float abr = 0.f;
+    moment_rows<ESP>(sA, n, dB, m, dA, cs, ics, nk2, momR + 2 * (size_t)p * n, abr, aa);
+    if (!MF) ab = abr;
   } else {
-    aa = self_upper<ESP>(sA, n, threadIdx.x, nk, ne);
+    // counted from the far end of the block: the fit rows fill it from thread 0
+    aa = self_upper<ESP>(sA, n, blockDim.x - 1 - threadIdx.x, nk, ne);
   }
   const float3 t = block_sum3(ab, aa, bb, red);
   const float vab = t.x * Kc;
@@ -334,10 +431,10 @@ __global__ void score_bwd_mom_kernel(const int* __restrict__ pr, const int* __re
     const float4* mom = (isR ? momR : momF) + 2 * u;
     const float4 c = mom[0], o = mom[1];
     const int row = (isR ? pr[p] : pf[p]) * cnt + k;
-    (isR ? gR : gF).add(row, -aKc * (dAB * c.x + 2.f * dSelf * o.x),
-                        -aKc * (dAB * c.y + 2.f * dSelf * o.y),
-                        -aKc * (dAB * c.z + 2.f * dSelf * o.z),
-                        -cKc * (dAB * c.w + 2.f * dSelf * o.w), esp != 0);
+    const DenseSink sink{isR ? gR.gxyz : gF.gxyz, isR ? gR.gq : gF.gq};
+    sink.add(row, -aKc * (dAB * c.x + 2.f * dSelf * o.x),
+             -aKc * (dAB * c.y + 2.f * dSelf * o.y), -aKc * (dAB * c.z + 2.f * dSelf * o.z),
+             -cKc * (dAB * c.w + 2.f * dSelf * o.w), esp != 0);
   }
 }
 
@@ -478,9 +575,13 @@ int score_fwd_mom_dense_launch(const float* ref_xyz, const float* ref_q, int ref
       (!ref_mom && !fit_mom) || (esp && (!ref_q || !fit_q)))
     return set_error(FSS_ERR_INVALID, "fss_score_fwd_moments_dense: null pointer");
   const ScoreConsts c = score_consts(alpha, esp, inv_lam);
-  const size_t smem = sizeof(float4) * ((size_t)ref_n + fit_n) + 16;
+  // plain + negated/duplicated staging of both clouds
+  const size_t smem = 3 * sizeof(float4) * ((size_t)ref_n + fit_n) + 16;
+  // charge pre-scale sqrt(ne / nk) of the packed rows and its inverse for the moments
+  const double cs = (esp && c.ne < 0.f) ? std::sqrt((double)c.ne / (double)c.nk) : 0.0;
+  const float csf = (float)cs, icsf = cs > 0.0 ? (float)(1.0 / cs) : 0.f;
   using K = void (*)(const DenseSrc, const DenseSrc, const int*, const int*, float, float, float,
-                     float*, float*, float4*, float4*);
+                     float, float, float*, float*, float4*, float4*);
   const K table[2][3] = {
       {score_fwd_mom_kernel<false, true, false>, score_fwd_mom_kernel<false, false, true>,
        score_fwd_mom_kernel<false, true, true>},
@@ -488,11 +589,16 @@ int score_fwd_mom_dense_launch(const float* ref_xyz, const float* ref_q, int ref
        score_fwd_mom_kernel<true, true, true>}};
   const K kern = table[esp ? 1 : 0][ref_mom ? (fit_mom ? 2 : 0) : 1];
   cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // all of the unified L1 as shared memory: 7 CTAs of ~30 KB (300 + 300 points) per SM
+  if (ce == cudaSuccess)
+    ce = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                              (int)cudaSharedmemCarveoutMaxShared);
   if (ce != cudaSuccess)
     return set_error(FSS_ERR_CUDA, std::string("fss_score_fwd_moments_dense: ") + cudaGetErrorString(ce));
-  kern<<<P, score_threads(ref_n, fit_n), smem, st>>>(
+  kern<<<P, mom_threads(ref_n, fit_n), smem, st>>>(
       DenseSrc{ref_xyz, esp ? ref_q : nullptr, ref_n}, DenseSrc{fit_xyz, esp ? fit_q : nullptr, fit_n},
-      pair_ref, pair_fit, c.nk, c.ne, c.Kc, score, overlaps, reinterpret_cast<float4*>(ref_mom),
+      pair_ref, pair_fit, c.nk, c.ne, c.Kc, csf, icsf, score, overlaps,
+      reinterpret_cast<float4*>(ref_mom),
       reinterpret_cast<float4*>(fit_mom));
   return check_launch("fss_score_fwd_moments_dense");
 }

@@ -158,21 +158,22 @@ def test_one_sided_backward_matches_two_sided(cuda, esp, query_side):
     s1, g1, gc1, gt1 = run(False)
     s2, g2, gc2, gt2 = run(True)
     assert gt1 is None and gt2 is not None
-    torch.testing.assert_close(s1, s2, rtol=2e-6, atol=0)
+    torch.testing.assert_close(s1, s2, rtol=5e-6, atol=0)
     torch.testing.assert_close(g1, g2, rtol=2e-5, atol=1e-7)
     if esp:
         torch.testing.assert_close(gc1, gc2, rtol=2e-5, atol=1e-7)
     with torch.no_grad():
         s0 = (AG.get_overlap_esp(X[:6], t, C[:6], tc, alpha=1.216, lam=0.3) if esp
               else AG.get_overlap(X[:6], t, alpha=1.216))
-    torch.testing.assert_close(s0, s1, rtol=2e-6, atol=0)
+    torch.testing.assert_close(s0, s1, rtol=5e-6, atol=0)
 
 
 @pytest.mark.parametrize("esp", [0, 1])
 def test_moment_backward_matches_two_pass_backward(cuda, esp):
     """fss_score_fwd_moments_dense + fss_score_bwd_moments_dense against fss_score_fwd_dense
     + fss_score_bwd_dense on the same batch (odd cloud sizes, a broadcast target): overlaps
-    to fp32 rounding, gradients of both sides to 1e-6 relative."""
+    and gradients of both sides to fp32 rounding (the moments kernel evaluates the exponent
+    with pre-scaled charges and packed f32x2 arithmetic, so the last bits differ)."""
     from fast_shepherd_score_b200 import _lib
     from fast_shepherd_score_b200._lib import ptr, stream_ptr
     rng = np.random.default_rng(9)
@@ -209,10 +210,11 @@ def test_moment_backward_matches_two_pass_backward(cuda, esp):
                                            ptr(ova), ptr(gs), ptr(m1), ptr(m2),
                                            *(ptr(t) for t in gb), st) == 0
     torch.cuda.synchronize(cuda)
-    torch.testing.assert_close(ovb, ova, rtol=2e-6, atol=0)
-    torch.testing.assert_close(sb, sa, rtol=2e-6, atol=0)
+    torch.testing.assert_close(ovb, ova, rtol=5e-6, atol=0)
+    torch.testing.assert_close(sb, sa, rtol=5e-6, atol=0)
     for a, b in zip(ga, gb):
-        torch.testing.assert_close(b, a, rtol=1e-6, atol=1e-7)
+        scale = a.abs().max().item()
+        torch.testing.assert_close(b, a, rtol=1e-5, atol=1e-6 * scale)
 
 
 def test_graph_captured_step_matches_eager(cuda):
