@@ -113,7 +113,9 @@ class DenseTanimoto(torch.autograd.Function):
     With grad mode on, the forward also writes the adjoint moments of every side that needs a
     gradient (``fss_score_fwd_moments_dense``), so the backward is one elementwise launch and
     the Gaussians are evaluated once per step; a side nobody differentiates (e.g. a shared
-    target) gets no moments and no adjoint at all."""
+    target) gets no moments and no adjoint at all.  Clouds too large for the moments kernel's
+    shared-memory staging (about 4700 points together) keep the inputs and take the two-pass
+    adjoint (``fss_score_fwd_dense`` + ``fss_score_bwd_dense``)."""
 
     @staticmethod
     def forward(ctx, x1, x2, q1, q2, alpha, inv_lam, grad_on):
@@ -132,33 +134,46 @@ class DenseTanimoto(torch.autograd.Function):
         lib = _lib.load()
         args = (ptr(x1), ptr(q1), x1.shape[1], ptr(x2), ptr(q2), x2.shape[1], ptr(pr, _i32),
                 ptr(pf, _i32), B, float(alpha), int(esp), float(inv_lam), ptr(score), ptr(ov))
-        m1 = torch.empty(B, x1.shape[1], 8, dtype=_f32, device=dev) if side1 else None
-        m2 = torch.empty(B, x2.shape[1], 8, dtype=_f32, device=dev) if side2 else None
+        m1 = m2 = None
         if side1 or side2:
-            check(lib.fss_score_fwd_moments_dense(*args, ptr(m1), ptr(m2), stream_ptr(dev)),
-                  "score_fwd_moments_dense")
-        else:
+            m1 = torch.empty(B, x1.shape[1], 8, dtype=_f32, device=dev) if side1 else None
+            m2 = torch.empty(B, x2.shape[1], 8, dtype=_f32, device=dev) if side2 else None
+            rc = lib.fss_score_fwd_moments_dense(*args, ptr(m1), ptr(m2), stream_ptr(dev))
+            if rc == _lib.FSS_ERR_UNSUPPORTED:
+                m1 = m2 = None   # clouds too large to stage: the two-pass adjoint below
+            else:
+                check(rc, "score_fwd_moments_dense")
+        if m1 is None and m2 is None:
             check(lib.fss_score_fwd_dense(*args, stream_ptr(dev)), "score_fwd_dense")
-        ctx.save_for_backward(pr, pf, ov, m1, m2)
-        ctx.cfg = (float(alpha), esp, float(inv_lam), x1.shape, x2.shape, dev)
+        two_pass = (side1 or side2) and m1 is None and m2 is None
+        keep = (x1, x2, q1, q2) if two_pass else (None, None, None, None)
+        ctx.save_for_backward(pr, pf, ov, m1, m2, *keep)
+        ctx.cfg = (float(alpha), esp, float(inv_lam), x1.shape, x2.shape, dev, side1, side2)
         return score
 
     @staticmethod
     def backward(ctx, g_score):
-        pr, pf, ov, m1, m2 = ctx.saved_tensors
-        alpha, esp, inv_lam, shape1, shape2, dev = ctx.cfg
+        pr, pf, ov, m1, m2, x1, x2, q1, q2 = ctx.saved_tensors
+        alpha, esp, inv_lam, shape1, shape2, dev, side1, side2 = ctx.cfg
         need = ctx.needs_input_grad
-        if m1 is None and m2 is None:
+        if not (side1 or side2):
             return None, None, None, None, None, None, None
-        g1 = torch.zeros(shape1, dtype=_f32, device=dev) if m1 is not None else None
-        g2 = torch.zeros(shape2, dtype=_f32, device=dev) if m2 is not None else None
-        gq1 = torch.zeros(shape1[:2], dtype=_f32, device=dev) if esp and g1 is not None else None
-        gq2 = torch.zeros(shape2[:2], dtype=_f32, device=dev) if esp and g2 is not None else None
+        g1 = torch.zeros(shape1, dtype=_f32, device=dev) if side1 else None
+        g2 = torch.zeros(shape2, dtype=_f32, device=dev) if side2 else None
+        gq1 = torch.zeros(shape1[:2], dtype=_f32, device=dev) if esp and side1 else None
+        gq2 = torch.zeros(shape2[:2], dtype=_f32, device=dev) if esp and side2 else None
         g = g_score.to(_f32).contiguous()
-        check(_lib.load().fss_score_bwd_moments_dense(
-            ptr(pr, _i32), ptr(pf, _i32), int(pr.shape[0]), shape1[1], shape2[1], alpha,
-            int(esp), inv_lam, ptr(ov), ptr(g), ptr(m1), ptr(m2), ptr(g1), ptr(gq1), ptr(g2),
-            ptr(gq2), stream_ptr(dev)), "score_bwd_moments_dense")
+        lib = _lib.load()
+        if m1 is not None or m2 is not None:
+            check(lib.fss_score_bwd_moments_dense(
+                ptr(pr, _i32), ptr(pf, _i32), int(pr.shape[0]), shape1[1], shape2[1], alpha,
+                int(esp), inv_lam, ptr(ov), ptr(g), ptr(m1), ptr(m2), ptr(g1), ptr(gq1),
+                ptr(g2), ptr(gq2), stream_ptr(dev)), "score_bwd_moments_dense")
+        else:
+            check(lib.fss_score_bwd_dense(
+                ptr(x1), ptr(q1), shape1[1], ptr(x2), ptr(q2), shape2[1], ptr(pr, _i32),
+                ptr(pf, _i32), int(pr.shape[0]), alpha, int(esp), inv_lam, ptr(ov), ptr(g),
+                ptr(g1), ptr(gq1), ptr(g2), ptr(gq2), stream_ptr(dev)), "score_bwd_dense")
         return (g1 if need[0] else None, g2 if need[1] else None,
                 gq1 if esp and need[2] else None, gq2 if esp and need[3] else None,
                 None, None, None)

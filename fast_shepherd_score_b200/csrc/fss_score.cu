@@ -575,8 +575,17 @@ int score_fwd_mom_dense_launch(const float* ref_xyz, const float* ref_q, int ref
       (!ref_mom && !fit_mom) || (esp && (!ref_q || !fit_q)))
     return set_error(FSS_ERR_INVALID, "fss_score_fwd_moments_dense: null pointer");
   const ScoreConsts c = score_consts(alpha, esp, inv_lam);
-  // plain + negated/duplicated staging of both clouds
+  // plain + negated/duplicated staging of both clouds (48 bytes a point): clouds whose sum
+  // exceeds the per-CTA shared memory (about 4700 points) take the two-pass form instead
   const size_t smem = 3 * sizeof(float4) * ((size_t)ref_n + fit_n) + 16;
+  int dev = 0, optin = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+    return set_error(FSS_ERR_CUDA, "fss_score_fwd_moments_dense: device query failed");
+  if (smem > (size_t)optin)
+    return set_error(FSS_ERR_UNSUPPORTED,
+                     "fss_score_fwd_moments_dense: clouds too large for the staged moments "
+                     "kernel; use fss_score_fwd_dense + fss_score_bwd_dense");
   // charge pre-scale sqrt(ne / nk) of the packed rows and its inverse for the moments
   const double cs = (esp && c.ne < 0.f) ? std::sqrt((double)c.ne / (double)c.nk) : 0.0;
   const float csf = (float)cs, icsf = cs > 0.0 ? (float)(1.0 / cs) : 0.f;

@@ -270,7 +270,10 @@ int fss_score_bwd_dense(const float *ref_xyz, const float *ref_q, int32_t ref_po
  * (charge component g (c_k - c_y)); ref_moments is (n_pairs, ref_points, 8) floats,
  * fit_moments (n_pairs, fit_points, 8).  fss_score_bwd_moments_dense then turns them into the
  * gradients without a second pass over the pairs.  The overlaps may differ from
- * fss_score_fwd_dense's in the last bits (other summation order). */
+ * fss_score_fwd_dense's in the last bits (other summation order).  Both clouds are staged in
+ * shared memory at 48 bytes a point: when 48 (ref_points + fit_points) + 16 bytes exceed the
+ * device's per-block limit the call returns FSS_ERR_UNSUPPORTED and writes nothing (the
+ * two-pass fss_score_fwd_dense / fss_score_bwd_dense handle those sizes). */
 int fss_score_fwd_moments_dense(const float *ref_xyz, const float *ref_q, int32_t ref_points,
                                 const float *fit_xyz, const float *fit_q, int32_t fit_points,
                                 const int32_t *pair_ref, const int32_t *pair_fit,

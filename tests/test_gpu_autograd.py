@@ -255,3 +255,24 @@ def test_graph_captured_step_matches_eager(cuda):
     torch.testing.assert_close(got[0], s_eager.detach(), rtol=0, atol=0)
     torch.testing.assert_close(got[1], q.grad, rtol=0, atol=0)
     torch.testing.assert_close(got[2], qc.grad, rtol=0, atol=0)
+
+
+@pytest.mark.parametrize("n", [700, 2500])
+def test_large_clouds_both_adjoint_paths(cuda, n):
+    """700-point clouds take the moments kernel with several rows per thread; 2500 + 2500
+    points exceed its shared-memory staging (48 bytes a point) and take the two-pass adjoint.
+    Both match the fp64 oracle: score 1e-5 relative, gradients 1e-4."""
+    from oracle import scores as osc
+    rng = np.random.default_rng(11)
+    (x, cx), (y, cy) = syn.sphere_clouds(rng, [n, n])
+    y = y + 0.3
+    lam = 0.3 * AG.LAM_SCALING
+    X, Y, CX, CY = (_leaf(a, cuda) for a in (x, y, cx, cy))
+    v = AG.get_overlap_esp(X, Y, CX, CY, alpha=1.216, lam=lam)
+    v.backward()
+    np.testing.assert_allclose(v.item(), osc.esp_tanimoto(x, y, cx, cy, 1.216, lam), rtol=1e-5)
+    gx, gy, gcx, gcy = osc.esp_tanimoto_grad(x, y, cx, cy, 1.216, lam)
+    _close_grad(X.grad.cpu().numpy(), gx)
+    _close_grad(Y.grad.cpu().numpy(), gy)
+    _close_grad(CX.grad.cpu().numpy(), gcx)
+    _close_grad(CY.grad.cpu().numpy(), gcy)
