@@ -66,26 +66,23 @@ __device__ __forceinline__ float3 block_sum3(float a, float b, float c, float3* 
 template <bool ESP>
 __device__ __forceinline__ float point_sum(float4 x, const float4* __restrict__ Y, int m,
                                            float nk, float ne) {
-  float s[4] = {0.f, 0.f, 0.f, 0.f};
-  int j = 0;
-  for (; j + 4 <= m; j += 4) {
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const float4 y = Y[j + u];
-      const float dx = x.x - y.x, dy = x.y - y.y, dz = x.z - y.z;
-      float E = nk * (dx * dx + dy * dy + dz * dz);
-      if (ESP) { const float dc = x.w - y.w; E = fmaf(ne * dc, dc, E); }
-      s[u] += ex2(E);
-    }
-  }
-  for (int u = 0; j < m; ++j, ++u) {
-    const float4 y = Y[j];
+  auto g = [&](int k) {
+    const float4 y = Y[k];
     const float dx = x.x - y.x, dy = x.y - y.y, dz = x.z - y.z;
     float E = nk * (dx * dx + dy * dy + dz * dz);
     if (ESP) { const float dc = x.w - y.w; E = fmaf(ne * dc, dc, E); }
-    s[u] += ex2(E);
+    return ex2(E);
+  };
+  float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+  int j = 0;
+  for (; j + 4 <= m; j += 4) {
+    s0 += g(j); s1 += g(j + 1); s2 += g(j + 2); s3 += g(j + 3);
   }
-  return (s[0] + s[1]) + (s[2] + s[3]);
+  // remainder with static accumulator indices (a runtime index would put them in local memory)
+  if (j < m) s0 += g(j);
+  if (j + 1 < m) s1 += g(j + 1);
+  if (j + 2 < m) s2 += g(j + 2);
+  return (s0 + s1) + (s2 + s3);
 }
 
 // Strict upper triangle of a self overlap, sum_{i<j} g(x_i, x_j), for the rows owned by
@@ -265,87 +262,115 @@ __global__ void __launch_bounds__(kScoreMaxThreads) score_bwd_kernel(
   }
 }
 
-// Negated, duplicated staging of a cloud for the packed rows below: point k occupies two
-// float4, (-x, -x, -y, -y) and (-z, -z, -c', -c') with c' = c * cs, so one 16-byte shared
-// load yields the f32x2 operands "minus this point" for two rows at once.
-__device__ __forceinline__ void stage_neg2(float4* __restrict__ d, float4 p, float cs) {
-  const float c = p.w * cs;
-  d[0] = make_float4(-p.x, -p.x, -p.y, -p.y);
-  d[1] = make_float4(-p.z, -p.z, -c, -c);
+// Factored staging of a (centred) cloud for the moment rows: with
+//   E_jk = nk |b_j - y_k|^2 + ne (c_j - c_k)^2 = w_j + P_k . b_j + P_k.w + Q_k c_j,
+//   w_j = nk |b_j|^2 + ne c_j^2,  P_k = -2 nk y_k,  P_k.w = nk |y_k|^2 + ne c_k^2,
+//   Q_k = -2 ne c_k,
+// a term costs 3 FFMA (+1 for the charge) instead of the direct form's 4 differences, 3 for
+// the square and 2 more for the charge.  Points go in pairs (k, k+1) along the f32x2 lanes:
+// F[2r] = (Px_k, Px_k+1, Py_k, Py_k+1), F[2r+1] = (Pz_k, Pz_k+1, Pw_k, Pw_k+1),
+// Qp[r] = (Q_k, Q_k+1); an odd cloud's last pair has a dummy second point with Pw = -inf
+// (its Gaussian is exactly 0).
+__device__ __forceinline__ void stage_factored(const float4* __restrict__ X, int cnt, float nk,
+                                               float ne, float4* __restrict__ F,
+                                               float2* __restrict__ Qp) {
+  for (int r = threadIdx.x; r < (cnt + 1) / 2; r += blockDim.x) {
+    float px[2], py[2], pz[2], pw[2], q[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int k = 2 * r + h;
+      if (k < cnt) {
+        const float4 y = X[k];
+        px[h] = -2.f * nk * y.x; py[h] = -2.f * nk * y.y; pz[h] = -2.f * nk * y.z;
+        pw[h] = fmaf(ne * y.w, y.w, nk * (y.x * y.x + y.y * y.y + y.z * y.z));
+        q[h] = -2.f * ne * y.w;
+      } else {
+        px[h] = py[h] = pz[h] = q[h] = 0.f;
+        pw[h] = -INFINITY;
+      }
+    }
+    F[2 * r] = make_float4(px[0], px[1], py[0], py[1]);
+    F[2 * r + 1] = make_float4(pz[0], pz[1], pw[0], pw[1]);
+    Qp[r] = make_float2(q[0], q[1]);
+  }
 }
 
-// Adjoint moments of two rows at once (f32x2 lanes: lane x = row 0, lane y = row 1) against
-// a cloud staged by stage_neg2: returns sum_k g per lane and sets (mx, my, mz, mc) =
-// sum_k g (x - o_k, ..., c' - o_k').  The charges are pre-scaled by cs = sqrt(ne / nk), so
-// the exponent nk (|x - o|^2 + (c' - o')^2) equals nk |x - o|^2 + ne (c - o_c)^2 with one
-// packed FFMA for the charge term instead of a multiply and an FFMA; the packed FADD2 /
-// FMUL2 / FFMA2 instructions cut the kernel's issued instructions by a quarter against
-// point_grad's scalar loop (the FMA sub-pipes still execute every lane-op: a packed op
-// occupies both halves of the pipe, so the FP32 pipe cycles per term do not change).  One
-// running sum per lane (the two lanes already give each instruction two independent terms,
-// and a second partial sum would push the kernel past 56 registers).
+// One row b (centred, w = charge) against a factored cloud: S' = sum_k 2^(E_jk - w_j) and the
+// raw sums sum_k 2^(E_jk - w_j) (P_k, Q_k), two points per f32x2 instruction.
 template <bool ESP>
-__device__ __forceinline__ float2 rows2_grad(float2 X, float2 Y, float2 Z, float2 C,
-                                             const float4* __restrict__ O, int cnt, float2 nk2,
-                                             float2& mx, float2& my, float2& mz, float2& mc) {
+__device__ __forceinline__ void row_factored(float4 b, const float4* __restrict__ F,
+                                             const float2* __restrict__ Qp, int npair, float& S,
+                                             float& sx, float& sy, float& sz, float& sq) {
   const float2 z2 = make_float2(0.f, 0.f);
-  float2 s = z2, ax = z2, ay = z2, az = z2, ac = z2;
+  const float2 bx = make_float2(b.x, b.x), by = make_float2(b.y, b.y),
+               bz = make_float2(b.z, b.z), bc = make_float2(b.w, b.w);
+  float2 s = z2, ax = z2, ay = z2, az = z2, aq = z2;
 #pragma unroll 4
-  for (int k = 0; k < cnt; ++k) {
-    const float4 a = O[2 * k], b = O[2 * k + 1];
-    const float2 dx = __fadd2_rn(X, make_float2(a.x, a.y));
-    const float2 dy = __fadd2_rn(Y, make_float2(a.z, a.w));
-    const float2 dz = __fadd2_rn(Z, make_float2(b.x, b.y));
-    float2 d2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-    float2 dc = z2;
+  for (int r = 0; r < npair; ++r) {
+    const float4 f0 = F[2 * r], f1 = F[2 * r + 1];
+    const float2 PX = make_float2(f0.x, f0.y), PY = make_float2(f0.z, f0.w),
+                 PZ = make_float2(f1.x, f1.y), PW = make_float2(f1.z, f1.w);
+    float2 E = __ffma2_rn(PX, bx, __ffma2_rn(PY, by, __ffma2_rn(PZ, bz, PW)));
+    float2 Q = z2;
     if (ESP) {
-      dc = __fadd2_rn(C, make_float2(b.z, b.w));
-      d2 = __ffma2_rn(dc, dc, d2);
+      Q = Qp[r];
+      E = __ffma2_rn(Q, bc, E);
     }
-    const float2 E = __fmul2_rn(d2, nk2);
     const float2 g = make_float2(ex2(E.x), ex2(E.y));
     s = __fadd2_rn(s, g);
-    ax = __ffma2_rn(g, dx, ax);
-    ay = __ffma2_rn(g, dy, ay);
-    az = __ffma2_rn(g, dz, az);
-    if (ESP) ac = __ffma2_rn(g, dc, ac);
+    ax = __ffma2_rn(g, PX, ax);
+    ay = __ffma2_rn(g, PY, ay);
+    az = __ffma2_rn(g, PZ, az);
+    if (ESP) aq = __ffma2_rn(g, Q, aq);
   }
-  mx = ax; my = ay; mz = az; mc = ac;
-  return s;
+  S = s.x + s.y; sx = ax.x + ax.y; sy = ay.x + ay.y; sz = az.x + az.y; sq = aq.x + aq.y;
 }
 
-// Rows of one cloud X (plain staging) with moments against the other cloud and itself (both
-// staged by stage_neg2), two rows per thread: row t and row t + ceil(cnt/2) (the second lane
-// repeats row t, and is discarded, for the middle row of an odd cloud).  Adds the rows'
-// cross and self Gaussian sums to *cross / *self and writes the moment rows of pair p.
+// Moments of one row against one cloud: returns sum_k g and writes the float4
+// sum_k g (b - y_k, c_b - c_k).  Factored (two points per packed instruction) unless the
+// row's factor 2^(-w_j) could overflow, then the direct form (point_grad on the plain cloud).
+template <bool ESP>
+__device__ __forceinline__ float row_moments(float4 b, float w, bool direct,
+                                             const float4* __restrict__ Xp, int cnt,
+                                             const float4* __restrict__ F,
+                                             const float2* __restrict__ Qp, float nk, float ne,
+                                             float inv2nk, float inv2ne, float& mx,
+                                             float& my, float& mz, float& mq) {
+  if (direct) return point_grad<ESP>(b, Xp, cnt, nk, ne, mx, my, mz, mq);
+  float S, sx, sy, sz, sq;
+  row_factored<ESP>(b, F, Qp, (cnt + 1) / 2, S, sx, sy, sz, sq);
+  // sum g (b - y) = 2^w (b S' - sum g' y), y = P / (-2 nk); likewise the charges
+  const float scale = ex2(w);
+  mx = scale * fmaf(sx, inv2nk, b.x * S);
+  my = scale * fmaf(sy, inv2nk, b.y * S);
+  mz = scale * fmaf(sz, inv2nk, b.z * S);
+  mq = ESP ? scale * fmaf(sq, inv2ne, b.w * S) : 0.f;
+  return scale * S;
+}
+
+// Rows of cloud X with moments against the other cloud and itself; adds the rows' Gaussian
+// sums to cross / self and writes the two moment rows of each point of pair p.
 template <bool ESP>
 __device__ __forceinline__ void moment_rows(const float4* __restrict__ X, int cnt,
-                                            const float4* __restrict__ Oother, int n_other,
-                                            const float4* __restrict__ Oself, float cs, float ics,
-                                            float2 nk2, float4* __restrict__ mom, float& cross,
-                                            float& self) {
-  const int h = (cnt + 1) / 2;
-  for (int t = threadIdx.x; t < h; t += blockDim.x) {
-    const int r0 = t, r1 = t + h < cnt ? t + h : t;
-    const float4 p0 = X[r0], p1 = X[r1];
-    const float2 px = make_float2(p0.x, p1.x), py = make_float2(p0.y, p1.y),
-                 pz = make_float2(p0.z, p1.z), pc = make_float2(p0.w * cs, p1.w * cs);
-    float2 mx, my, mz, mc;
-    // cross rows first, stored before the self rows so their moments hold no registers
-    const float2 sc = rows2_grad<ESP>(px, py, pz, pc, Oother, n_other, nk2, mx, my, mz, mc);
-    cross += sc.x;
-    mom[2 * r0] = make_float4(mx.x, my.x, mz.x, mc.x * ics);
-    if (r1 != r0) {
-      cross += sc.y;
-      mom[2 * r1] = make_float4(mx.y, my.y, mz.y, mc.y * ics);
-    }
-    const float2 ss = rows2_grad<ESP>(px, py, pz, pc, Oself, cnt, nk2, mx, my, mz, mc);
-    self += ss.x;
-    mom[2 * r0 + 1] = make_float4(mx.x, my.x, mz.x, mc.x * ics);
-    if (r1 != r0) {
-      self += ss.y;
-      mom[2 * r1 + 1] = make_float4(mx.y, my.y, mz.y, mc.y * ics);
-    }
+                                            const float4* __restrict__ Fx,
+                                            const float2* __restrict__ Qx,
+                                            const float4* __restrict__ O, int n_other,
+                                            const float4* __restrict__ Fo,
+                                            const float2* __restrict__ Qo, float nk, float ne,
+                                            float inv2nk, float inv2ne, float4* __restrict__ mom,
+                                            float& cross, float& self) {
+  for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
+    const float4 b = X[j];
+    float w = nk * (b.x * b.x + b.y * b.y + b.z * b.z);
+    if (ESP) w = fmaf(ne * b.w, b.w, w);
+    const bool direct = -w > kFactorMax;
+    float mx, my, mz, mq;
+    cross += row_moments<ESP>(b, w, direct, O, n_other, Fo, Qo, nk, ne, inv2nk, inv2ne, mx, my,
+                              mz, mq);
+    mom[2 * j] = make_float4(mx, my, mz, mq);
+    self += row_moments<ESP>(b, w, direct, X, cnt, Fx, Qx, nk, ne, inv2nk, inv2ne, mx, my, mz,
+                             mq);
+    mom[2 * j + 1] = make_float4(mx, my, mz, mq);
   }
 }
 
@@ -355,47 +380,65 @@ __device__ __forceinline__ void moment_rows(const float4* __restrict__ X, int cn
 // differences).  The pair's overlaps come out of the same passes (V_AB from the fit rows when
 // MF, V_XX from the full rows of a side with moments, the upper triangle otherwise), so the
 // backward is one elementwise step and the Gaussians are evaluated once per step instead of
-// twice.  Shared memory: both clouds plain (n + m float4) and negated/duplicated (2(n + m)).
+// twice.  Both clouds are moved to the ref centroid (the score and every difference are
+// translation invariant) so the factored rows stay inside their overflow bound.  Shared
+// memory per point: plain float4 (16 B) + factored half-pairs (20 B).
 template <bool ESP, bool MR, bool MF>
 __global__ void __launch_bounds__(kMomMaxThreads, kMomMinBlocks) score_fwd_mom_kernel(
     const DenseSrc ref, const DenseSrc fit, const int* __restrict__ pr,
-    const int* __restrict__ pf, float nk, float ne, float Kc, float cs, float ics, float* score,
-    float* ov, float4* __restrict__ momR, float4* __restrict__ momF) {
+    const int* __restrict__ pf, float nk, float ne, float Kc, float inv2nk, float inv2ne,
+    float* score, float* ov, float4* __restrict__ momR, float4* __restrict__ momF) {
   extern __shared__ __align__(16) float4 smem[];
   __shared__ float3 red[kScoreMaxThreads / 32];
   const int p = blockIdx.x;
   const int n = ref.n, m = fit.n;
+  const int hn = (n + 1) / 2, hm = (m + 1) / 2;
   const int r0 = ref.begin(pr[p]), f0 = fit.begin(pf[p]);
   float4* sA = smem;
   float4* sB = sA + n;
-  float4* dA = sB + m;
-  float4* dB = dA + 2 * n;
+  float4* fA = sB + m;
+  float4* fB = fA + 2 * hn;
+  float2* qA = reinterpret_cast<float2*>(fB + 2 * hm);
+  float2* qB = qA + hn;
+  float cx = 0.f, cy = 0.f, cz = 0.f;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     const float4 v = ref.load(r0 + i);
     sA[i] = v;
-    stage_neg2(dA + 2 * i, v, cs);
+    cx += v.x; cy += v.y; cz += v.z;
+  }
+  for (int j = threadIdx.x; j < m; j += blockDim.x) sB[j] = fit.load(f0 + j);
+  const float3 c = block_sum3(cx, cy, cz, red);   // includes the barrier after the loads
+  const float inv_n = n > 0 ? 1.f / (float)n : 0.f;
+  const float ox = c.x * inv_n, oy = c.y * inv_n, oz = c.z * inv_n;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const float4 v = sA[i];
+    sA[i] = make_float4(v.x - ox, v.y - oy, v.z - oz, v.w);
   }
   for (int j = threadIdx.x; j < m; j += blockDim.x) {
-    const float4 v = fit.load(f0 + j);
-    sB[j] = v;
-    stage_neg2(dB + 2 * j, v, cs);
+    const float4 v = sB[j];
+    sB[j] = make_float4(v.x - ox, v.y - oy, v.z - oz, v.w);
   }
   __syncthreads();
-  const float2 nk2 = make_float2(nk, nk);
+  stage_factored(sA, n, nk, ESP ? ne : 0.f, fA, qA);
+  stage_factored(sB, m, nk, ESP ? ne : 0.f, fB, qB);
+  __syncthreads();
   float ab = 0.f, aa = 0.f, bb = 0.f;
   if (MF) {
-    moment_rows<ESP>(sB, m, dA, n, dB, cs, ics, nk2, momF + 2 * (size_t)p * m, ab, bb);
+    moment_rows<ESP>(sB, m, fB, qB, sA, n, fA, qA, nk, ne, inv2nk, inv2ne,
+                     momF + 2 * (size_t)p * m, ab, bb);
   } else {
     bb = self_upper<ESP>(sB, m, blockDim.x - 1 - threadIdx.x, nk, ne);
   }
   if (MR) {
     float abr = 0.f;
-    moment_rows<ESP>(sA, n, dB, m, dA, cs, ics, nk2, momR + 2 * (size_t)p * n, abr, aa);
+    moment_rows<ESP>(sA, n, fA, qA, sB, m, fB, qB, nk, ne, inv2nk, inv2ne,
+                     momR + 2 * (size_t)p * n, abr, aa);
     if (!MF) ab = abr;
   } else {
     // counted from the far end of the block: the fit rows fill it from thread 0
     aa = self_upper<ESP>(sA, n, blockDim.x - 1 - threadIdx.x, nk, ne);
   }
+  __syncthreads();   // red is reused
   const float3 t = block_sum3(ab, aa, bb, red);
   const float vab = t.x * Kc;
   const float vaa = (MR ? t.y : fmaf(2.f, t.y, (float)n)) * Kc;
@@ -575,9 +618,12 @@ int score_fwd_mom_dense_launch(const float* ref_xyz, const float* ref_q, int ref
       (!ref_mom && !fit_mom) || (esp && (!ref_q || !fit_q)))
     return set_error(FSS_ERR_INVALID, "fss_score_fwd_moments_dense: null pointer");
   const ScoreConsts c = score_consts(alpha, esp, inv_lam);
-  // plain + negated/duplicated staging of both clouds (48 bytes a point): clouds whose sum
-  // exceeds the per-CTA shared memory (about 4700 points) take the two-pass form instead
-  const size_t smem = 3 * sizeof(float4) * ((size_t)ref_n + fit_n) + 16;
+  // plain (16 bytes a point) + factored half-pairs (2 float4 + 1 float2 per two points) of
+  // both clouds: clouds whose sum exceeds the per-CTA shared memory (about 6000 points) take
+  // the two-pass form instead
+  const size_t hn = ((size_t)ref_n + 1) / 2, hm = ((size_t)fit_n + 1) / 2;
+  const size_t smem = sizeof(float4) * ((size_t)ref_n + fit_n + 2 * (hn + hm)) +
+                      sizeof(float2) * (hn + hm) + 16;
   int dev = 0, optin = 0;
   if (cudaGetDevice(&dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
@@ -586,9 +632,9 @@ int score_fwd_mom_dense_launch(const float* ref_xyz, const float* ref_q, int ref
     return set_error(FSS_ERR_UNSUPPORTED,
                      "fss_score_fwd_moments_dense: clouds too large for the staged moments "
                      "kernel; use fss_score_fwd_dense + fss_score_bwd_dense");
-  // charge pre-scale sqrt(ne / nk) of the packed rows and its inverse for the moments
-  const double cs = (esp && c.ne < 0.f) ? std::sqrt((double)c.ne / (double)c.nk) : 0.0;
-  const float csf = (float)cs, icsf = cs > 0.0 ? (float)(1.0 / cs) : 0.f;
+  // 1/(2 nk), 1/(2 ne): the factored rows' sums of g P and g Q back to sums of g y and g c
+  const float inv2nk = (float)(0.5 / (double)c.nk);
+  const float inv2ne = (esp && c.ne < 0.f) ? (float)(0.5 / (double)c.ne) : 0.f;
   using K = void (*)(const DenseSrc, const DenseSrc, const int*, const int*, float, float, float,
                      float, float, float*, float*, float4*, float4*);
   const K table[2][3] = {
@@ -606,7 +652,7 @@ int score_fwd_mom_dense_launch(const float* ref_xyz, const float* ref_q, int ref
     return set_error(FSS_ERR_CUDA, std::string("fss_score_fwd_moments_dense: ") + cudaGetErrorString(ce));
   kern<<<P, mom_threads(ref_n, fit_n), smem, st>>>(
       DenseSrc{ref_xyz, esp ? ref_q : nullptr, ref_n}, DenseSrc{fit_xyz, esp ? fit_q : nullptr, fit_n},
-      pair_ref, pair_fit, c.nk, c.ne, c.Kc, csf, icsf, score, overlaps,
+      pair_ref, pair_fit, c.nk, c.ne, c.Kc, inv2nk, inv2ne, score, overlaps,
       reinterpret_cast<float4*>(ref_mom),
       reinterpret_cast<float4*>(fit_mom));
   return check_launch("fss_score_fwd_moments_dense");
