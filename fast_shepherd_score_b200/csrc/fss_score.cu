@@ -38,8 +38,8 @@ int score_threads(int maxN, int maxM) {
 }
 
 // Block-wide sums of three values (fixed order: warp butterfly, then warps in index order).
-// Threads per pair of the moments kernel: its rows go two to a thread (f32x2 lanes), so about
-// one thread per two points of the larger cloud, whole warps, 64..kMomMaxThreads.
+// Threads per pair of the moments kernel: about two rows (points of the larger cloud) per
+// thread, whole warps, 64..kMomMaxThreads.
 int mom_threads(int maxN, int maxM) {
   const int half = (std::max(maxN, maxM) + 1) / 2;
   const int t = ((half + 31) / 32) * 32;
