@@ -276,3 +276,31 @@ def test_large_clouds_both_adjoint_paths(cuda, n):
     _close_grad(Y.grad.cpu().numpy(), gy)
     _close_grad(CX.grad.cpu().numpy(), gcx)
     _close_grad(CY.grad.cpu().numpy(), gcy)
+
+
+def test_moments_guard_rows_mixed_with_factored_rows(cuda):
+    """Surfaces of radius ~10.5 A: with alpha 1.216 the factored exponent's row factor passes
+    its 2^96 bound near that radius, so warps mix rows in the factored and the direct form.
+    Scores and both sides' gradients still match the fp64 oracle (1e-5 / 1e-4)."""
+    from oracle import scores as osc
+    rng = np.random.default_rng(12)
+
+    def surface(n):
+        u = rng.standard_normal((n, 3))
+        u /= np.linalg.norm(u, axis=1, keepdims=True)
+        return 10.5 * u + 0.8 * rng.standard_normal((n, 3)), 0.1 * rng.standard_normal(n)
+
+    (x, cx), (y, cy) = surface(320), surface(280)
+    y = y + np.array([0.4, -0.3, 0.2])
+    lam = 0.3 * AG.LAM_SCALING
+    w = -1.216 / 2 * np.log2(np.e) * np.sum((x - x.mean(0)) ** 2, axis=1)
+    assert (w < -96).any() and (w > -96).any()   # both forms occur
+    X, Y, CX, CY = (_leaf(a, cuda) for a in (x, y, cx, cy))
+    v = AG.get_overlap_esp(X, Y, CX, CY, alpha=1.216, lam=lam)
+    v.backward()
+    np.testing.assert_allclose(v.item(), osc.esp_tanimoto(x, y, cx, cy, 1.216, lam), rtol=1e-5)
+    gx, gy, gcx, gcy = osc.esp_tanimoto_grad(x, y, cx, cy, 1.216, lam)
+    _close_grad(X.grad.cpu().numpy(), gx)
+    _close_grad(Y.grad.cpu().numpy(), gy)
+    _close_grad(CX.grad.cpu().numpy(), gcx)
+    _close_grad(CY.grad.cpu().numpy(), gcy)
