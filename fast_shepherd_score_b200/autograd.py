@@ -14,9 +14,10 @@ torch ops that pack them.
 * :func:`get_overlap`, :func:`get_overlap_esp` -- the reference's signatures for one pair
   ((N,3) vs (M,3)) or a matched batch ((B,N,3) vs (B,M,3)); :class:`DenseTanimoto` runs them
   on the padded tensors directly, with no packing and gradients written straight into the
-  input shapes: ``fss_score_fwd_dense`` without grad, ``fss_score_fwd_moments_dense`` (value
-  plus per-point adjoint moments in one pass) and the elementwise
-  ``fss_score_bwd_moments_dense`` with grad.
+  input shapes: ``fss_score_fwd_moments_dense`` (value, plus per-point adjoint moments of the
+  sides that need a gradient, in one pass) and the elementwise ``fss_score_bwd_moments_dense``;
+  clouds too large for its shared-memory staging take ``fss_score_fwd_dense`` /
+  ``fss_score_bwd_dense``.
 """
 from __future__ import annotations
 
@@ -134,18 +135,17 @@ class DenseTanimoto(torch.autograd.Function):
         lib = _lib.load()
         args = (ptr(x1), ptr(q1), x1.shape[1], ptr(x2), ptr(q2), x2.shape[1], ptr(pr, _i32),
                 ptr(pf, _i32), B, float(alpha), int(esp), float(inv_lam), ptr(score), ptr(ov))
-        m1 = m2 = None
-        if side1 or side2:
-            m1 = torch.empty(B, x1.shape[1], 8, dtype=_f32, device=dev) if side1 else None
-            m2 = torch.empty(B, x2.shape[1], 8, dtype=_f32, device=dev) if side2 else None
-            rc = lib.fss_score_fwd_moments_dense(*args, ptr(m1), ptr(m2), stream_ptr(dev))
-            if rc == _lib.FSS_ERR_UNSUPPORTED:
-                m1 = m2 = None   # clouds too large to stage: the two-pass adjoint below
-            else:
-                check(rc, "score_fwd_moments_dense")
-        if m1 is None and m2 is None:
+        m1 = torch.empty(B, x1.shape[1], 8, dtype=_f32, device=dev) if side1 else None
+        m2 = torch.empty(B, x2.shape[1], 8, dtype=_f32, device=dev) if side2 else None
+        # factored kernel (value only when neither side needs moments)
+        rc = lib.fss_score_fwd_moments_dense(*args, ptr(m1), ptr(m2), stream_ptr(dev))
+        two_pass = rc == _lib.FSS_ERR_UNSUPPORTED
+        if two_pass:   # clouds too large to stage: direct kernel, two-pass adjoint below
+            m1 = m2 = None
             check(lib.fss_score_fwd_dense(*args, stream_ptr(dev)), "score_fwd_dense")
-        two_pass = (side1 or side2) and m1 is None and m2 is None
+        else:
+            check(rc, "score_fwd_moments_dense")
+        two_pass = two_pass and (side1 or side2)
         keep = (x1, x2, q1, q2) if two_pass else (None, None, None, None)
         ctx.save_for_backward(pr, pf, ov, m1, m2, *keep)
         ctx.cfg = (float(alpha), esp, float(inv_lam), x1.shape, x2.shape, dev, side1, side2)

@@ -369,6 +369,31 @@ __device__ __forceinline__ float upper_row(const float4* __restrict__ X, int n, 
   return ex2(w) * (S + (s.x + s.y));
 }
 
+// Full row against another cloud's factored pairs, value only: sum_k g(b, y_k) (direct form
+// beyond the factor bound).
+template <bool ESP>
+__device__ __forceinline__ float cross_row(float4 b, const float4* __restrict__ Y, int cnt,
+                                           const float4* __restrict__ F,
+                                           const float2* __restrict__ Qp, float nk, float ne) {
+  float w = nk * (b.x * b.x + b.y * b.y + b.z * b.z);
+  if (ESP) w = fmaf(ne * b.w, b.w, w);
+  if (-w > kFactorMax) return point_sum<ESP>(b, Y, cnt, nk, ne);
+  const float2 bx = make_float2(b.x, b.x), by = make_float2(b.y, b.y),
+               bz = make_float2(b.z, b.z), bc = make_float2(b.w, b.w);
+  float2 s = make_float2(0.f, 0.f);
+#pragma unroll 4
+  for (int q = 0; q < (cnt + 1) / 2; ++q) {
+    const float4 f0 = F[2 * q], f1 = F[2 * q + 1];
+    float2 E = __ffma2_rn(make_float2(f0.x, f0.y), bx,
+                          __ffma2_rn(make_float2(f0.z, f0.w), by,
+                                     __ffma2_rn(make_float2(f1.x, f1.y), bz,
+                                                make_float2(f1.z, f1.w))));
+    if (ESP) E = __ffma2_rn(Qp[q], bc, E);
+    s = __fadd2_rn(s, make_float2(ex2(E.x), ex2(E.y)));
+  }
+  return ex2(w) * (s.x + s.y);
+}
+
 // Strict upper triangle of a self overlap from the factored pairs, rows in balanced pairs
 // (r, n-1-r) owned by thread slot t, as self_upper.
 template <bool ESP>
@@ -494,6 +519,10 @@ __global__ void __launch_bounds__(kMomMaxThreads, kMomMinBlocks) score_fwd_mom_k
   } else {
     // counted from the far end of the block: the fit rows fill it from thread 0
     aa = self_upper_factored<ESP>(sA, n, blockDim.x - 1 - threadIdx.x, fA, qA, nk, ne);
+  }
+  if (!MR && !MF) {   // value only: the cross term from the fit rows
+    for (int j = threadIdx.x; j < m; j += blockDim.x)
+      ab += cross_row<ESP>(sB[j], sA, n, fA, qA, nk, ne);
   }
   __syncthreads();   // red is reused
   const float3 t = block_sum3(ab, aa, bb, red);
@@ -672,7 +701,7 @@ int score_fwd_mom_dense_launch(const float* ref_xyz, const float* ref_q, int ref
                      "fss_score_fwd_moments_dense: more than fss_max_points() points");
   if (P == 0) return FSS_OK;
   if (!ref_xyz || !fit_xyz || !pair_ref || !pair_fit || !score || !overlaps ||
-      (!ref_mom && !fit_mom) || (esp && (!ref_q || !fit_q)))
+      (esp && (!ref_q || !fit_q)))
     return set_error(FSS_ERR_INVALID, "fss_score_fwd_moments_dense: null pointer");
   const ScoreConsts c = score_consts(alpha, esp, inv_lam);
   // plain (16 bytes a point) + factored half-pairs (2 float4 + 1 float2 per two points) of
@@ -694,12 +723,12 @@ int score_fwd_mom_dense_launch(const float* ref_xyz, const float* ref_q, int ref
   const float inv2ne = (esp && c.ne < 0.f) ? (float)(0.5 / (double)c.ne) : 0.f;
   using K = void (*)(const DenseSrc, const DenseSrc, const int*, const int*, float, float, float,
                      float, float, float*, float*, float4*, float4*);
-  const K table[2][3] = {
+  const K table[2][4] = {
       {score_fwd_mom_kernel<false, true, false>, score_fwd_mom_kernel<false, false, true>,
-       score_fwd_mom_kernel<false, true, true>},
+       score_fwd_mom_kernel<false, true, true>, score_fwd_mom_kernel<false, false, false>},
       {score_fwd_mom_kernel<true, true, false>, score_fwd_mom_kernel<true, false, true>,
-       score_fwd_mom_kernel<true, true, true>}};
-  const K kern = table[esp ? 1 : 0][ref_mom ? (fit_mom ? 2 : 0) : 1];
+       score_fwd_mom_kernel<true, true, true>, score_fwd_mom_kernel<true, false, false>}};
+  const K kern = table[esp ? 1 : 0][ref_mom ? (fit_mom ? 2 : 0) : (fit_mom ? 1 : 3)];
   cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   // all of the unified L1 as shared memory: 7 CTAs of ~30 KB (300 + 300 points) per SM
   if (ce == cudaSuccess)

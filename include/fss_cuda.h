@@ -262,9 +262,10 @@ int fss_score_bwd_dense(const float *ref_xyz, const float *ref_q, int32_t ref_po
                         float *grad_fit_xyz, float *grad_fit_q, void *stream);
 
 /* Forward with adjoint moments (no counterpart in the reference, which differentiates
- * get_overlap / get_overlap_esp by torch autograd): as fss_score_fwd_dense, and in the same
- * pass, for each side whose moments pointer is non-NULL (at least one), writes per pair p and
- * point k of that side two float4 rows (x, y, z, charge):
+ * get_overlap / get_overlap_esp by torch autograd): as fss_score_fwd_dense (with both moments
+ * pointers NULL it computes only the scores and overlaps), and in the same pass, for each
+ * side whose moments pointer is non-NULL, writes per pair p and point k of that side two
+ * float4 rows (x, y, z, charge):
  *   moments[8 (p * points + k) + 0..3] = sum over the other cloud's points y of g (x_k - y)
  *   moments[8 (p * points + k) + 4..7] = sum over the own cloud's points y of g (x_k - y)
  * (charge component g (c_k - c_y)); ref_moments is (n_pairs, ref_points, 8) floats,

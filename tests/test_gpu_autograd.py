@@ -304,3 +304,26 @@ def test_moments_guard_rows_mixed_with_factored_rows(cuda):
     _close_grad(Y.grad.cpu().numpy(), gy)
     _close_grad(CX.grad.cpu().numpy(), gcx)
     _close_grad(CY.grad.cpu().numpy(), gcy)
+
+
+@pytest.mark.parametrize("n", [300, 2500])
+def test_no_grad_scores_match_oracle(cuda, n):
+    """Under torch.no_grad the dense forward is the factored value-only kernel (300 points) or,
+    past its shared-memory staging, the direct kernel (2500 + 2500 points); both give the fp64
+    oracle's vol and ESP Tanimoto scores to 1e-5."""
+    from oracle import scores as osc
+    rng = np.random.default_rng(13)
+    surf = syn.sphere_clouds(rng, [n] * 4)
+    X = torch.tensor(np.stack([p for p, _ in surf[:2]]), device=cuda)
+    Y = torch.tensor(np.stack([p for p, _ in surf[2:]]) + 0.3, device=cuda)
+    CX = torch.tensor(np.stack([c for _, c in surf[:2]]), device=cuda)
+    CY = torch.tensor(np.stack([c for _, c in surf[2:]]), device=cuda)
+    lam = 0.3 * AG.LAM_SCALING
+    with torch.no_grad():
+        e = AG.get_overlap_esp(X, Y, CX, CY, alpha=1.216, lam=lam).cpu().numpy()
+        v = AG.get_overlap(X, Y, alpha=0.81).cpu().numpy()
+    for b in range(2):
+        x, y = X[b].cpu().numpy().astype(np.float64), Y[b].cpu().numpy().astype(np.float64)
+        cx, cy = CX[b].cpu().numpy(), CY[b].cpu().numpy()
+        np.testing.assert_allclose(e[b], osc.esp_tanimoto(x, y, cx, cy, 1.216, lam), rtol=1e-5)
+        np.testing.assert_allclose(v[b], osc.shape_tanimoto(x, y, 0.81), rtol=1e-5)
