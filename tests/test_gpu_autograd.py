@@ -82,8 +82,9 @@ def test_against_fp64_finite_differences(cuda):
 
 def test_config4_size_invariances_and_oracle_sample(cuda):
     """1024 queries (60 atoms + 300 surface points, charges N(0, 0.1)) against 4 fixed
-    targets: translating both clouds leaves every score unchanged, so the gradients of each
-    pair sum to zero; a sample of pairs matches the fp64 analytic gradients."""
+    targets that need no gradient: finite gradients everywhere, and a sample of pairs matches
+    the fp64 analytic gradients and scores (the rigid-motion invariances at this size are
+    checked with both sides differentiable in the next test)."""
     from oracle import scores as osc
     rng = np.random.default_rng(4)
     nq, nt = 1024, 4
@@ -327,3 +328,32 @@ def test_no_grad_scores_match_oracle(cuda, n):
         cx, cy = CX[b].cpu().numpy(), CY[b].cpu().numpy()
         np.testing.assert_allclose(e[b], osc.esp_tanimoto(x, y, cx, cy, 1.216, lam), rtol=1e-5)
         np.testing.assert_allclose(v[b], osc.shape_tanimoto(x, y, 0.81), rtol=1e-5)
+
+
+def test_config4_size_rigid_motion_invariance(cuda):
+    """1024 pairs (60 atoms + 300 charged surface points a side), both sides differentiable:
+    a rigid motion of both clouds leaves each score unchanged, so per pair the coordinate
+    gradients sum to zero over both clouds (translation) and so do x cross g (rotation), to
+    1e-4 of the pair's total gradient magnitude (times its extent for the torque)."""
+    rng = np.random.default_rng(14)
+    nq = 1024
+    atoms = syn.ball_clouds(rng, [60] * (2 * nq))
+    surf = syn.sphere_clouds(rng, [300] * (2 * nq))
+    A = torch.tensor(np.stack(atoms), device=cuda)
+    S = torch.tensor(np.stack([p for p, _ in surf]), device=cuda)
+    Q = torch.tensor(np.stack([c for _, c in surf]), device=cuda)
+    ta, qa = A[:nq].clone().requires_grad_(True), (A[nq:] + 0.5).requires_grad_(True)
+    ts, qs = S[:nq].clone().requires_grad_(True), (S[nq:] + 0.5).requires_grad_(True)
+    tc, qc = Q[:nq].clone().requires_grad_(True), Q[nq:].clone().requires_grad_(True)
+    vol = AG.get_overlap(ta, qa, alpha=0.81)
+    esp = AG.get_overlap_esp(ts, qs, tc, qc, alpha=1.216)
+    (vol.sum() + esp.sum()).backward()
+    for (x1, x2) in ((ta, qa), (ts, qs)):
+        g = torch.cat([x1.grad, x2.grad], 1).double()          # (nq, n1 + n2, 3)
+        x = torch.cat([x1.detach(), x2.detach()], 1).double()
+        mag = g.norm(dim=2).sum(1)
+        force = g.sum(1).norm(dim=1)
+        torque = torch.cross(x, g, dim=2).sum(1).norm(dim=1)
+        ext = x.norm(dim=2).max(1).values
+        assert (force <= 1e-4 * mag).all(), (force / mag).max().item()
+        assert (torque <= 1e-4 * mag * ext).all(), (torque / (mag * ext)).max().item()
