@@ -77,7 +77,7 @@ _SIGS = {
     "fss_score_fwd_moments_dense": ([_vp, _vp, _i32, _vp, _vp, _i32, _vp, _vp, _i32, _f32,
                                      _i32, _f32] + [_vp] * 5, ctypes.c_int),
     "fss_score_bwd_moments_dense": ([_vp, _vp, _i32, _i32, _i32, _f32, _i32, _f32]
-                                    + [_vp] * 9, ctypes.c_int),
+                                    + [_vp] * 8 + [_i32, _vp], ctypes.c_int),
     "fss_probe_peak": ([_i32, _i32, _i32, _vp, ctypes.POINTER(ctypes.c_longlong), _vp],
                        ctypes.c_int),
 }
@@ -91,6 +91,8 @@ _LOCK = threading.Lock()
 def load(build_if_missing: bool = True):
     """Load (building first if needed) and type the shared library."""
     global _LIB
+    if _LIB is not None:   # loaded: no lock on the per-call path
+        return _LIB
     with _LOCK:
         if _LIB is not None:
             return _LIB

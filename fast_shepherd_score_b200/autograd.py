@@ -107,6 +107,11 @@ def _pair_index(B, n_mol, device):
     return t
 
 
+def _f32c(t):
+    """float32 contiguous view or copy (no dispatcher round trip when already so)."""
+    return t if t.dtype is _f32 and t.is_contiguous() else t.to(_f32).contiguous()
+
+
 class DenseTanimoto(torch.autograd.Function):
     """score_b = V_AB / (V_AA + V_BB - V_AB) for padded (B, N, 3) / (B, M, 3) batches (either
     side may be a single molecule broadcast over the batch); optional (B, N) charges.
@@ -123,9 +128,9 @@ class DenseTanimoto(torch.autograd.Function):
         esp = q1 is not None
         B = max(x1.shape[0], x2.shape[0])
         dev = x1.device
-        x1, x2 = x1.to(_f32).contiguous(), x2.to(_f32).contiguous()
-        q1 = q1.to(_f32).contiguous() if esp else None
-        q2 = q2.to(_f32).contiguous() if esp else None
+        x1, x2 = _f32c(x1), _f32c(x2)
+        q1 = _f32c(q1) if esp else None
+        q2 = _f32c(q2) if esp else None
         pr, pf = _pair_index(B, x1.shape[0], dev), _pair_index(B, x2.shape[0], dev)
         score = torch.empty(B, dtype=_f32, device=dev)
         ov = torch.empty(B, 3, dtype=_f32, device=dev)
@@ -158,17 +163,27 @@ class DenseTanimoto(torch.autograd.Function):
         need = ctx.needs_input_grad
         if not (side1 or side2):
             return None, None, None, None, None, None, None
-        g1 = torch.zeros(shape1, dtype=_f32, device=dev) if side1 else None
-        g2 = torch.zeros(shape2, dtype=_f32, device=dev) if side2 else None
-        gq1 = torch.zeros(shape1[:2], dtype=_f32, device=dev) if esp and side1 else None
-        gq2 = torch.zeros(shape2[:2], dtype=_f32, device=dev) if esp and side2 else None
+        B = int(pr.shape[0])
+        moments = m1 is not None or m2 is not None
+        # the moments backward stores the rows of a side with one molecule per pair; a
+        # broadcast molecule (and the two-pass adjoint) accumulates into zeroed buffers
+        own1, own2 = moments and shape1[0] == B, moments and shape2[0] == B
+
+        def buf(shape, own):
+            return (torch.empty if own else torch.zeros)(shape, dtype=_f32, device=dev)
+
+        g1 = buf(shape1, own1) if side1 else None
+        g2 = buf(shape2, own2) if side2 else None
+        gq1 = buf(shape1[:2], own1) if esp and side1 else None
+        gq2 = buf(shape2[:2], own2) if esp and side2 else None
         g = g_score.to(_f32).contiguous()
         lib = _lib.load()
-        if m1 is not None or m2 is not None:
+        if moments:
             check(lib.fss_score_bwd_moments_dense(
-                ptr(pr, _i32), ptr(pf, _i32), int(pr.shape[0]), shape1[1], shape2[1], alpha,
-                int(esp), inv_lam, ptr(ov), ptr(g), ptr(m1), ptr(m2), ptr(g1), ptr(gq1),
-                ptr(g2), ptr(gq2), stream_ptr(dev)), "score_bwd_moments_dense")
+                ptr(pr, _i32), ptr(pf, _i32), B, shape1[1], shape2[1], alpha, int(esp),
+                inv_lam, ptr(ov), ptr(g), ptr(m1), ptr(m2), ptr(g1), ptr(gq1), ptr(g2),
+                ptr(gq2), int(own1) | (int(own2) << 1), stream_ptr(dev)),
+                "score_bwd_moments_dense")
         else:
             check(lib.fss_score_bwd_dense(
                 ptr(x1), ptr(q1), shape1[1], ptr(x2), ptr(q2), shape2[1], ptr(pr, _i32),

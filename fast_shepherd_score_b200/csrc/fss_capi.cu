@@ -85,7 +85,7 @@ int score_bwd_mom_dense_launch(const int32_t* pair_ref, const int32_t* pair_fit,
                                const float* overlaps, const float* grad_score,
                                const float* ref_mom, const float* fit_mom, float* grad_ref_xyz,
                                float* grad_ref_q, float* grad_fit_xyz, float* grad_fit_q,
-                               cudaStream_t st);
+                               int overwrite, cudaStream_t st);
 
 int probe_launch(int which, int iters, int blocks_per_sm, float* out, long long* ops,
                  cudaStream_t st);
@@ -233,11 +233,11 @@ int fss_score_bwd_moments_dense(const int32_t* pair_ref, const int32_t* pair_fit
                                 const float* grad_score, const float* ref_moments,
                                 const float* fit_moments, float* grad_ref_xyz,
                                 float* grad_ref_q, float* grad_fit_xyz, float* grad_fit_q,
-                                void* stream) {
+                                int32_t overwrite, void* stream) {
   FSS_GUARD(fss::score_bwd_mom_dense_launch(pair_ref, pair_fit, n_pairs, ref_points, fit_points,
                                             alpha, esp, inv_lam, overlaps, grad_score,
                                             ref_moments, fit_moments, grad_ref_xyz, grad_ref_q,
-                                            grad_fit_xyz, grad_fit_q, S(stream)));
+                                            grad_fit_xyz, grad_fit_q, overwrite, S(stream)));
 }
 
 int fss_probe_peak(int32_t which, int32_t iters, int32_t blocks_per_sm, float* out,

@@ -190,6 +190,12 @@ struct DenseSink {
     atomicAdd(o + 0, x); atomicAdd(o + 1, y); atomicAdd(o + 2, z);
     if (esp && gq) atomicAdd(gq + k, c);
   }
+  // plain stores, for a side whose every molecule row belongs to exactly one pair
+  __device__ __forceinline__ void put(int k, float x, float y, float z, float c, bool esp) const {
+    float* o = gxyz + 3 * (size_t)k;
+    o[0] = x; o[1] = y; o[2] = z;
+    if (esp && gq) gq[k] = c;
+  }
 };
 
 template <bool ESP, class Src>
@@ -537,9 +543,11 @@ __global__ void __launch_bounds__(kMomMaxThreads, kMomMinBlocks) score_fwd_mom_k
 
 // Backward from the moments: one thread per (pair, point) of each side with moments; the
 // same chain rule and the same expressions as score_bwd_kernel, added atomically into the
-// molecule's row (a broadcast molecule is shared by every pair).
+// molecule's row (a broadcast molecule is shared by every pair), or stored for a side whose
+// bit is set in `overwrite` (bit 0 ref, bit 1 fit: each row belongs to one pair).
 __global__ void score_bwd_mom_kernel(const int* __restrict__ pr, const int* __restrict__ pf,
                                      int P, int n, int m, float aKc, float cKc, int esp,
+                                     int overwrite,
                                      const float* __restrict__ ov, const float* __restrict__ gs,
                                      const float4* __restrict__ momR,
                                      const float4* __restrict__ momF, const DenseSink gR,
@@ -561,9 +569,12 @@ __global__ void score_bwd_mom_kernel(const int* __restrict__ pr, const int* __re
     const float4 c = mom[0], o = mom[1];
     const int row = (isR ? pr[p] : pf[p]) * cnt + k;
     const DenseSink sink{isR ? gR.gxyz : gF.gxyz, isR ? gR.gq : gF.gq};
-    sink.add(row, -aKc * (dAB * c.x + 2.f * dSelf * o.x),
-             -aKc * (dAB * c.y + 2.f * dSelf * o.y), -aKc * (dAB * c.z + 2.f * dSelf * o.z),
-             -cKc * (dAB * c.w + 2.f * dSelf * o.w), esp != 0);
+    const float gx = -aKc * (dAB * c.x + 2.f * dSelf * o.x);
+    const float gy = -aKc * (dAB * c.y + 2.f * dSelf * o.y);
+    const float gz = -aKc * (dAB * c.z + 2.f * dSelf * o.z);
+    const float gc = -cKc * (dAB * c.w + 2.f * dSelf * o.w);
+    if ((overwrite >> (isR ? 0 : 1)) & 1) sink.put(row, gx, gy, gz, gc, esp != 0);
+    else sink.add(row, gx, gy, gz, gc, esp != 0);
   }
 }
 
@@ -749,7 +760,7 @@ int score_bwd_mom_dense_launch(const int32_t* pair_ref, const int32_t* pair_fit,
                                const float* overlaps, const float* grad_score,
                                const float* ref_mom, const float* fit_mom, float* grad_ref_xyz,
                                float* grad_ref_q, float* grad_fit_xyz, float* grad_fit_q,
-                               cudaStream_t st) {
+                               int overwrite, cudaStream_t st) {
   if (P < 0 || ref_n < 0 || fit_n < 0 || !(alpha > 0.f))
     return set_error(FSS_ERR_INVALID, "fss_score_bwd_moments_dense: bad sizes or alpha");
   if (P == 0) return FSS_OK;
@@ -764,7 +775,7 @@ int score_bwd_mom_dense_launch(const int32_t* pair_ref, const int32_t* pair_fit,
   const long long want = (total + 255) / 256;
   const int grid = (int)std::min<long long>(want, (long long)num_sms() * 8);
   score_bwd_mom_kernel<<<grid, 256, 0, st>>>(
-      pair_ref, pair_fit, P, ref_n, fit_n, c.aKc, c.cKc, esp, overlaps, grad_score,
+      pair_ref, pair_fit, P, ref_n, fit_n, c.aKc, c.cKc, esp, overwrite & 3, overlaps, grad_score,
       reinterpret_cast<const float4*>(ref_mom), reinterpret_cast<const float4*>(fit_mom),
       DenseSink{grad_ref_xyz, grad_ref_q}, DenseSink{grad_fit_xyz, grad_fit_q});
   return check_launch("fss_score_bwd_moments_dense");

@@ -284,14 +284,16 @@ int fss_score_fwd_moments_dense(const float *ref_xyz, const float *ref_q, int32_
 /* ADDS into grad_* what fss_score_bwd_dense adds, from the forward's overlaps and moments, for
  * each side whose moments and grad_*_xyz are both non-NULL (grad_*_q may be NULL when
  * esp == 0).  Same expressions as fss_score_bwd_dense, so equal moments and overlaps give
- * bit-identical gradients. */
+ * bit-identical gradients.  Bit 0 (ref) / bit 1 (fit) of `overwrite` STORE that side's
+ * gradients instead of adding them (no zeroing needed): only valid when every molecule of the
+ * side belongs to exactly one pair. */
 int fss_score_bwd_moments_dense(const int32_t *pair_ref, const int32_t *pair_fit,
                                 int32_t n_pairs, int32_t ref_points, int32_t fit_points,
                                 float alpha, int32_t esp, float inv_lam, const float *overlaps,
                                 const float *grad_score, const float *ref_moments,
                                 const float *fit_moments, float *grad_ref_xyz,
                                 float *grad_ref_q, float *grad_fit_xyz, float *grad_fit_q,
-                                void *stream);
+                                int32_t overwrite, void *stream);
 
 /* ---------------------------------------------------------------------------------------
  * Roof probe (measurement support, no reference counterpart): launches a throughput kernel

@@ -172,8 +172,9 @@ def test_one_sided_backward_matches_two_sided(cuda, esp, query_side):
 @pytest.mark.parametrize("esp", [0, 1])
 def test_moment_backward_matches_two_pass_backward(cuda, esp):
     """fss_score_fwd_moments_dense + fss_score_bwd_moments_dense against fss_score_fwd_dense
-    + fss_score_bwd_dense on the same batch (odd cloud sizes, a broadcast target): overlaps
-    and gradients of both sides to fp32 rounding (the moments kernel evaluates the exponent
+    + fss_score_bwd_dense on the same batch (odd cloud sizes, a broadcast target, whose
+    gradient accumulates over the pairs, while the per-pair side is stored over NaN-filled
+    buffers): overlaps and gradients of both sides to fp32 rounding (the moments kernel evaluates the exponent
     with pre-scaled charges and packed f32x2 arithmetic, so the last bits differ)."""
     from fast_shepherd_score_b200 import _lib
     from fast_shepherd_score_b200._lib import ptr, stream_ptr
@@ -207,9 +208,12 @@ def test_moment_backward_matches_two_pass_backward(cuda, esp):
                                            0.81, esp, inv_lam, ptr(sb), ptr(ovb), ptr(m1),
                                            ptr(m2), st) == 0
     gb = fresh()
+    gb[0].fill_(float("nan"))   # the ref side (one molecule per pair) is stored, not added
+    if esp:                     # (no charge gradients are written without ESP)
+        gb[1].fill_(float("nan"))
     assert lib.fss_score_bwd_moments_dense(ptr(pr), ptr(pf), B, N, M, 0.81, esp, inv_lam,
                                            ptr(ova), ptr(gs), ptr(m1), ptr(m2),
-                                           *(ptr(t) for t in gb), st) == 0
+                                           *(ptr(t) for t in gb), 1, st) == 0
     torch.cuda.synchronize(cuda)
     torch.testing.assert_close(ovb, ova, rtol=5e-6, atol=0)
     torch.testing.assert_close(sb, sa, rtol=5e-6, atol=0)
