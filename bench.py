@@ -682,7 +682,8 @@ def run_score_grad(args, wl):
     ho = [torch.empty(nq).pin_memory(), torch.empty(nq).pin_memory()] + \
         [torch.empty_like(x).pin_memory() for x in hq]
     e2e_ms = []
-    for i in range((max(1, min(args.steps, 3)) + 1) if args.e2e else 0):
+    # a step is ~1 ms end to end: the median of 20 (after one warm-up) steadies the host jitter
+    for i in range(21 if args.e2e else 0):
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
         a, s_, c = (x.to(dev, non_blocking=True).requires_grad_(True) for x in hq)
