@@ -266,7 +266,7 @@ def _tuned_tile(mode, shape, ref, fit, ref_ph, fit_ph, pair_ref, pair_fit, seed_
     cost = cs_r.counts[pr].astype(np.int64) * cs_f.counts[pf].astype(np.int64)
     # enough pairs for many waves of CTAs, so the sample is throughput- not latency-bound and
     # its load balance resembles the full launch's: 16 pairs per SM, or half the batch (up to
-    # 64 per SM) so tiles with long work items (1-2 lanes per pose) are not judged by a tail
+    # 64 per SM) so tiles with long work items (1-2 lanes per pose) are not ranked by a tail
     sms = torch.cuda.get_device_properties(seed_q.device).multi_processor_count
     k = min(P, max(16 * sms, min(P // 2, 64 * sms)))
     sel = torch.from_numpy(autotune.sample_pairs(cost, k)).to(seed_q.device)
