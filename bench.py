@@ -65,6 +65,28 @@ WORKLOADS = {
 }
 
 
+# The headline metric (the 50-start x 200-step alignment workloads); both arms of the bench
+# print this exact string for it, so their lines are directly comparable.
+HEADLINE_METRIC = ("aligned pairs/s (50 starts\u00d7200 steps) batched vs plain; p50/p99 screen "
+                   "latency")
+
+
+def metric_of(wl):
+    """The metric string of a workload, identical in the CUDA and the reference arm."""
+    if wl["mode"] == "score_grad":
+        return ("scored queries/s (vol + surface-ESP Tanimoto with coordinate and charge "
+                "gradients)")
+    if wl["starts"] == 50 and wl["steps"] == 200:
+        return HEADLINE_METRIC
+    return f"aligned pairs/s ({wl['mode']}: {wl['starts']} starts x {wl['steps']} Adam steps)"
+
+
+def dist_env():
+    """(world size, rank, local rank) of this process (torchrun's environment)."""
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
 def make_inputs(wl, n_pairs, seed):
     from fast_shepherd_score_b200 import synthetic as syn
     from fast_shepherd_score_b200.api import HostBatch
@@ -213,12 +235,7 @@ def run_cuda(args, wl):
     from fast_shepherd_score_b200 import align as al
     from fast_shepherd_score_b200.layout import cost_order_device
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    world, rank, local = dist_env()
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     n_pairs = args.pairs or wl["pairs"]
@@ -318,9 +335,6 @@ def run_cuda(args, wl):
         assert np.all(np.isfinite(out.scores))
 
     if rank != 0:
-        if world > 1:
-            dist.barrier()
-            dist.destroy_process_group()
         return None
 
     # ---- roofline ---------------------------------------------------------------------
@@ -332,7 +346,7 @@ def run_cuda(args, wl):
     roof = min(peak["ex2"], peak["ffma"] / per_term_fp32)
 
     line = {
-        "metric": "aligned pairs/s (50 starts x 200 Adam steps), batched fused kernel",
+        "metric": metric_of(wl),
         "value": round(value, 2), "unit": "aligned pairs/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -371,10 +385,6 @@ def run_cuda(args, wl):
             line["comparators"]["batched_over_plain"] = round(value / plain["value"], 1)
     if args.server and world == 1:
         line["server"] = server_bench(dev, duration=args.server_seconds)
-    print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
     return line
 
 
@@ -607,12 +617,7 @@ def run_score_grad(args, wl):
     import torch
     import torch.distributed as dist
     from fast_shepherd_score_b200 import autograd as AG
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    world, rank, local = dist_env()
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     nq = args.pairs or wl["pairs"]
@@ -699,17 +704,13 @@ def run_score_grad(args, wl):
     if world > 1:
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
     if rank != 0:
-        if world > 1:
-            dist.barrier()
-            dist.destroy_process_group()
         return None
     peak = measure_peak(dev)
     achieved = terms / (ms_per_step * 1e-3)
     h2d = sum(x.nbytes for x in hq)
     d2h = nq * 4 * 2 + h2d
     line = {
-        "metric": "scored queries/s (vol + surface-ESP Tanimoto with coordinate and charge "
-                  "gradients)",
+        "metric": metric_of(wl),
         "value": round(value, 2), "unit": "queries/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
@@ -747,10 +748,6 @@ def run_score_grad(args, wl):
                                 "sample": f"{k} queries (fp64 numpy restatement of the "
                                           "reference's torch scoring and its gradients, one "
                                           "thread)"}
-    print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
     return line
 
 
@@ -763,12 +760,7 @@ def run_esp_combo(args, wl):
     import torch.distributed as dist
     from fast_shepherd_score_b200 import align as al, kernels as K
     from fast_shepherd_score_b200.layout import CloudSet
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    world, rank, local = dist_env()
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     n_pairs = args.pairs or wl["pairs"]
@@ -879,16 +871,12 @@ def run_esp_combo(args, wl):
     if world > 1:
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
     if rank != 0:
-        if world > 1:
-            dist.barrier()
-            dist.destroy_process_group()
         return None
     peak = measure_peak(dev)
     kavg = statistics.mean(a.elapsed_time(b) for a, b in kern)
     achieved = terms / (kavg * 1e-3)
     line = {
-        "metric": "aligned pairs/s (vol_and_surf_esp: 8 starts x 60 Adam steps), batched fused "
-                  "kernel",
+        "metric": metric_of(wl),
         "value": round(value, 2), "unit": "aligned pairs/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -914,10 +902,6 @@ def run_esp_combo(args, wl):
     }
     if args.cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(wl, raw, budget_s=args.cpu_seconds)
-    print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
     return line
 
 
@@ -940,8 +924,7 @@ def _reference_score_grad(args, wl, world):
         if it >= args.warmup:
             rates.append(k / (time.perf_counter() - t0))
     value = statistics.median(rates)
-    line = {"impl": "reference", "metric": "scored queries/s (vol + surface-ESP Tanimoto with "
-                                           "coordinate and charge gradients)",
+    line = {"impl": "reference", "metric": metric_of(wl),
             "value": round(value, 3), "unit": "queries/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1e3 * nq / value, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -950,7 +933,6 @@ def _reference_score_grad(args, wl, world):
                              "kind": "port", "sample": f"{budget:.1f} s of queries per step"},
             "e2e": {"value": round(value, 3), "unit": "queries/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
     return line
 
 
@@ -980,7 +962,7 @@ def run_reference(args, wl):
     ms = statistics.median(times) * 1e3
     value = k / (ms * 1e-3)
     line = {"impl": "reference",
-            "metric": f"aligned pairs/s ({wl['starts']} starts x {wl['steps']} Adam steps)",
+            "metric": metric_of(wl),
             "value": round(value, 3), "unit": "aligned pairs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -994,8 +976,48 @@ def run_reference(args, wl):
                                        "present on the GPU box)"},
             "e2e": {"value": round(value, 3), "unit": "aligned pairs/s",
                     "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
     return line
+
+
+# The other workloads, measured in the same run and reported under the line's "configs" key
+# (one GPU only): each with its own value, kernel time, algorithmic work and roofline fraction.
+CONFIG_WORKLOADS = ("vol", "vol_pharm", "score_grad", "vol_and_surf_esp")
+
+
+def run_workload(args, wl):
+    if wl["mode"] == "vol_and_surf_esp":
+        return run_esp_combo(args, wl)
+    if wl["mode"] == "score_grad":
+        return run_score_grad(args, wl)
+    return run_cuda(args, wl)
+
+
+def other_configs(args, headline):
+    """Short runs of the other workloads (warm-up 3, at most 5 timed steps, no CPU legs)."""
+    sub = argparse.Namespace(**vars(args))
+    sub.steps, sub.warmup = max(3, min(args.steps, 5)), 3
+    sub.pairs, sub.tile = 0, ""
+    sub.cpu_baseline = sub.comparators = sub.server = False
+    out = {}
+    for name in CONFIG_WORKLOADS:
+        if name == headline:
+            continue
+        line = run_workload(sub, WORKLOADS[name])
+        roof = line["roofline"]
+        rec = {"workload": line["config"]["workload"], "metric": line["metric"],
+               "value": line["value"], "unit": line["unit"], "steps": sub.steps,
+               "warmup": sub.warmup, "ms_per_step": line["ms_per_step"],
+               "e2e": line["e2e"]["value"],
+               "kernel_ms": roof.get("kernel_ms"),
+               "terms_per_launch": roof.get("terms_per_launch", roof.get("terms_per_step")),
+               "roofline": {k: roof[k] for k in ("achieved", "peak", "unit", "frac")},
+               "clocks": {k: line["clocks"].get(k) for k in ("sm_mhz", "reasons")}}
+        if "tile" in line["config"]:
+            rec["tile"] = line["config"]["tile"]
+        if "eager" in line:
+            rec["eager"] = line["eager"]["value"]
+        out[name] = rec
+    return out
 
 
 def main(argv=None):
@@ -1013,6 +1035,8 @@ def main(argv=None):
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-server", dest="server", action="store_false",
                     help="skip the screening-server leg (Poisson stream, p50/p99)")
+    ap.add_argument("--no-configs", dest="configs", action="store_false",
+                    help="skip the short runs of the other workloads (the 'configs' key)")
     ap.add_argument("--server-seconds", type=float, default=20.0)
     ap.add_argument("--tile", default="", help="fixed tiling instead of the autotuner: "
                     "lanes_per_pose,chunks,cta_per_sm,accumulate[,kernel_variant] (e.g. 32,0,0,2 or "
@@ -1029,12 +1053,26 @@ def main(argv=None):
         print(json.dumps({"server": server_bench(dev, duration=args.server_seconds)}), flush=True)
         return None
     if args.impl == "reference":
-        return run_reference(args, wl)
-    if wl["mode"] == "vol_and_surf_esp":
-        return run_esp_combo(args, wl)
-    if wl["mode"] == "score_grad":
-        return run_score_grad(args, wl)
-    return run_cuda(args, wl)
+        line = run_reference(args, wl)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return line
+    world, rank, _ = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        line = run_workload(args, wl)
+        if line is not None and args.configs and world == 1:
+            line["configs"] = other_configs(args, args.workload)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+    return line
 
 
 if __name__ == "__main__":

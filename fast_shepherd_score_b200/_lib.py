@@ -119,20 +119,23 @@ def load(build_if_missing: bool = True):
         return lib
 
 
+_STATUS_EXC = {FSS_ERR_INVALID: ValueError, FSS_ERR_NOMEM: MemoryError,
+               FSS_ERR_UNSUPPORTED: ValueError}
+
+
+def raise_status(rc: int, msg: str) -> None:
+    """Raise the Python exception of an fss_status code: FSS_ERR_INVALID / UNSUPPORTED ->
+    ValueError, FSS_ERR_NOMEM -> MemoryError (callers halve a batch on it), else
+    RuntimeError."""
+    raise _STATUS_EXC.get(rc, RuntimeError)(msg)
+
+
 def check(rc: int, what: str = "") -> None:
-    """Raise the Python exception matching an fss_status code."""
+    """Raise the Python exception matching an fss_status code returned by the library."""
     if rc == FSS_OK:
         return
     msg = load().fss_last_error().decode(errors="replace")
-    if what:
-        msg = f"{what}: {msg}"
-    if rc == FSS_ERR_INVALID:
-        raise ValueError(msg)
-    if rc == FSS_ERR_NOMEM:
-        raise MemoryError(msg)
-    if rc == FSS_ERR_UNSUPPORTED:
-        raise ValueError(msg)
-    raise RuntimeError(msg)
+    raise_status(rc, f"{what}: {msg}" if what else msg)
 
 
 def ptr(t, dtype=None, name="tensor"):

@@ -30,7 +30,7 @@ from typing import Optional
 import numpy as np
 import torch
 
-from . import _lib, autotune, kernels, legacy_seeds
+from . import _lib, autotune, kernels, legacy_seeds, memory
 from ._lib import AlignDesc, check, ptr, stream_ptr
 from .layout import CloudSet, PharmSet, cost_order_device
 
@@ -48,9 +48,18 @@ _SCRATCH: dict = {}
 LAST_TILE: dict = {}   # tiling of the most recent fused launch (for reports)
 
 
-def _scratch(device) -> torch.Tensor:
-    """Per-device 2-int32 scratch (work counter + status) reused by every launch on it."""
-    key = torch.device(device).index
+def _scratch(device, stream=None) -> torch.Tensor:
+    """The 2-int32 scratch (persistent-grid work counter + status word) of launches on
+    (device, stream), defaulting to the device's current stream.
+
+    The launch resets the counter on its own stream before the kernel starts, so launches on
+    one stream are ordered and can share one buffer; two launches that may run at the same
+    time (different streams, e.g. a server's stream and the caller's) must not, or both
+    kernels would take work items from the same counter.  Hence one buffer per stream."""
+    device = torch.device(device)
+    if stream is None:
+        stream = torch.cuda.current_stream(device)
+    key = (device.index, int(stream.cuda_stream))
     s = _SCRATCH.get(key)
     if s is None:
         s = torch.zeros(2, dtype=_i32, device=device)
@@ -96,6 +105,9 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
     ``validate=False`` skips the pair-index range check (a device read-back) for callers that
     validated their indices on the host; ``check_status=False`` skips reading the kernel's
     status word (both keep the launch free of host synchronisation).
+    ``scratch`` (2 int32: work counter, status word) defaults to one buffer per (device,
+    current stream); a caller passing its own must not share it between launches that can
+    overlap on the GPU.
     """
     m = MODE_IDS[mode]
     shape = m != _lib.MODE_PHARM
@@ -180,12 +192,11 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
         accumulate = tile.get("accumulate", 0)
         kernel_variant = tile.get("kernel_variant", 0)
     if rows is None:
-        rows = (torch.empty(P * S, dtype=_f32, device=dev),
-                torch.empty(P * S, 4, dtype=_f32, device=dev),
-                torch.empty(P * S, 3, dtype=_f32, device=dev))
+        rows = (memory.empty(P * S, _f32, dev), memory.empty((P * S, 4), _f32, dev),
+                memory.empty((P * S, 3), _f32, dev))
     if out is None:
-        out = (torch.empty(P, dtype=_f32, device=dev), torch.empty(P, 4, dtype=_f32, device=dev),
-               torch.empty(P, 3, dtype=_f32, device=dev))
+        out = (memory.empty(P, _f32, dev), memory.empty((P, 4), _f32, dev),
+               memory.empty((P, 3), _f32, dev))
     scratch = _scratch(dev) if scratch is None else scratch
     LAST_TILE.clear()
     LAST_TILE.update(lanes_per_pose=int(lanes_per_pose), chunks=int(chunks),

@@ -28,7 +28,7 @@ import torch
 
 from . import align as al
 from . import kernels as K
-from . import legacy_seeds
+from . import legacy_seeds, memory
 from .layout import CloudSet, PharmSet, _offsets
 
 LAM_SCALING = al.LAM_SCALING
@@ -184,13 +184,45 @@ def align_host(mode: str, ref: HostBatch, fit: HostBatch, *, pair_ref=None, pair
 
 def align_device(mode, ref: Optional[CloudSet], fit: Optional[CloudSet],
                  ref_ph: Optional[PharmSet], fit_ph: Optional[PharmSet], pair_ref, pair_fit,
-                 *, alpha=0.81, lam=0.3, color_weight=0.5, num_seeds=50, steps=200, lr=0.1,
-                 seeds=None, ref_self=None, fit_self=None, ref_self_ph=None, fit_self_ph=None,
-                 similarity="tanimoto", extended_points=False, only_extended=False,
-                 trans_centres: Optional[CloudSet] = None, num_repeats_per_trans: int = 10,
-                 topk: int = 30, **tile):
+                 *, num_seeds=50, seeds=None, trans_centres: Optional[CloudSet] = None,
+                 num_repeats_per_trans: int = 10, topk: int = 30,
+                 max_chunk_pairs: Optional[int] = None, **kw):
     """Device-resident form of :func:`align_host` (all tensors already on the GPU).
     ``similarity`` / ``extended_points`` / ``only_extended`` apply to mode "pharm".
+
+    The pairs run in memory-bounded chunks (:mod:`fast_shepherd_score_b200.memory`): a chunk
+    holds at most 0.7 x the free device memory (or ``max_chunk_pairs`` pairs) and halves on
+    an out-of-memory error.  Pairs are independent, so the results equal one call's.
+    Everything else is :func:`_align_device_once`."""
+    P = int(pair_ref.shape[0])
+    if seeds is not None:
+        starts, grid = int(seeds[0].shape[1]), 0
+    elif trans_centres is not None:
+        starts = topk
+        grid = 5 + num_repeats_per_trans * int(trans_centres.max_points)
+    else:
+        starts, grid = int(num_seeds), 0
+
+    def process(a, k):
+        sd = None if seeds is None else (seeds[0][a:a + k], seeds[1][a:a + k])
+        return _align_device_once(mode, ref, fit, ref_ph, fit_ph, pair_ref[a:a + k],
+                                  pair_fit[a:a + k], num_seeds=num_seeds, seeds=sd,
+                                  trans_centres=trans_centres,
+                                  num_repeats_per_trans=num_repeats_per_trans, topk=topk, **kw)
+
+    return memory.run_chunked(P, memory.align_bytes_per_pair(starts, grid), process,
+                              pair_ref.device, max_chunk=max_chunk_pairs)
+
+
+def _align_device_once(mode, ref: Optional[CloudSet], fit: Optional[CloudSet],
+                       ref_ph: Optional[PharmSet], fit_ph: Optional[PharmSet], pair_ref,
+                       pair_fit, *, alpha=0.81, lam=0.3, color_weight=0.5, num_seeds=50,
+                       steps=200, lr=0.1, seeds=None, ref_self=None, fit_self=None,
+                       ref_self_ph=None, fit_self_ph=None, similarity="tanimoto",
+                       extended_points=False, only_extended=False,
+                       trans_centres: Optional[CloudSet] = None,
+                       num_repeats_per_trans: int = 10, topk: int = 30, **tile):
+    """One call of :func:`align_device` without chunking.
 
     ``trans_centres`` (a CloudSet indexed like the reference molecules) selects the
     translation-seeded starts of the reference's ``trans_init=True``: per pair the legacy grid
@@ -226,8 +258,8 @@ def align_device(mode, ref: Optional[CloudSet], fit: Optional[CloudSet],
             pr, pf = pair_ref[a:a + step], pair_fit[a:a + step]
             gq, gt, G = legacy_seeds.grid_packed(g_ref, g_fit, trans_centres, pr, pf,
                                                  num_repeats_per_trans, shift)
-            coarse = align_device(mode, ref, fit, ref_ph, fit_ph, pr, pf, steps=1,
-                                  seeds=(gq, gt), **kw)
+            coarse = _align_device_once(mode, ref, fit, ref_ph, fit_ph, pr, pf, steps=1,
+                                        seeds=(gq, gt), **kw)
             q_, t_ = legacy_seeds.select(coarse.rows[0], gq, gt, G, topk)
             sel_q.append(q_)
             sel_t.append(t_)

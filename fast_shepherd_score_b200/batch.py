@@ -170,12 +170,13 @@ class MoleculePairBatch:
                          verbose: bool = False, backend: Optional[str] = None,
                          return_aligned: bool = False):
         _resolve(backend)
-        sc = A._align_batch_pharm(self.pairs, similarity=similarity,
-                                  extended_points=extended_points, only_extended=only_extended,
-                                  trans_init=trans_init,
-                                  num_repeats=self._seeds("pharm", num_repeats),
-                                  steps_fine=self._steps("pharm", max_num_steps), lr=lr)
-        scores = np.asarray(sc, dtype=float)
+        A._align_batch_pharm(self.pairs, similarity=similarity,
+                             extended_points=extended_points, only_extended=only_extended,
+                             trans_init=trans_init, num_repeats=self._seeds("pharm", num_repeats),
+                             steps_fine=self._steps("pharm", max_num_steps), lr=lr)
+        # read back from the pairs, as the reference does (_batch.py:1335): the aligner's
+        # contract is the in-place result
+        scores = np.array([float(p.sim_aligned_pharm) for p in self.pairs], dtype=float)
         if not return_aligned:
             return scores, [None] * len(self.pairs), [None] * len(self.pairs)
         ancs, vecs = [], []

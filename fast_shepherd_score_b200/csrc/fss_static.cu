@@ -12,6 +12,8 @@
 // The array exists once per device that loads the library and lives until process exit.
 // Every call shares it: calls whose work overlaps on the GPU (different streams, or
 // different host threads without ordering) race on it and must be serialised by the caller.
+#include <cuda.h>  // driver types only; the two driver calls are looked up at run time
+
 #include <mutex>
 #include <string>
 
@@ -30,7 +32,39 @@ static __device__ __align__(256) unsigned char g_align_scratch[kStaticBytes];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-void* g_addr[kMaxDevices] = {};
+// Per device: the address of g_align_scratch in the context it was resolved in.  A
+// cudaDeviceReset destroys that context (and the module with the array); the next call
+// then finds another context id and resolves the address again.
+struct Slot {
+  unsigned long long ctx_id;
+  void* addr;
+};
+Slot g_slot[kMaxDevices] = {};
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+CtxGetCurrentFn g_ctx_current = nullptr;
+CtxGetIdFn g_ctx_id = nullptr;
+
+// Unique id of the context current on this thread (0: none current, or no driver support).
+unsigned long long current_context_id() {
+  if (!g_ctx_current || !g_ctx_id) {
+    cudaDriverEntryPointQueryResult q1, q2;
+    void *f1 = nullptr, *f2 = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f1, 12000, cudaEnableDefault, &q1) !=
+            cudaSuccess || q1 != cudaDriverEntryPointSuccess ||
+        cudaGetDriverEntryPointByVersion("cuCtxGetId", &f2, 12000, cudaEnableDefault, &q2) !=
+            cudaSuccess || q2 != cudaDriverEntryPointSuccess)
+      return 0;
+    g_ctx_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+    g_ctx_id = reinterpret_cast<CtxGetIdFn>(f2);
+  }
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (g_ctx_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+  if (g_ctx_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 
 int scratch_address(void** out) {
   int dev = 0;
@@ -41,15 +75,20 @@ int scratch_address(void** out) {
   if (dev < 0 || dev >= kMaxDevices)
     return set_error(FSS_ERR_UNSUPPORTED, "fss_align_static: device ordinal above 63");
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_addr[dev]) {  // first call on this device (with it current): resolve the address
+  Slot& slot = g_slot[dev];
+  const unsigned long long ctx = current_context_id();
+  if (!slot.addr || ctx == 0 || ctx != slot.ctx_id) {
+    // first call on this device (or in a new context of it), with the device current:
+    // resolve the array's device address
     void* p = nullptr;
     ce = cudaGetSymbolAddress(&p, g_align_scratch);
     if (ce != cudaSuccess || !p)
       return set_error(FSS_ERR_CUDA, std::string("fss_align_static: cudaGetSymbolAddress: ") +
                                          cudaGetErrorString(ce));
-    g_addr[dev] = p;
+    slot.addr = p;
+    slot.ctx_id = current_context_id();  // the lookup above made the context current
   }
-  *out = g_addr[dev];
+  *out = slot.addr;
   return FSS_OK;
 }
 
@@ -84,7 +123,18 @@ int align_static_launch(const fss_align_desc* d, cudaStream_t st) {
       return set_error(FSS_ERR_CUDA, std::string("fss_align_static: row reset: ") +
                                          cudaGetErrorString(ce));
   }
-  return align_launch(&local, st);
+  rc = align_launch(&local, st);
+  if (rc != FSS_OK) return rc;
+  // the caller's optional status word (device int32) receives this call's flags, ordered
+  // after the launch on `st` (bit 0: a pair larger than the declared max_* extents)
+  if (d->scratch) {
+    cudaError_t ce = cudaMemcpyAsync(d->scratch, local.scratch + 1, sizeof(int32_t),
+                                     cudaMemcpyDeviceToDevice, st);
+    if (ce != cudaSuccess)
+      return set_error(FSS_ERR_CUDA, std::string("fss_align_static: status copy: ") +
+                                         cudaGetErrorString(ce));
+  }
+  return FSS_OK;
 }
 
 }  // namespace fss

@@ -1,10 +1,10 @@
 """Screening front-end: ``screen()`` / ``screen_many()`` over a sharded profile store.
 
-Mirrors shepherd_score/screen.py for the CUDA path: ``ProfileStore`` (:317-606) reads and
-writes the reference's on-disk format (``manifest.json`` with ``version`` 1 and a shard list,
-``shard_NNNNN.npz`` holding concatenated arrays with CSR offsets, float16 or float32),
-``screen_many`` (:1038) streams every shard once for a whole query panel, ``screen`` (:1141)
-is the one-query wrapper, ``Hit`` (:75) is ``(score, id, transform)``.
+Mirrors shepherd_score/screen.py for the CUDA path: the library is a ``ProfileStore``
+(:mod:`fast_shepherd_score_b200.store`, the reference's on-disk format; a store object of
+shepherd_score itself is accepted too), ``screen_many`` (:1038) streams every shard once for
+a whole query panel, ``screen`` (:1141) is the one-query wrapper, ``Hit`` (:75) is
+``(score, id, transform)``.
 
 Each shard is uploaded once (float16 coordinates expand to float32 on the device) and kept
 as packed device clouds; every query is one reference molecule staged once per work item,
@@ -14,9 +14,7 @@ are selected on the device, so only K transforms are built per shard and query.
 from __future__ import annotations
 
 import heapq
-import json
 import os
-import re
 from collections import namedtuple
 from typing import List, Optional, Sequence
 
@@ -25,7 +23,8 @@ import torch
 
 from . import api
 from .layout import CloudSet, PharmSet, _offsets
-from .modes import CANONICAL_MODES, canonical, seeds_for, steps_for
+from .modes import canonical, seeds_for, steps_for
+from .store import ProfileStore  # noqa: F401  (re-exported: the screening entry points take it)
 
 Hit = namedtuple("Hit", ["score", "id", "transform"])
 
@@ -41,201 +40,6 @@ def ALPHA(num_points):
     f = interp1d(np.array([50, 100, 150, 200, 300, 400]),
                  np.array([0.6011, 0.8668, 1.022, 1.118, 1.216, 1.258]), "quadratic")
     return float(f(num_points))
-
-
-def _schema_from_modes(modes) -> dict:
-    """Which arrays a store keeps for its modes (screen.py:203-216)."""
-    modes = {canonical(m) for m in modes}
-    unknown = modes - set(CANONICAL_MODES)
-    if unknown:
-        raise ValueError(f"unknown modes {sorted(unknown)}; valid: {list(CANONICAL_MODES)}")
-    return dict(surf=bool({"surf", "surf_esp", "vol_and_surf_esp"} & modes),
-                surf_esp=bool({"surf_esp", "vol_and_surf_esp"} & modes),
-                charges=bool({"vol_esp", "vol_and_surf_esp"} & modes),
-                with_H="vol_and_surf_esp" in modes, radii="vol_and_surf_esp" in modes,
-                centers_w_H="vol_and_surf_esp" in modes,
-                pharm=bool({"pharm", "vol_color", "vol_pharm"} & modes))
-
-
-def _supports(schema, mode) -> bool:
-    """screen.py:219-236 (plus vol_pharm, which needs the pharmacophore arrays)."""
-    mode = canonical(mode)
-    if mode == "vol":
-        return True
-    if mode == "vol_esp":
-        return schema["charges"]
-    if mode == "surf":
-        return schema["surf"]
-    if mode == "surf_esp":
-        return schema["surf"] and schema["surf_esp"]
-    if mode in ("pharm", "vol_color", "vol_pharm"):
-        return schema["pharm"]
-    if mode == "vol_and_surf_esp":
-        return (schema["surf"] and schema["surf_esp"] and schema["centers_w_H"]
-                and schema["radii"] and schema["charges"] and schema["with_H"])
-    return False
-
-
-class ProfileStore:
-    """Sharded on-disk molecule profiles (the reference's format, VERSION 1)."""
-    MANIFEST = "manifest.json"
-    VERSION = 1
-
-    def __init__(self, path, manifest, rw):
-        self.path, self.manifest, self._rw = path, manifest, rw
-        self._buf: list = []
-        self._n = int(manifest.get("n_total", 0))
-        self._shard_id = len(manifest.get("shards", []))
-
-    # ---- writer -----------------------------------------------------------------------
-    @classmethod
-    def create(cls, path, *, num_surf_points: int, modes: Sequence[str], dtype: str = "float16",
-               shard_size: int = 100_000, pre_centered: bool = True,
-               overwrite: bool = False) -> "ProfileStore":
-        if dtype not in ("float16", "float32"):
-            raise ValueError("dtype must be 'float16' or 'float32'")
-        schema = _schema_from_modes(modes)
-        os.makedirs(path, exist_ok=True)
-        mpath = os.path.join(path, cls.MANIFEST)
-        if os.path.exists(mpath) and not overwrite:
-            raise FileExistsError(f"{mpath} already exists; pass overwrite=True to replace it")
-        if overwrite:
-            for f in os.listdir(path):
-                if f == cls.MANIFEST or re.fullmatch(r"shard_\d{5}\.npz", f):
-                    os.remove(os.path.join(path, f))
-        manifest = dict(version=cls.VERSION, num_surf_points=int(num_surf_points),
-                        modes=list(modes), schema=schema, dtype=dtype,
-                        shard_size=int(shard_size), pre_centered=bool(pre_centered), n_total=0,
-                        shards=[])
-        st = cls(path, manifest, "w")
-        st._write_manifest()
-        return st
-
-    def add_arrays(self, *, atom_pos, surf_pos=None, surf_esp=None, partial_charges=None,
-                   pharm_types=None, pharm_ancs=None, pharm_vecs=None, centers_w_H=None,
-                   radii=None, nonH_atoms_idx=None, id=None) -> None:
-        """Buffer one molecule given as arrays (centred on its atom COM when the store is
-        pre-centred, as the reference's writer does).  Stores with hydrogens
-        (vol_and_surf_esp) take ``partial_charges``, ``radii`` and ``centers_w_H`` for all
-        atoms and ``nonH_atoms_idx`` (default: the first len(atom_pos) atoms are the heavy
-        ones)."""
-        if self._rw != "w":
-            raise RuntimeError("store is open for reading")
-        rec = dict(atom_pos=np.asarray(atom_pos, np.float32), surf_pos=surf_pos,
-                   surf_esp=surf_esp, partial_charges=partial_charges, pharm_types=pharm_types,
-                   pharm_ancs=pharm_ancs, pharm_vecs=pharm_vecs, centers_w_H=centers_w_H,
-                   radii=radii, nonH=nonH_atoms_idx,
-                   id=self._n + len(self._buf) if id is None else id)
-        if self.manifest["schema"]["with_H"]:
-            if centers_w_H is None or radii is None or partial_charges is None:
-                raise ValueError("a store with hydrogens needs centers_w_H, radii and "
-                                 "partial_charges for every atom")
-            if rec["nonH"] is None:
-                rec["nonH"] = np.arange(len(rec["atom_pos"]), dtype=np.int64)
-        if self.manifest["pre_centered"]:
-            c = rec["atom_pos"].mean(0)
-            rec["atom_pos"] = rec["atom_pos"] - c
-            if surf_pos is not None:
-                rec["surf_pos"] = np.asarray(surf_pos, np.float32) - c
-            if pharm_ancs is not None:
-                rec["pharm_ancs"] = np.asarray(pharm_ancs, np.float32) - c
-            if centers_w_H is not None:
-                rec["centers_w_H"] = np.asarray(centers_w_H, np.float32) - c
-        self._buf.append(rec)
-        if len(self._buf) >= self.manifest["shard_size"]:
-            self._flush()
-
-    def close(self):
-        if self._rw == "w":
-            self._flush()
-            self._write_manifest()
-
-    def __enter__(self):
-        return self
-
-    def __exit__(self, *exc):
-        self.close()
-
-    def _write_manifest(self):
-        with open(os.path.join(self.path, self.MANIFEST), "w") as fh:
-            json.dump(self.manifest, fh, indent=2)
-
-    def _flush(self):
-        if not self._buf:
-            return
-        sch = self.manifest["schema"]
-        dt = np.float16 if self.manifest["dtype"] == "float16" else np.float32
-        recs = self._buf
-        off = lambda L: np.concatenate([[0], np.cumsum(L)]).astype(np.int64)
-        out = {"ids": np.array([r["id"] for r in recs])}
-        out["atom_off"] = off([len(r["atom_pos"]) for r in recs])
-        out["atom_pos"] = np.concatenate([r["atom_pos"] for r in recs]).astype(dt)
-        if sch["surf"]:
-            out["surf_pos"] = np.stack([r["surf_pos"] for r in recs]).astype(dt)
-        if sch["surf_esp"]:
-            out["surf_esp"] = np.stack([r["surf_esp"] for r in recs]).astype(dt)
-        if sch["charges"] and sch["with_H"]:
-            # layout of the reference's writer (screen.py:470-481): all-atom arrays with their
-            # own offsets, heavy-atom indices into them
-            out["all_off"] = off([len(r["partial_charges"]) for r in recs])
-            out["charges"] = np.concatenate([r["partial_charges"] for r in recs]).astype(dt)
-            out["nonH"] = np.concatenate([r["nonH"] for r in recs]).astype(np.int64)
-            if sch["radii"]:
-                out["radii"] = np.concatenate([r["radii"] for r in recs]).astype(dt)
-            if sch["centers_w_H"]:
-                out["cwh"] = np.concatenate([r["centers_w_H"] for r in recs]).astype(dt)
-        elif sch["charges"]:
-            out["charges"] = np.concatenate([r["partial_charges"] for r in recs]).astype(dt)
-        if sch["pharm"]:
-            out["pharm_off"] = off([len(r["pharm_types"]) for r in recs])
-            out["pharm_types"] = np.concatenate([r["pharm_types"] for r in recs]).astype(np.int32)
-            out["pharm_ancs"] = np.concatenate([r["pharm_ancs"] for r in recs]).astype(dt)
-            out["pharm_vecs"] = np.concatenate([r["pharm_vecs"] for r in recs]).astype(dt)
-        name = f"shard_{self._shard_id:05d}.npz"
-        np.savez(os.path.join(self.path, name), **out)
-        self.manifest["shards"].append(dict(name=name, n=len(recs), start=self._n))
-        self._n += len(recs)
-        self.manifest["n_total"] = self._n
-        self._buf = []
-        self._shard_id += 1
-        self._write_manifest()
-
-    # ---- reader -----------------------------------------------------------------------
-    @classmethod
-    def open(cls, path) -> "ProfileStore":
-        with open(os.path.join(path, cls.MANIFEST)) as fh:
-            manifest = json.load(fh)
-        if manifest.get("version") != cls.VERSION:
-            raise ValueError(f"ProfileStore at {path!r} has on-disk format version "
-                             f"{manifest.get('version')!r}; this reader reads {cls.VERSION}")
-        return cls(path, manifest, "r")
-
-    def __len__(self):
-        return int(self.manifest["n_total"])
-
-    @property
-    def num_surf_points(self) -> int:
-        return int(self.manifest["num_surf_points"])
-
-    @property
-    def modes(self) -> tuple:
-        return tuple(self.manifest["modes"])
-
-    @property
-    def pre_centered(self) -> bool:
-        return bool(self.manifest["pre_centered"])
-
-    @property
-    def num_shards(self) -> int:
-        return len(self.manifest["shards"])
-
-    def supports(self, mode) -> bool:
-        return _supports(self.manifest["schema"], mode)
-
-    def read_shard(self, idx: int):
-        sh = self.manifest["shards"][idx]
-        with np.load(os.path.join(self.path, sh["name"])) as data:
-            return sh, {k: data[k] for k in data.files}
 
 
 # -----------------------------------------------------------------------------------------

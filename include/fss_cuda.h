@@ -208,10 +208,14 @@ int fss_align(const fss_align_desc *desc, void *stream);
  * per-(pair, start) rows and the work counter live in one library-owned __device__ array
  * of FSS_STATIC_MAX_ROWS rows (about 4 MiB per device, held until the process exits), so
  * n_pairs * n_starts above FSS_STATIC_MAX_ROWS is rejected with FSS_ERR_UNSUPPORTED.
- * out_score/out_q/out_t are required.  The first call on a device resolves the array's
- * address (cudaGetSymbolAddress) with that device current; make that first call before
- * any stream capture.  All calls share the array, so calls that overlap on the GPU race;
- * a pair larger than the declared max_* extents returns a NaN score. */
+ * out_score/out_q/out_t are required.  The first call on a device (and the first after a
+ * cudaDeviceReset, which gives the device a new context) resolves the array's address
+ * (cudaGetSymbolAddress) with that device current; make that first call before any stream
+ * capture.  All calls share the array, so calls that overlap on the GPU race.  A pair
+ * larger than the declared max_* extents returns a NaN score; when `scratch` is not NULL it
+ * is read as ONE device int32 that receives the call's status flags (as fss_align's
+ * scratch[1]: bit 0 set when a pair exceeded the extents), copied on `stream` after the
+ * launch. */
 #define FSS_STATIC_MAX_ROWS 131072
 int fss_align_static(const fss_align_desc *desc, void *stream);
 
