@@ -384,7 +384,9 @@ def run_cuda(args, wl):
         if plain:
             line["comparators"]["batched_over_plain"] = round(value / plain["value"], 1)
     if args.server and world == 1:
-        line["server"] = server_bench(dev, duration=args.server_seconds)
+        line["server"] = server_bench(dev, duration=args.server_seconds,
+                                      launch_pairs=args.server_launch_pairs,
+                                      policy=args.server_policy)
     return line
 
 
@@ -515,15 +517,17 @@ def comparators(wl, raw, dev, n_plain=16, n_graph=256):
     return out
 
 
-def server_bench(dev, duration=20.0, n_lib=1_000_000, load=0.6, seed=7):
+def server_bench(dev, duration=20.0, n_lib=1_000_000, load=0.6, seed=7, launch_pairs=32768,
+                 policy="srpt"):
     """Screening server under a Poisson request stream (bounded run, rank 0).
 
     1M-molecule device-resident library (15-60 atoms + 3-20 pharmacophores), shape +
     directional pharmacophore scoring, 20 starts x 100 Adam steps, request sizes log-uniform
-    in [1e3, 1e5] library molecules, offered load = `load` x the measured capacity."""
+    in [1e3, 1e5] library molecules, offered load = `load` x the measured capacity; at most
+    ``launch_pairs`` pairs per fused launch, admission ``policy`` ("srpt" or "fifo")."""
     import torch
     from fast_shepherd_score_b200 import align as al, kernels as K, synthetic as syn
-    from fast_shepherd_score_b200.server import ScreenServer
+    from fast_shepherd_score_b200.server import ScreenServer, latency_by_decade
     t0 = time.perf_counter()
     atoms, ph = syn.library_on_device(n_lib, seed, dev)
     torch.cuda.synchronize(dev)
@@ -554,7 +558,7 @@ def server_bench(dev, duration=20.0, n_lib=1_000_000, load=0.6, seed=7):
     # library bytes a pair reads from HBM: the molecule's packed atoms + pharmacophores
     mol_bytes = (atoms.pts.nbytes + ph.anc.nbytes + ph.vec.nbytes) / n_lib
     with ScreenServer((atoms, ph), mode="vol_pharm", starts=20, steps=100, lanes_per_pose=lpp,
-                      max_pairs_per_launch=65536, tile=tile) as srv:
+                      max_pairs_per_launch=launch_pairs, tile=tile, policy=policy) as srv:
         # capacity: after one warm-up request (first launches load kernels and grow the
         # pinned-buffer cache), two large requests in flight together
         srv.submit(pool[1], rng.choice(n_lib, 65536, replace=False), top_k=100).result()
@@ -582,6 +586,7 @@ def server_bench(dev, duration=20.0, n_lib=1_000_000, load=0.6, seed=7):
             f.result()
         wall = time.perf_counter() - t_start
         lat = np.array(srv.latencies[3:]) * 1e3      # drop the warm-up and capacity probes
+        by_size = latency_by_decade(srv.size_latency[3:])
         st = srv.stats()
     return {"library": n_lib, "mode": "vol_pharm (shape + directional pharmacophore)",
             "starts": 20, "adam_steps": 100, "request_pairs": "log-uniform [1e3, 1e5]",
@@ -591,6 +596,7 @@ def server_bench(dev, duration=20.0, n_lib=1_000_000, load=0.6, seed=7):
             "pairs_per_s": round((st["pairs_done"] - n_probe) / wall, 1),
             "p50_ms": round(float(np.percentile(lat, 50)), 2),
             "p99_ms": round(float(np.percentile(lat, 99)), 2),
+            "by_request_size": by_size, "policy": policy, "max_pairs_per_launch": launch_pairs,
             "max_queue_depth": st["max_queue_depth"], "tile": dict(tile, lanes_per_pose=lpp),
             "library_bytes_per_molecule": round(mol_bytes, 1),
             "library_hbm_gbs_at_capacity": round(cap * mol_bytes / 1e9, 3),
@@ -1038,6 +1044,9 @@ def main(argv=None):
     ap.add_argument("--no-configs", dest="configs", action="store_false",
                     help="skip the short runs of the other workloads (the 'configs' key)")
     ap.add_argument("--server-seconds", type=float, default=20.0)
+    ap.add_argument("--server-launch-pairs", type=int, default=32768,
+                    help="largest fused launch of the screening server (pairs)")
+    ap.add_argument("--server-policy", default="srpt", choices=["srpt", "fifo"])
     ap.add_argument("--tile", default="", help="fixed tiling instead of the autotuner: "
                     "lanes_per_pose,chunks,cta_per_sm,accumulate[,kernel_variant] (e.g. 32,0,0,2 or "
                     "16,7,0,0,4)")
@@ -1050,7 +1059,9 @@ def main(argv=None):
         import torch
         dev = torch.device("cuda", 0)
         torch.cuda.set_device(dev)
-        print(json.dumps({"server": server_bench(dev, duration=args.server_seconds)}), flush=True)
+        print(json.dumps({"server": server_bench(dev, duration=args.server_seconds,
+                                                 launch_pairs=args.server_launch_pairs,
+                                                 policy=args.server_policy)}), flush=True)
         return None
     if args.impl == "reference":
         line = run_reference(args, wl)

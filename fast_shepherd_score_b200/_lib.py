@@ -49,7 +49,7 @@ class AlignDesc(ctypes.Structure):
         ("max_ref_atoms", _i32), ("max_fit_atoms", _i32), ("max_ref_surf", _i32),
         ("max_fit_surf", _i32), ("esp_inv_lam", _f32), ("coulomb", _f32),
         ("probe_radius", _f32), ("esp_weight", _f32), ("esp_stride", _i32),
-        ("scratch", _vp),
+        ("scratch", _vp), ("fit_f16", _i32),
     ]
 
 
@@ -60,9 +60,10 @@ _SIGS = {
     "fss_overlap_grad": ([_vp] * 8 + [_i32] * 3 + [_f32, _f32, _i32] + [_vp] * 4, ctypes.c_int),
     "fss_pharm_grad": ([_vp] * 10 + [_i32] * 5 + [_vp] * 4, ctypes.c_int),
     "fss_tanimoto_adam_step": ([_vp] * 13 + [_i32, _f32, _vp], ctypes.c_int),
-    "fss_self_overlap": ([_vp, _vp, _i32, _i32, _f32, _i32, _f32, _vp, _vp], ctypes.c_int),
-    "fss_pharm_self_overlap": ([_vp, _vp, _vp, _i32, _i32, _i32, _i32, _vp, _vp], ctypes.c_int),
-    "fss_seeds": ([_vp] * 6 + [_i32, _i32, _vp, _i32, _vp, _vp, _vp], ctypes.c_int),
+    "fss_self_overlap": ([_vp, _vp, _i32, _i32, _f32, _i32, _f32, _i32, _vp, _vp], ctypes.c_int),
+    "fss_pharm_self_overlap": ([_vp, _vp, _vp, _i32, _i32, _i32, _i32, _i32, _vp, _vp],
+                               ctypes.c_int),
+    "fss_seeds": ([_vp] * 6 + [_i32, _i32, _vp, _i32, _i32, _vp, _vp, _vp], ctypes.c_int),
     "fss_align": ([ctypes.POINTER(AlignDesc), _vp], ctypes.c_int),
     "fss_align_static": ([ctypes.POINTER(AlignDesc), _vp], ctypes.c_int),
     "fss_pick_best": ([_vp] * 3 + [_i32, _i32] + [_vp] * 4, ctypes.c_int),
@@ -113,7 +114,7 @@ def load(build_if_missing: bool = True):
             fn = getattr(lib, name)
             fn.argtypes = argt
             fn.restype = rest
-        if lib.fss_abi_version() != 2:
+        if lib.fss_abi_version() != 3:
             raise RuntimeError("libfss_cuda.so ABI version mismatch; rebuild the library")
         _LIB = lib
         return lib

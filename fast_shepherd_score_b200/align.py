@@ -207,15 +207,23 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
     d.mode, d.n_pairs, d.n_starts, d.steps = m, P, S, int(steps)
     d.pair_ref, d.pair_fit = ptr(pair_ref, _i32), ptr(pair_fit, _i32)
     d.order = ptr(order, _i32) if order is not None else None
+    # the fit (library) side may be kept in float16; the kernel widens it while staging
+    halves = set()
     if shape:
-        d.ref_pts, d.ref_off = ptr(ref.pts, _f32), ptr(ref.off, _i32)
-        d.fit_pts, d.fit_off = ptr(fit.pts, _f32), ptr(fit.off, _i32)
+        d.ref_pts, d.ref_off = ptr(ref.pts, _f32, "ref points"), ptr(ref.off, _i32)
+        d.fit_pts, h = kernels.points(fit.pts, "fit points")
+        halves.add(h)
+        d.fit_off = ptr(fit.off, _i32)
         d.max_ref_points, d.max_fit_points = ref.max_points, fit.max_points
     if pharm:
-        d.ref_anc, d.ref_ph_off = ptr(ref_ph.anc, _f32), ptr(ref_ph.off, _i32)
-        d.fit_anc, d.fit_ph_off = ptr(fit_ph.anc, _f32), ptr(fit_ph.off, _i32)
+        d.ref_anc, d.ref_ph_off = ptr(ref_ph.anc, _f32, "ref anchors"), ptr(ref_ph.off, _i32)
+        d.fit_anc, h = kernels.points(fit_ph.anc, "fit anchors")
+        halves.add(h)
+        d.fit_ph_off = ptr(fit_ph.off, _i32)
         if directional:
-            d.ref_vec, d.fit_vec = ptr(ref_ph.vec, _f32), ptr(fit_ph.vec, _f32)
+            d.ref_vec = ptr(ref_ph.vec, _f32, "ref vectors")
+            d.fit_vec, h = kernels.points(fit_ph.vec, "fit vectors")
+            halves.add(h)
         d.max_ref_features, d.max_fit_features = ref_ph.max_points, fit_ph.max_points
         d.ref_self_ph = ptr(ref_self_ph, _f32) if ref_self_ph is not None else None
         d.fit_self_ph = ptr(fit_self_ph, _f32) if fit_self_ph is not None else None
@@ -249,6 +257,9 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
         d.esp_stride = int(esp_stride)
     if similarity != "tanimoto":
         d.similarity, d.tversky_sigma = 1, TVERSKY_SIGMA[similarity]
+    if len(halves) > 1:
+        raise ValueError("the fit clouds and pharmacophores must share one dtype")
+    d.fit_f16 = halves.pop() if halves else 0
     d.scratch = ptr(scratch, _i32)
     check(_lib.load().fss_align(d, stream_ptr(dev)), f"align[{mode}]")
     if check_status:

@@ -319,6 +319,8 @@ def _centred_pharm(ps: PharmSet):
     """The set with every molecule's anchors centred on its own centroid (types kept).  The
     centroid is a padded per-molecule sum (the reference's masked sum, pharm.py:215-219), so
     it is deterministic (an atomic scatter-add would make the last bits run-dependent)."""
+    if ps.anc.dtype != torch.float32:
+        raise ValueError("mode 'pharm' re-centres its anchors: it needs float32 sets")
     dev = ps.anc.device
     n = torch.as_tensor(ps.counts, device=dev)
     mol = torch.repeat_interleave(torch.arange(len(ps.counts), device=dev), n)

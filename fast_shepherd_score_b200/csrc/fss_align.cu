@@ -32,7 +32,7 @@ __global__ void pick_best_kernel(const float* __restrict__ rs, const float* __re
 // Self overlaps of packed clouds at the identity pose (one CTA of 32 threads per molecule).
 // ---------------------------------------------------------------------------------------
 template <bool ESP>
-__global__ void self_overlap_kernel(const float4* __restrict__ pts, const int* __restrict__ off,
+__global__ void self_overlap_kernel(const Pts pts, const int* __restrict__ off,
                                     int n_mol, int max_n, float k, float e, float inv2k, float Kc,
                                     float* out) {
   extern __shared__ __align__(16) float4 smem[];
@@ -61,9 +61,8 @@ __global__ void self_overlap_kernel(const float4* __restrict__ pts, const int* _
 }
 
 template <int EXT>
-__global__ void pharm_self_kernel(const float4* __restrict__ anc, const float4* __restrict__ vec,
-                                  const int* __restrict__ off, int n_mol, int max_n,
-                                  PharmTables tab, float* out) {
+__global__ void pharm_self_kernel(const Pts anc, const Pts vec, const int* __restrict__ off,
+                                  int n_mol, int max_n, PharmTables tab, float* out) {
   extern __shared__ __align__(16) float4 smem[];
   __shared__ float red[96];
   const int m = blockIdx.x;
@@ -77,8 +76,8 @@ __global__ void pharm_self_kernel(const float4* __restrict__ anc, const float4* 
   float4* sFA = sRV + n;
   float4* sFV = sFA + n;
   const float3 c = block_centroid(anc + o0, n, red);
-  stage_ref_pharm(anc + o0, vec ? vec + o0 : nullptr, n, c, sRA, sRV);
-  stage_fit_pharm(anc + o0, vec ? vec + o0 : nullptr, n, sFA, sFV);
+  stage_ref_pharm(anc + o0, vec + o0, n, c, sRA, sRV);
+  stage_fit_pharm(anc + o0, vec + o0, n, sFA, sFV);
   __syncthreads();
   Rot R;
 #pragma unroll
@@ -166,6 +165,11 @@ int align_launch(const fss_align_desc* d, cudaStream_t st) {
   if ((d->mode == FSS_MODE_PHARM || d->mode == FSS_MODE_SHAPE_PHARM) && (!d->ref_vec || !d->fit_vec))
     return set_error(FSS_ERR_INVALID, "fss_align: directional pharm needs vectors");
   if (shape && !(d->alpha > 0.f)) return set_error(FSS_ERR_INVALID, "fss_align: alpha must be > 0");
+  if (d->fit_f16 != 0 && d->fit_f16 != 1)
+    return set_error(FSS_ERR_INVALID, "fss_align: fit_f16 must be 0 or 1");
+  if (d->fit_f16 && combo)
+    return set_error(FSS_ERR_UNSUPPORTED, "fss_align: float16 fit clouds are not supported in "
+                                          "mode ESP_COMBO");
   const int maxN = shape ? d->max_ref_points : 0, maxM = shape ? d->max_fit_points : 0;
   const int maxNp = pharm ? d->max_ref_features : 0, maxMp = pharm ? d->max_fit_features : 0;
   const int maxNa = combo ? d->max_ref_atoms : 0, maxMa = combo ? d->max_fit_atoms : 0;
@@ -257,6 +261,7 @@ int align_launch(const fss_align_desc* d, cudaStream_t st) {
     p.esp_w = d->esp_weight;
     p.esp_stride = d->esp_stride > 0 ? d->esp_stride : 1;
   }
+  p.fit_f16 = d->fit_f16;
   p.tab = make_pharm_tables(d->mode != FSS_MODE_SHAPE_COLOR);
   p.row_score = d->row_score; p.row_q = d->row_q; p.row_t = d->row_t;
   p.counter = d->scratch;
@@ -299,7 +304,7 @@ int pick_best_launch(const float* rs, const float* rq, const float* rt, int P, i
 }
 
 int self_overlap_launch(const float* pts, const int32_t* off, int n_mol, int max_n, float alpha,
-                        int esp, float inv_lam, float* out, cudaStream_t st) {
+                        int esp, float inv_lam, int f16, float* out, cudaStream_t st) {
   if (n_mol < 0 || !pts || !off || !out || !(alpha > 0.f))
     return set_error(FSS_ERR_INVALID, "fss_self_overlap: bad arguments");
   if (max_n > kMaxPoints) return set_error(FSS_ERR_UNSUPPORTED, "fss_self_overlap: molecule too large");
@@ -314,18 +319,18 @@ int self_overlap_launch(const float* pts, const int32_t* off, int n_mol, int max
   if (esp) {
     ce = cudaFuncSetAttribute(self_overlap_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (ce == cudaSuccess)
-      self_overlap_kernel<true><<<n_mol, 32, smem, st>>>(reinterpret_cast<const float4*>(pts), off, n_mol, max_n, k, e, inv2k, Kc, out);
+      self_overlap_kernel<true><<<n_mol, 32, smem, st>>>(Pts(pts, f16), off, n_mol, max_n, k, e, inv2k, Kc, out);
   } else {
     ce = cudaFuncSetAttribute(self_overlap_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (ce == cudaSuccess)
-      self_overlap_kernel<false><<<n_mol, 32, smem, st>>>(reinterpret_cast<const float4*>(pts), off, n_mol, max_n, k, 0.f, inv2k, Kc, out);
+      self_overlap_kernel<false><<<n_mol, 32, smem, st>>>(Pts(pts, f16), off, n_mol, max_n, k, 0.f, inv2k, Kc, out);
   }
   if (ce != cudaSuccess) return set_error(FSS_ERR_CUDA, std::string("fss_self_overlap: ") + cudaGetErrorString(ce));
   return check_launch("fss_self_overlap");
 }
 
 int pharm_self_launch(const float* anc, const float* vec, const int32_t* off, int n_mol, int max_n,
-                      int directional, int extended, float* out, cudaStream_t st) {
+                      int directional, int extended, int f16, float* out, cudaStream_t st) {
   if (n_mol < 0 || !anc || !off || !out || (directional && !vec))
     return set_error(FSS_ERR_INVALID, "fss_pharm_self_overlap: bad arguments");
   if (extended < 0 || extended > 2 || (extended && !directional))
@@ -338,8 +343,7 @@ int pharm_self_launch(const float* anc, const float* vec, const int32_t* off, in
               : extended == 2 ? pharm_self_kernel<2> : pharm_self_kernel<0>;
   cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (ce != cudaSuccess) return set_error(FSS_ERR_CUDA, std::string("fss_pharm_self_overlap: ") + cudaGetErrorString(ce));
-  kern<<<n_mol, 32, smem, st>>>(reinterpret_cast<const float4*>(anc),
-                                reinterpret_cast<const float4*>(vec), off, n_mol, max_n,
+  kern<<<n_mol, 32, smem, st>>>(Pts(anc, f16), Pts(vec, f16), off, n_mol, max_n,
                                 make_pharm_tables(directional != 0), out);
   return check_launch("fss_pharm_self_overlap");
 }

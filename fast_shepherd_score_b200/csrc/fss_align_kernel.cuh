@@ -44,6 +44,7 @@ struct AlignParams {
   int maxNa, maxMa, maxNs, maxMs;
   float coulomb, probe, nkl, esp_w;  // nkl = -log2(e) / (LAM_SCALING * lam)
   int esp_stride;
+  int fit_f16;  // fit clouds / pharmacophores stored as float16 (x, y, z, w), widened in staging
   PharmTables tab;
   float* row_score; float* row_q; float* row_t;
   int* counter;
@@ -161,7 +162,7 @@ __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
       else if constexpr (TCE)
         stage_ref_tce<kEsp>(p.ref_pts + r0, N, c, p.k, p.e, sP, nbMax);
       else stage_ref<kEsp>(p.ref_pts + r0, N, c, p.k, p.e, sP, sQc);
-      stage_copy(p.fit_pts + f0, M, sB);
+      stage_copy(Pts(p.fit_pts, p.fit_f16) + f0, M, sB);
     }
     if (kCombo) {
       // reference-side arrays move into the centred frame of the shape channel
@@ -189,7 +190,8 @@ __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
     if (kPharm) {
       if (!kShape) c = block_centroid(p.ref_anc + rp0, Np, red);
       stage_ref_pharm(p.ref_anc + rp0, p.ref_vec ? p.ref_vec + rp0 : nullptr, Np, c, sRA, sRV);
-      stage_fit_pharm(p.fit_anc + fp0, p.fit_vec ? p.fit_vec + fp0 : nullptr, Mp, sFA, sFV);
+      stage_fit_pharm(Pts(p.fit_anc, p.fit_f16) + fp0, Pts(p.fit_vec, p.fit_f16) + fp0, Mp, sFA,
+                      sFV);
     }
     __syncthreads();
 

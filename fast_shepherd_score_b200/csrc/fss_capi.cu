@@ -52,7 +52,7 @@ int tanimoto_adam_launch(const float* V, const float* dQ, const float* dT, const
                          float* best, float* bq, float* bt, int K, float lr, cudaStream_t st);
 int seeds_launch(const float* ref_pts, const int32_t* ref_off, const float* fit_pts,
                  const int32_t* fit_off, const int32_t* pair_ref, const int32_t* pair_fit,
-                 int P, int S, const float* fibo, int n_fibo, float* sq, float* st,
+                 int P, int S, const float* fibo, int n_fibo, int fit_f16, float* sq, float* st,
                  cudaStream_t stream);
 int score_fwd_launch(const float* ref_pts, const int32_t* ref_off, const float* fit_pts,
                      const int32_t* fit_off, const int32_t* pair_ref, const int32_t* pair_fit,
@@ -139,24 +139,31 @@ int fss_tanimoto_adam_step(const float* V, const float* dQ, const float* dT, con
 }
 
 int fss_self_overlap(const float* pts, const int32_t* off, int32_t n_mol, int32_t max_points,
-                     float alpha, int32_t esp, float inv_lam, float* out, void* stream) {
-  FSS_GUARD(fss::self_overlap_launch(pts, off, n_mol, max_points, alpha, esp, inv_lam, out,
-                                     S(stream)));
+                     float alpha, int32_t esp, float inv_lam, int32_t pts_f16, float* out,
+                     void* stream) {
+  if (pts_f16 != 0 && pts_f16 != 1)
+    return fss::set_error(FSS_ERR_INVALID, "fss_self_overlap: pts_f16 must be 0 or 1");
+  FSS_GUARD(fss::self_overlap_launch(pts, off, n_mol, max_points, alpha, esp, inv_lam, pts_f16,
+                                     out, S(stream)));
 }
 
 int fss_pharm_self_overlap(const float* anc, const float* vec, const int32_t* off,
                            int32_t n_mol, int32_t max_features, int32_t directional,
-                           int32_t extended, float* out, void* stream) {
+                           int32_t extended, int32_t pts_f16, float* out, void* stream) {
+  if (pts_f16 != 0 && pts_f16 != 1)
+    return fss::set_error(FSS_ERR_INVALID, "fss_pharm_self_overlap: pts_f16 must be 0 or 1");
   FSS_GUARD(fss::pharm_self_launch(anc, vec, off, n_mol, max_features, directional, extended,
-                                   out, S(stream)));
+                                   pts_f16, out, S(stream)));
 }
 
 int fss_seeds(const float* ref_pts, const int32_t* ref_off, const float* fit_pts,
               const int32_t* fit_off, const int32_t* pair_ref, const int32_t* pair_fit,
               int32_t n_pairs, int32_t n_seeds, const float* fibo_q, int32_t n_fibo,
-              float* seed_q, float* seed_t, void* stream) {
+              int32_t fit_f16, float* seed_q, float* seed_t, void* stream) {
+  if (fit_f16 != 0 && fit_f16 != 1)
+    return fss::set_error(FSS_ERR_INVALID, "fss_seeds: fit_f16 must be 0 or 1");
   FSS_GUARD(fss::seeds_launch(ref_pts, ref_off, fit_pts, fit_off, pair_ref, pair_fit, n_pairs,
-                              n_seeds, fibo_q, n_fibo, seed_q, seed_t, S(stream)));
+                              n_seeds, fibo_q, n_fibo, fit_f16, seed_q, seed_t, S(stream)));
 }
 
 int fss_align(const fss_align_desc* desc, void* stream) {

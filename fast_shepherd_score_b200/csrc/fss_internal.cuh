@@ -1,5 +1,6 @@
 // fss_internal.cuh -- host/device plumbing shared by the libfss_cuda translation units.
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -17,6 +18,38 @@ constexpr int kMaxPoints = 4096;
 // Thread-local error message + status helpers (fss_capi.cu).
 int set_error(int code, const std::string& msg);
 int check_launch(const char* what);
+
+// A packed cloud in global memory: float32 (x, y, z, w) points, or float16 (x, y, z, w)
+// points (8 bytes each, a library kept in float16 on the device) that are widened here, in
+// the staging loads.  Only staging code reads through it; the pairwise loops read the
+// staged float32 copies in shared memory.  The format flag is uniform across a launch.
+struct Pts {
+  const void* base;
+  int f16;
+  __host__ __device__ Pts() : base(nullptr), f16(0) {}
+  __host__ __device__ Pts(const float4* p) : base(p), f16(0) {}  // NOLINT: implicit on purpose
+  __host__ __device__ Pts(const void* p, int half) : base(p), f16(half) {}
+  __device__ __forceinline__ float4 operator[](int i) const {
+    if (!f16) return reinterpret_cast<const float4*>(base)[i];
+    const uint2 raw = reinterpret_cast<const uint2*>(base)[i];
+    const float2 xy = __half22float2(*reinterpret_cast<const __half2*>(&raw.x));
+    const float2 zw = __half22float2(*reinterpret_cast<const __half2*>(&raw.y));
+    return make_float4(xy.x, xy.y, zw.x, zw.y);
+  }
+  // A pharmacophore anchor: float32 storage carries the type in w's bits, float16 storage
+  // carries it as a (small, exact) float16 value.
+  __device__ __forceinline__ float4 anchor(int i) const {
+    float4 a = (*this)[i];
+    if (f16) a.w = __int_as_float(__float2int_rn(a.w));
+    return a;
+  }
+  __host__ __device__ Pts operator+(int o) const {
+    if (!base) return *this;
+    return f16 ? Pts(reinterpret_cast<const uint2*>(base) + o, 1)
+               : Pts(reinterpret_cast<const float4*>(base) + o, 0);
+  }
+  __host__ __device__ explicit operator bool() const { return base != nullptr; }
+};
 
 // Block-wide sum of a float3 (blockDim.x a multiple of 32, <= 1024); every thread gets it.
 __device__ __forceinline__ float3 block_sum3(float3 v, float* red) {
@@ -38,7 +71,7 @@ __device__ __forceinline__ float3 block_sum3(float3 v, float* red) {
 // Centroid of n packed points; every thread of the block gets it.  The sum has a fixed order
 // (lane-strided partial sums of warp 0, then a butterfly), so the centroid -- and the rounding
 // of everything staged relative to it -- does not depend on the CTA size of the launch.
-__device__ __forceinline__ float3 block_centroid(const float4* __restrict__ g, int n, float* red) {
+__device__ __forceinline__ float3 block_centroid(const Pts g, int n, float* red) {
   float3 s = make_float3(0.f, 0.f, 0.f);
   if (threadIdx.x < 32) {
     for (int i = threadIdx.x; i < n; i += 32) {
@@ -63,7 +96,7 @@ __device__ __forceinline__ float3 block_centroid(const float4* __restrict__ g, i
 //   sPd[2i] = (2k a.x, 2k a.x, 2k a.y, 2k a.y), sPd[2i+1] = (2k a.z, 2k a.z, P.w, P.w)
 // with P.w = -k|a|^2 - e c^2, and for ESP sQd[i] = (2 e c_i, 2 e c_i).
 template <bool ESP>
-__device__ __forceinline__ void stage_ref(const float4* __restrict__ g, int n, float3 c, float k,
+__device__ __forceinline__ void stage_ref(const Pts g, int n, float3 c, float k,
                                           float e, float4* sPd, float2* sQd) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     const float4 p = g[i];
@@ -79,7 +112,7 @@ __device__ __forceinline__ void stage_ref(const float4* __restrict__ g, int n, f
   }
 }
 
-__device__ __forceinline__ void stage_copy(const float4* __restrict__ g, int n, float4* s) {
+__device__ __forceinline__ void stage_copy(const Pts g, int n, float4* s) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) s[i] = g[i];
 }
 
@@ -91,11 +124,10 @@ __device__ __forceinline__ float clamp_type(float w) {
 }
 
 // Reference pharmacophores: anchors centred on c (type bits kept), unit vectors.
-__device__ __forceinline__ void stage_ref_pharm(const float4* __restrict__ ga,
-                                                const float4* __restrict__ gv, int n, float3 c,
+__device__ __forceinline__ void stage_ref_pharm(const Pts ga, const Pts gv, int n, float3 c,
                                                 float4* sA, float4* sV) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const float4 a = ga[i];
+    const float4 a = ga.anchor(i);
     sA[i] = make_float4(a.x - c.x, a.y - c.y, a.z - c.z, clamp_type(a.w));
     if (gv) {
       const float4 v = gv[i];
@@ -107,11 +139,10 @@ __device__ __forceinline__ void stage_ref_pharm(const float4* __restrict__ ga,
 }
 
 // Fit pharmacophores in their body frame: anchors as given, unit vectors.
-__device__ __forceinline__ void stage_fit_pharm(const float4* __restrict__ ga,
-                                                const float4* __restrict__ gv, int n,
+__device__ __forceinline__ void stage_fit_pharm(const Pts ga, const Pts gv, int n,
                                                 float4* sA, float4* sV) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const float4 a = ga[i];
+    const float4 a = ga.anchor(i);
     sA[i] = make_float4(a.x, a.y, a.z, clamp_type(a.w));
     if (gv) {
       const float4 v = gv[i];
@@ -134,8 +165,8 @@ int align_launch(const fss_align_desc* d, cudaStream_t st);
 int pick_best_launch(const float* rs, const float* rq, const float* rt, int P, int S, float* os,
                      float* oq, float* ot, cudaStream_t st);
 int self_overlap_launch(const float* pts, const int32_t* off, int n_mol, int max_n, float alpha,
-                        int esp, float inv_lam, float* out, cudaStream_t st);
+                        int esp, float inv_lam, int f16, float* out, cudaStream_t st);
 int pharm_self_launch(const float* anc, const float* vec, const int32_t* off, int n_mol, int max_n,
-                      int directional, int extended, float* out, cudaStream_t st);
+                      int directional, int extended, int f16, float* out, cudaStream_t st);
 
 }  // namespace fss

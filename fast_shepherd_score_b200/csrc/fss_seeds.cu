@@ -87,7 +87,7 @@ __device__ void sym3x3_axes(const M3& A, M3& out) {
 }
 
 // Inertia tensor about the fp64 centroid of n points (_masked_principal_axes, :258-278).
-__device__ void inertia(const float4* __restrict__ pts, int n, double shift_x, double shift_y,
+__device__ void inertia(const Pts pts, int n, double shift_x, double shift_y,
                         double shift_z, M3& I) {
   double cx = 0, cy = 0, cz = 0;
   for (int i = 0; i < n; ++i) {
@@ -129,7 +129,7 @@ __device__ void quat_rot(const T q_in[4], T R[3][3]) {
 }
 
 __global__ void seeds_kernel(const float4* __restrict__ rp, const int* __restrict__ roff,
-                             const float4* __restrict__ fp, const int* __restrict__ foff,
+                             const Pts fp, const int* __restrict__ foff,
                              const int* __restrict__ pair_ref, const int* __restrict__ pair_fit,
                              int P, int S, const float* __restrict__ fibo, int n_fibo,
                              float* __restrict__ sq, float* __restrict__ st) {
@@ -144,7 +144,7 @@ __global__ void seeds_kernel(const float4* __restrict__ rp, const int* __restric
   }
   const int ri = pair_ref[pi], fi = pair_fit[pi];
   const float4* A = rp + roff[ri];
-  const float4* B = fp + foff[fi];
+  const Pts B = fp + foff[fi];
   const int N = roff[ri + 1] - roff[ri], M = foff[fi + 1] - foff[fi];
   // float32 centroids (the COM used by the translations)
   float rc[3] = {0.f, 0.f, 0.f}, fc[3] = {0.f, 0.f, 0.f};
@@ -261,7 +261,7 @@ __global__ void seeds_kernel(const float4* __restrict__ rp, const int* __restric
 
 int seeds_launch(const float* ref_pts, const int32_t* ref_off, const float* fit_pts,
                  const int32_t* fit_off, const int32_t* pair_ref, const int32_t* pair_fit,
-                 int P, int S, const float* fibo, int n_fibo, float* sq, float* st,
+                 int P, int S, const float* fibo, int n_fibo, int fit_f16, float* sq, float* st,
                  cudaStream_t stream) {
   if (P < 0 || S < 1 || S > 64 || (S > 1 && S < 5))
     return set_error(FSS_ERR_INVALID, "fss_seeds: n_seeds must be 1 or in [5, 64]");
@@ -271,8 +271,8 @@ int seeds_launch(const float* ref_pts, const int32_t* ref_off, const float* fit_
   if (!ref_pts || !ref_off || !fit_pts || !fit_off || !pair_ref || !pair_fit || !sq || !st)
     return set_error(FSS_ERR_INVALID, "fss_seeds: null pointer");
   seeds_kernel<<<(P + 63) / 64, 64, 0, stream>>>(
-      reinterpret_cast<const float4*>(ref_pts), ref_off, reinterpret_cast<const float4*>(fit_pts),
-      fit_off, pair_ref, pair_fit, P, S, fibo, n_fibo, sq, st);
+      reinterpret_cast<const float4*>(ref_pts), ref_off, Pts(fit_pts, fit_f16 ? 1 : 0), fit_off,
+      pair_ref, pair_fit, P, S, fibo, n_fibo, sq, st);
   return check_launch("fss_seeds");
 }
 

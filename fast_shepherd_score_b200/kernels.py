@@ -152,12 +152,21 @@ def tanimoto_adam_step(V, dQ, dT, U, q, t, mq, vq, mt, vt, best, bq, bt, lr):
 # ------------------------------------------------------------------------------------------
 # Packed layout kernels
 # ------------------------------------------------------------------------------------------
+def points(t: torch.Tensor, name: str = "points"):
+    """(device pointer, float16 flag) of packed (n, 4) points: float32, or float16 for a
+    library kept in float16 (the kernels widen it in their staging loads)."""
+    if isinstance(t, torch.Tensor) and t.dtype == torch.float16:
+        return ptr(t, torch.float16, name), 1
+    return ptr(t, _f32, name), 0
+
+
 def self_overlap(cs: CloudSet, alpha: float, esp: bool = False, lam: Optional[float] = None):
     """Per-molecule self overlap of a packed cloud set (shape, or ESP with lam)."""
     out = torch.empty(cs.n_mol, dtype=_f32, device=cs.device)
     inv_lam = 1.0 / float(lam) if esp else 0.0
-    check(_lib.load().fss_self_overlap(ptr(cs.pts, _f32), ptr(cs.off, _i32), cs.n_mol,
-                                       cs.max_points, float(alpha), int(esp), inv_lam, ptr(out),
+    pts, f16 = points(cs.pts, "cloud points")
+    check(_lib.load().fss_self_overlap(pts, ptr(cs.off, _i32), cs.n_mol, cs.max_points,
+                                       float(alpha), int(esp), inv_lam, f16, ptr(out),
                                        stream_ptr(cs.device)), "self_overlap")
     return out
 
@@ -167,10 +176,14 @@ def pharm_self_overlap(ps: PharmSet, directional: bool = True, extended: int = 0
     anchors) or 2 (extended points only), as batch_pharm_self_overlap
     (accel/drivers/pharm_overlap.py:413)."""
     out = torch.empty(ps.n_mol, dtype=_f32, device=ps.anc.device)
-    check(_lib.load().fss_pharm_self_overlap(ptr(ps.anc, _f32), ptr(ps.vec, _f32),
-                                             ptr(ps.off, _i32), ps.n_mol, ps.max_points,
-                                             int(directional), int(extended), ptr(out),
-                                             stream_ptr(ps.anc.device)), "pharm_self_overlap")
+    anc, f16 = points(ps.anc, "pharmacophore anchors")
+    vec, vf16 = points(ps.vec, "pharmacophore vectors")
+    if vf16 != f16:
+        raise ValueError("pharmacophore anchors and vectors must share one dtype")
+    check(_lib.load().fss_pharm_self_overlap(anc, vec, ptr(ps.off, _i32), ps.n_mol,
+                                             ps.max_points, int(directional), int(extended), f16,
+                                             ptr(out), stream_ptr(ps.anc.device)),
+          "pharm_self_overlap")
     return out
 
 
@@ -229,8 +242,10 @@ def seeds(ref: CloudSet, fit: CloudSet, pair_ref, pair_fit, num_seeds: int):
     fibo = _fibo_device(n_fibo, dev) if n_fibo else None
     sq = torch.empty(P, S, 4, dtype=_f32, device=dev)
     st = torch.empty(P, S, 3, dtype=_f32, device=dev)
-    check(_lib.load().fss_seeds(ptr(ref.pts, _f32), ptr(ref.off, _i32), ptr(fit.pts, _f32),
+    fit_pts, fit_f16 = points(fit.pts, "fit points")
+    check(_lib.load().fss_seeds(ptr(ref.pts, _f32, "ref points"), ptr(ref.off, _i32), fit_pts,
                                 ptr(fit.off, _i32), ptr(pair_ref, _i32), ptr(pair_fit, _i32), P,
-                                S, ptr(fibo, _f32), n_fibo, ptr(sq), ptr(st), stream_ptr(dev)),
+                                S, ptr(fibo, _f32), n_fibo, fit_f16, ptr(sq), ptr(st),
+                                stream_ptr(dev)),
           "seeds")
     return sq, st

@@ -21,7 +21,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 import torch
 
-from . import api
+from . import api, library
 from .layout import CloudSet, PharmSet, _offsets
 from .modes import canonical, seeds_for, steps_for
 from .store import ProfileStore  # noqa: F401  (re-exported: the screening entry points take it)
@@ -46,75 +46,45 @@ def ALPHA(num_points):
 # Device-side shard expansion
 # -----------------------------------------------------------------------------------------
 def _dev(a, device, dtype=torch.float32):
-    """Upload an array in its stored dtype (float16 halves the copy), widen on the device."""
-    t = torch.from_numpy(np.ascontiguousarray(a))
-    if torch.cuda.is_available():
-        t = t.pin_memory()
-    return t.to(device, non_blocking=True).to(dtype)
+    """Upload an array in its stored dtype, then convert on the device (radii only)."""
+    return library.upload(a, device).to(dtype)
 
 
-def _cloud_from_csr(pos, off, device, w=None) -> CloudSet:
-    off = np.asarray(off, np.int64)
-    n = np.diff(off)
-    pts = torch.zeros(int(off[-1]), 4, device=device)
-    pts[:, :3] = _dev(pos, device)
-    if w is not None:
-        pts[:, 3] = _dev(w, device)
-    return CloudSet(pts, torch.from_numpy(off.astype(np.int32)).to(device), n,
-                    int(n.max()) if len(n) else 0)
+# the fit sets the fused kernel reads directly keep a float16 store's dtype on the device (the
+# kernels widen it while staging); the pharmacophore mode re-centres its anchors and the
+# ShaEP combo mode has no float16 form, so those two widen on upload
+_KEEP_HALF = ("vol", "vol_esp", "surf", "surf_esp", "vol_color", "vol_pharm")
 
 
-def _cloud_from_dense(pos, device, w=None) -> CloudSet:
-    K, S, _ = pos.shape
-    pts = torch.zeros(K * S, 4, device=device)
-    pts[:, :3] = _dev(pos.reshape(-1, 3), device)
-    if w is not None:
-        pts[:, 3] = _dev(w.reshape(-1), device)
-    counts = np.full(K, S, np.int64)
-    return CloudSet(pts, torch.from_numpy(_offsets(counts)).to(device), counts, S)
-
-
-def _pharm_from_csr(types, ancs, vecs, off, device, with_vectors=True) -> PharmSet:
-    off = np.asarray(off, np.int64)
-    n = np.diff(off)
-    total = int(off[-1])
-    anc = torch.zeros(total, 4, device=device)
-    anc[:, :3] = _dev(ancs, device)
-    ty = np.asarray(types).astype(np.int64)
-    ty = np.where((ty < 0) | (ty > 8), 8, ty).astype(np.int32)
-    anc[:, 3] = torch.from_numpy(ty).to(device).view(torch.float32)
-    vec = torch.zeros(total, 4, device=device)
-    if with_vectors and vecs is not None:
-        vec[:, :3] = _dev(vecs, device)
-    return PharmSet(anc, vec, torch.from_numpy(off.astype(np.int32)).to(device), n,
-                    int(n.max()) if len(n) else 0)
-
-
-def shard_to_device(arrs: dict, mode: str, device, alpha: float = 0.81):
+def shard_to_device(arrs: dict, mode: str, device, alpha: float = 0.81, widen: bool = False):
     """(fit CloudSet or None, fit PharmSet or None, extra kwargs) of one shard for `mode`;
-    vol_and_surf_esp adds the atoms with hydrogens, their radii and the surfaces."""
+    vol_and_surf_esp adds the atoms with hydrogens, their radii and the surfaces.  Columns
+    of a float16 store stay float16 for the modes in ``_KEEP_HALF`` unless ``widen``."""
+    widen = widen or mode not in _KEEP_HALF
+    csr, dense = library.cloud_from_csr, library.cloud_from_dense
     if mode == "vol_and_surf_esp":
         # shape centres: heavy atoms at alpha 0.81, else the surface (aligners.py:795-803)
-        surf = _cloud_from_dense(arrs["surf_pos"], device, arrs["surf_esp"])
-        cs = (_cloud_from_csr(arrs["atom_pos"], arrs["atom_off"], device) if alpha == 0.81
-              else _cloud_from_dense(arrs["surf_pos"], device))
-        atoms = _cloud_from_csr(arrs["cwh"], arrs["all_off"], device, arrs["charges"])
+        surf = dense(arrs["surf_pos"], device, arrs["surf_esp"], widen=True)
+        cs = (csr(arrs["atom_pos"], arrs["atom_off"], device, widen=True) if alpha == 0.81
+              else dense(arrs["surf_pos"], device, widen=True))
+        atoms = csr(arrs["cwh"], arrs["all_off"], device, arrs["charges"], widen=True)
         return cs, None, dict(fit_atoms=atoms, fit_radii=_dev(arrs["radii"], device),
                               fit_surf=surf)
     if mode in ("vol", "vol_color", "vol_pharm"):
-        cs = _cloud_from_csr(arrs["atom_pos"], arrs["atom_off"], device)
+        cs = csr(arrs["atom_pos"], arrs["atom_off"], device, widen=widen)
     elif mode == "vol_esp":
-        cs = _cloud_from_csr(arrs["atom_pos"], arrs["atom_off"], device, arrs["charges"])
+        cs = csr(arrs["atom_pos"], arrs["atom_off"], device, arrs["charges"], widen=widen)
     elif mode == "surf":
-        cs = _cloud_from_dense(arrs["surf_pos"], device)
+        cs = dense(arrs["surf_pos"], device, widen=widen)
     elif mode == "surf_esp":
-        cs = _cloud_from_dense(arrs["surf_pos"], device, arrs["surf_esp"])
+        cs = dense(arrs["surf_pos"], device, arrs["surf_esp"], widen=widen)
     else:
         cs = None
     ps = None
     if mode in ("pharm", "vol_color", "vol_pharm"):
-        ps = _pharm_from_csr(arrs["pharm_types"], arrs["pharm_ancs"], arrs["pharm_vecs"],
-                             arrs["pharm_off"], device, with_vectors=(mode != "vol_color"))
+        ps = library.pharm_from_csr(arrs["pharm_types"], arrs["pharm_ancs"], arrs["pharm_vecs"],
+                                    arrs["pharm_off"], device,
+                                    with_vectors=(mode != "vol_color"), widen=widen)
     return cs, ps, {}
 
 
@@ -216,6 +186,9 @@ def _batch_kwargs(mode, ak, alpha):
         kw.update(alpha=alpha, lam=ak.get("lam", 0.001),
                   probe_radius=ak.get("probe_radius", 1.0),
                   esp_weight=ak.get("esp_weight", 0.5), esp_stride=ak.get("esp_stride", 1))
+    # an explicit kernel tile (lanes_per_pose, chunks, ...) passes through to the launch
+    from .align import TILE_KEYS
+    kw.update({k: int(ak[k]) for k in TILE_KEYS if ak.get(k)})
     return kw
 
 
@@ -239,7 +212,8 @@ def _screen_shards(qs, store: ProfileStore, mode: str, shards, kw: dict, ak: dic
         sh, arrs = store.read_shard(si)
         if center and not store.pre_centered:
             arrs = _center_shard(arrs, mode)
-        fit, fit_ph, fit_x = shard_to_device(arrs, mode, device, alpha)
+        # the translation-seeded grid reads the fit clouds on the host side: float32 there
+        fit, fit_ph, fit_x = shard_to_device(arrs, mode, device, alpha, widen=trans)
         K = int(sh["n"])
         pr = torch.zeros(K, dtype=torch.int32, device=device)
         pf = torch.arange(K, dtype=torch.int32, device=device)

@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define FSS_ABI_VERSION 2
+#define FSS_ABI_VERSION 3
 
 enum fss_status {
   FSS_OK = 0,
@@ -94,30 +94,40 @@ int fss_tanimoto_adam_step(const float *V, const float *dQ, const float *dT, con
  * Packed clouds (float4 + offsets) used by the fused alignment and the screening server.
  * ------------------------------------------------------------------------------------- */
 
+/* Point formats.  A packed cloud is float32 (x, y, z, w) per point, 16 bytes.  Where an
+ * argument is marked "f16-capable", a flag selects float16 (x, y, z, w) points instead,
+ * 8 bytes each (a screening library kept in float16 on the device, as the ProfileStore
+ * format's default dtype stores it); the kernels widen them to float32 in their staging
+ * loads.  Pharmacophore anchors in float16 carry the type as a float16 value in w (float32
+ * anchors carry the int32 type in w's bits); vectors are (vx, vy, vz, 0) in either format. */
+
 /* Self overlap per molecule at the identity pose (shape, or ESP when esp != 0 with
  * inv_lam = 1/lam).  Replaces _batch_self_overlap / _batch_self_overlap_esp
  * (shape_triton.py:436-448, esp_triton.py:393-425).  out (n_mol); max_points bounds every
- * molecule's count (a larger molecule gets NaN). */
+ * molecule's count (a larger molecule gets NaN).  pts is f16-capable (pts_f16 = 1). */
 int fss_self_overlap(const float *pts, const int32_t *off, int32_t n_mol, int32_t max_points,
-                     float alpha, int32_t esp, float inv_lam, float *out, void *stream);
+                     float alpha, int32_t esp, float inv_lam, int32_t pts_f16, float *out,
+                     void *stream);
 
 /* Pharmacophore self overlap per molecule (directional or colour tables); `extended` 0/1/2
  * as fss_align_desc.pharm_extended (directional tables only).
  * Replaces the identity-pose self overlaps of accel/drivers/pharm.py:336-346 and
- * batch_pharm_self_overlap (accel/drivers/pharm_overlap.py:413-439). */
+ * batch_pharm_self_overlap (accel/drivers/pharm_overlap.py:413-439).  anc and vec are
+ * f16-capable (pts_f16 = 1). */
 int fss_pharm_self_overlap(const float *anc, const float *vec, const int32_t *off,
                            int32_t n_mol, int32_t max_features, int32_t directional,
-                           int32_t extended, float *out, void *stream);
+                           int32_t extended, int32_t pts_f16, float *out, void *stream);
 
 /* Multi-start seeds for P pairs: identity, 4 PCA alignments (fp64 closed-form eigensolver),
  * up to 6 structured +-90 degree axis swaps, then the Fibonacci set `fibo_q` (n_fibo,4)
  * supplied by the caller, each with a COM-aligning translation; degenerate pairs
  * (< 3 points or non-finite) take the fixed fallback set.  Replaces batched_seeds_torch
- * (accel/drivers/_common.py:281-441).  seed_q (P,S,4), seed_t (P,S,3). */
+ * (accel/drivers/_common.py:281-441).  seed_q (P,S,4), seed_t (P,S,3).  fit_pts is
+ * f16-capable (fit_f16 = 1). */
 int fss_seeds(const float *ref_pts, const int32_t *ref_off, const float *fit_pts,
               const int32_t *fit_off, const int32_t *pair_ref, const int32_t *pair_fit,
               int32_t n_pairs, int32_t n_seeds, const float *fibo_q, int32_t n_fibo,
-              float *seed_q, float *seed_t, void *stream);
+              int32_t fit_f16, float *seed_q, float *seed_t, void *stream);
 
 /* Descriptor of one fused alignment launch (all pairs x starts x Adam steps). */
 typedef struct fss_align_desc {
@@ -190,6 +200,9 @@ typedef struct fss_align_desc {
   /* scratch: two device int32 -- [0] work counter, [1] status flags (bit 0: a pair was
    * larger than the max_* extents).  The launch zeroes both on `stream`. */
   int32_t *scratch;
+  /* 1: fit_pts, fit_anc and fit_vec are float16 points (f16-capable, see "Point formats");
+   * not in mode ESP_COMBO.  0: float32. */
+  int32_t fit_f16;
 } fss_align_desc;
 
 /* Fused persistent alignment: every (pair, start) pose runs all `steps` Adam steps inside

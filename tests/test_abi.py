@@ -26,7 +26,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_limits():
     lib = _lib.load()
-    assert lib.fss_abi_version() == 2
+    assert lib.fss_abi_version() == 3
     assert lib.fss_max_points() >= 1024
 
 
@@ -49,5 +49,5 @@ def test_invalid_arguments_raise_without_gpu():
     rc = lib.fss_pick_best(None, None, None, -1, 1, None, None, None, None)
     assert rc == _lib.FSS_ERR_INVALID
     assert b"fss_pick_best" in lib.fss_last_error()
-    rc = lib.fss_seeds(None, None, None, None, None, None, 4, 3, None, 0, None, None, None)
+    rc = lib.fss_seeds(None, None, None, None, None, None, 4, 3, None, 0, 0, None, None, None)
     assert rc == _lib.FSS_ERR_INVALID
