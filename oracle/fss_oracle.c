@@ -79,37 +79,55 @@ static void parallel_for(int n, int nthreads, int chunk, range_fn fn, void *ctx)
 #define B2 0.999
 #define ADAM_EPS 1e-8
 
+/* Precision of the per-pose overlap sums.  The default build (libfss_oracle.so) evaluates
+ * them in double as numba does.  Built with -DFSSO_ACC32 (libfss_oracle_f32.so), the terms,
+ * exp and every accumulation of pose_overlap / pose_pharm run in float instead -- the
+ * precision of the reference's Triton kernels, which accumulate their tiles in fp32
+ * (accel/kernels/shape_triton.py:114-177, pharm_triton.py:296-400).  Comparing the two
+ * builds measures how far two correct precisions of the same algorithm drift apart over a
+ * fine loop; the parity tests use it as the floor for the CUDA path's own drift. */
+#define ACC(x) ((acc_t)(x))
+#ifdef FSSO_ACC32
+typedef float acc_t;
+#define ACC_EXP expf
+#define ACC_ABS fabsf
+#else
+typedef double acc_t;
+#define ACC_EXP exp
+#define ACC_ABS fabs
+#endif
+
 enum { FSSO_SHAPE = 0, FSSO_ESP = 1, FSSO_PHARM = 2, FSSO_COMBO = 3, FSSO_COLOR_COMBO = 4 };
 
 static const double K_PI15 = 5.568327996831708; /* pi ** 1.5 */
 
 /* Rotation matrix from a (w,x,y,z) quaternion, as cpu.py:56-58 (q assumed unit). */
-static inline void rotmat(const float *q, double R[9]) {
+static inline void rotmat(const float *q, acc_t R[9]) {
     const float qr = q[0], qi = q[1], qj = q[2], qk = q[3];
-    R[0] = 1.0 - 2.0 * (double)(qj * qj + qk * qk);
-    R[1] = 2.0 * (double)(qi * qj - qk * qr);
-    R[2] = 2.0 * (double)(qi * qk + qj * qr);
-    R[3] = 2.0 * (double)(qi * qj + qk * qr);
-    R[4] = 1.0 - 2.0 * (double)(qi * qi + qk * qk);
-    R[5] = 2.0 * (double)(qj * qk - qi * qr);
-    R[6] = 2.0 * (double)(qi * qk - qj * qr);
-    R[7] = 2.0 * (double)(qj * qk + qi * qr);
-    R[8] = 1.0 - 2.0 * (double)(qi * qi + qj * qj);
+    R[0] = ACC(1.0) - ACC(2.0) * (acc_t)(qj * qj + qk * qk);
+    R[1] = ACC(2.0) * (acc_t)(qi * qj - qk * qr);
+    R[2] = ACC(2.0) * (acc_t)(qi * qk + qj * qr);
+    R[3] = ACC(2.0) * (acc_t)(qi * qj + qk * qr);
+    R[4] = ACC(1.0) - ACC(2.0) * (acc_t)(qi * qi + qk * qk);
+    R[5] = ACC(2.0) * (acc_t)(qj * qk - qi * qr);
+    R[6] = ACC(2.0) * (acc_t)(qi * qk - qj * qr);
+    R[7] = ACC(2.0) * (acc_t)(qj * qk + qi * qr);
+    R[8] = ACC(1.0) - ACC(2.0) * (acc_t)(qi * qi + qj * qj);
 }
 
 /* d(R(q) b)/dq contracted with a force f, body-frame point b (cpu.py:80-83). */
-static inline void quat_tail(const double f[3], double bx, double by, double bz,
-                             const float *q, double dQ[4]) {
-    const double qr = q[0], qi = q[1], qj = q[2], qk = q[3];
-    const double fx = f[0], fy = f[1], fz = f[2];
-    dQ[0] += fx * (-2.0 * qk * by + 2.0 * qj * bz) + fy * (2.0 * qk * bx - 2.0 * qi * bz)
-           + fz * (-2.0 * qj * bx + 2.0 * qi * by);
-    dQ[1] += fx * (2.0 * qj * by + 2.0 * qk * bz) + fy * (2.0 * qj * bx - 4.0 * qi * by - 2.0 * qr * bz)
-           + fz * (2.0 * qk * bx + 2.0 * qr * by - 4.0 * qi * bz);
-    dQ[2] += fx * (-4.0 * qj * bx + 2.0 * qi * by + 2.0 * qr * bz) + fy * (2.0 * qi * bx + 2.0 * qk * bz)
-           + fz * (-2.0 * qr * bx + 2.0 * qk * by - 4.0 * qj * bz);
-    dQ[3] += fx * (-4.0 * qk * bx - 2.0 * qr * by + 2.0 * qi * bz) + fy * (2.0 * qr * bx - 4.0 * qk * by + 2.0 * qj * bz)
-           + fz * (2.0 * qi * bx + 2.0 * qj * by);
+static inline void quat_tail(const acc_t f[3], acc_t bx, acc_t by, acc_t bz,
+                             const float *q, acc_t dQ[4]) {
+    const acc_t qr = q[0], qi = q[1], qj = q[2], qk = q[3];
+    const acc_t fx = f[0], fy = f[1], fz = f[2];
+    dQ[0] += fx * (-ACC(2.0) * qk * by + ACC(2.0) * qj * bz) + fy * (ACC(2.0) * qk * bx - ACC(2.0) * qi * bz)
+           + fz * (-ACC(2.0) * qj * bx + ACC(2.0) * qi * by);
+    dQ[1] += fx * (ACC(2.0) * qj * by + ACC(2.0) * qk * bz) + fy * (ACC(2.0) * qj * bx - ACC(4.0) * qi * by - ACC(2.0) * qr * bz)
+           + fz * (ACC(2.0) * qk * bx + ACC(2.0) * qr * by - ACC(4.0) * qi * bz);
+    dQ[2] += fx * (-ACC(4.0) * qj * bx + ACC(2.0) * qi * by + ACC(2.0) * qr * bz) + fy * (ACC(2.0) * qi * bx + ACC(2.0) * qk * bz)
+           + fz * (-ACC(2.0) * qr * bx + ACC(2.0) * qk * by - ACC(4.0) * qj * bz);
+    dQ[3] += fx * (-ACC(4.0) * qk * bx - ACC(2.0) * qr * by + ACC(2.0) * qi * bz) + fy * (ACC(2.0) * qr * bx - ACC(4.0) * qk * by + ACC(2.0) * qj * bz)
+           + fz * (ACC(2.0) * qi * bx + ACC(2.0) * qj * by);
 }
 
 /* One pose of the shape / ESP overlap with its SE(3) gradient.
@@ -117,36 +135,38 @@ static inline void quat_tail(const double f[3], double bx, double by, double bz,
  * Mirrors cpu.py:52-86 and cpu.py:166-199. */
 static void pose_overlap(const float *A, const float *B, const float *CA, const float *CB,
                          const float *q, const float *t, int n_real, int m_real,
-                         double alpha, double inv_lam, int need_grad,
-                         double *V, double dQ[4], double dT[3]) {
-    const double Kc = K_PI15 / pow(2.0 * alpha, 1.5);
-    const double a2 = alpha / 2.0;
-    double R[9];
+                         double alpha_d, double inv_lam_d, int need_grad,
+                         double *V, double dQ_out[4], double dT_out[3]) {
+    const acc_t alpha = (acc_t)alpha_d, inv_lam = (acc_t)inv_lam_d;
+    acc_t dQ[4], dT[3];
+    const acc_t Kc = (acc_t)K_PI15 / (acc_t)pow(ACC(2.0) * (double)alpha, ACC(1.5));
+    const acc_t a2 = alpha / ACC(2.0);
+    acc_t R[9];
     rotmat(q, R);
-    const double tx = t[0], ty = t[1], tz = t[2];
-    double Vacc = 0.0;
-    dT[0] = dT[1] = dT[2] = 0.0;
-    dQ[0] = dQ[1] = dQ[2] = dQ[3] = 0.0;
+    const acc_t tx = t[0], ty = t[1], tz = t[2];
+    acc_t Vacc = ACC(0.0);
+    dT[0] = dT[1] = dT[2] = ACC(0.0);
+    dQ[0] = dQ[1] = dQ[2] = dQ[3] = ACC(0.0);
     for (int m = 0; m < m_real; ++m) {
-        const double bx0 = B[3 * m], by0 = B[3 * m + 1], bz0 = B[3 * m + 2];
-        const double bx = R[0] * bx0 + R[1] * by0 + R[2] * bz0 + tx;
-        const double by = R[3] * bx0 + R[4] * by0 + R[5] * bz0 + ty;
-        const double bz = R[6] * bx0 + R[7] * by0 + R[8] * bz0 + tz;
-        double f[3] = {0.0, 0.0, 0.0};
+        const acc_t bx0 = B[3 * m], by0 = B[3 * m + 1], bz0 = B[3 * m + 2];
+        const acc_t bx = R[0] * bx0 + R[1] * by0 + R[2] * bz0 + tx;
+        const acc_t by = R[3] * bx0 + R[4] * by0 + R[5] * bz0 + ty;
+        const acc_t bz = R[6] * bx0 + R[7] * by0 + R[8] * bz0 + tz;
+        acc_t f[3] = {ACC(0.0), ACC(0.0), ACC(0.0)};
         const float cbm = CB ? CB[m] : 0.0f;
         for (int n = 0; n < n_real; ++n) {
-            const double dx = A[3 * n] - bx, dy = A[3 * n + 1] - by, dz = A[3 * n + 2] - bz;
-            const double r2 = dx * dx + dy * dy + dz * dz;
-            double g;
+            const acc_t dx = A[3 * n] - bx, dy = A[3 * n + 1] - by, dz = A[3 * n + 2] - bz;
+            const acc_t r2 = dx * dx + dy * dy + dz * dz;
+            acc_t g;
             if (CA) {
                 const float dc = CA[n] - cbm; /* float32 subtraction, as numba */
-                g = Kc * exp(-a2 * r2 - (double)(dc * dc) * inv_lam);
+                g = Kc * ACC_EXP(-a2 * r2 - (acc_t)(dc * dc) * inv_lam);
             } else {
-                g = Kc * exp(-a2 * r2);
+                g = Kc * ACC_EXP(-a2 * r2);
             }
             Vacc += g;
             if (need_grad) {
-                const double c = alpha * g;
+                const acc_t c = alpha * g;
                 f[0] += c * dx; f[1] += c * dy; f[2] += c * dz;
             }
         }
@@ -156,12 +176,14 @@ static void pose_overlap(const float *A, const float *B, const float *CA, const 
         }
     }
     *V = Vacc;
+    for (int c = 0; c < 4; ++c) dQ_out[c] = dQ[c];
+    for (int c = 0; c < 3; ++c) dT_out[c] = dT[c];
 }
 
-/* Unit vector with the 1e-12 norm floor of cpu.py:524-526. */
-static inline void unit_vec(const float *v, double out[3]) {
+/* Unit vector with the ACC(1e-12) norm floor of cpu.py:524-526. */
+static inline void unit_vec(const float *v, acc_t out[3]) {
     const float nrm = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-    const double inv = 1.0 / (nrm > 1e-12f ? (double)nrm : 1e-12);
+    const acc_t inv = ACC(1.0) / (nrm > 1e-12f ? (acc_t)nrm : ACC(1e-12));
     out[0] = v[0] * inv; out[1] = v[1] * inv; out[2] = v[2] * inv;
 }
 
@@ -178,44 +200,45 @@ static void pose_pharm(const float *A, const float *B, const float *RV, const fl
                        const int32_t *At, const int32_t *Bt, const float *q, const float *t,
                        int n_real, int m_real, const double *alphas, const double *Ks,
                        const int32_t *cats, int ext, int need_grad,
-                       double *O, double dQ[4], double dT[3]) {
-    double R[9];
+                       double *O, double dQ_out[4], double dT_out[3]) {
+    acc_t dQ[4], dT[3];
+    acc_t R[9];
     rotmat(q, R);
-    const double tx = t[0], ty = t[1], tz = t[2];
-    double Oacc = 0.0;
-    dT[0] = dT[1] = dT[2] = 0.0;
-    dQ[0] = dQ[1] = dQ[2] = dQ[3] = 0.0;
+    const acc_t tx = t[0], ty = t[1], tz = t[2];
+    acc_t Oacc = ACC(0.0);
+    dT[0] = dT[1] = dT[2] = ACC(0.0);
+    dQ[0] = dQ[1] = dQ[2] = dQ[3] = ACC(0.0);
     for (int i = 0; i < m_real; ++i) {
         const int ityp = Bt[i];
         const int icat = cats[ityp];
         if (icat == 3) continue;
-        const double ialpha = alphas[ityp], iK = Ks[ityp];
-        const double fax0 = B[3 * i], fay0 = B[3 * i + 1], faz0 = B[3 * i + 2];
-        double fv[3] = {0.0, 0.0, 0.0};
+        const acc_t ialpha = alphas[ityp], iK = Ks[ityp];
+        const acc_t fax0 = B[3 * i], fay0 = B[3 * i + 1], faz0 = B[3 * i + 2];
+        acc_t fv[3] = {ACC(0.0), ACC(0.0), ACC(0.0)};
         if (FV) unit_vec(FV + 3 * i, fv);
-        const double fatx = R[0] * fax0 + R[1] * fay0 + R[2] * faz0 + tx;
-        const double faty = R[3] * fax0 + R[4] * fay0 + R[5] * faz0 + ty;
-        const double fatz = R[6] * fax0 + R[7] * fay0 + R[8] * faz0 + tz;
-        const double fvtx = R[0] * fv[0] + R[1] * fv[1] + R[2] * fv[2];
-        const double fvty = R[3] * fv[0] + R[4] * fv[1] + R[5] * fv[2];
-        const double fvtz = R[6] * fv[0] + R[7] * fv[1] + R[8] * fv[2];
-        double f[3] = {0.0, 0.0, 0.0};   /* positional force sum_j alpha*K*w*E*(ref - rotfit) */
-        double wf[3] = {0.0, 0.0, 0.0};  /* weight force sum_j coeff * ref_vn */
-        double fe[3] = {0.0, 0.0, 0.0};  /* force at the extended point (ext != 0) */
+        const acc_t fatx = R[0] * fax0 + R[1] * fay0 + R[2] * faz0 + tx;
+        const acc_t faty = R[3] * fax0 + R[4] * fay0 + R[5] * faz0 + ty;
+        const acc_t fatz = R[6] * fax0 + R[7] * fay0 + R[8] * faz0 + tz;
+        const acc_t fvtx = R[0] * fv[0] + R[1] * fv[1] + R[2] * fv[2];
+        const acc_t fvty = R[3] * fv[0] + R[4] * fv[1] + R[5] * fv[2];
+        const acc_t fvtz = R[6] * fv[0] + R[7] * fv[1] + R[8] * fv[2];
+        acc_t f[3] = {ACC(0.0), ACC(0.0), ACC(0.0)};   /* positional force sum_j alpha*K*w*E*(ref - rotfit) */
+        acc_t wf[3] = {ACC(0.0), ACC(0.0), ACC(0.0)};  /* weight force sum_j coeff * ref_vn */
+        acc_t fe[3] = {ACC(0.0), ACC(0.0), ACC(0.0)};  /* force at the extended point (ext != 0) */
         const int use_ext = ext != 0 && (ityp == 0 || ityp == 1);
         for (int j = 0; j < n_real; ++j) {
             if (At[j] != ityp) continue;
-            const double dx = fatx - A[3 * j], dy = faty - A[3 * j + 1], dz = fatz - A[3 * j + 2];
-            const double r2 = dx * dx + dy * dy + dz * dz;
-            const double E = exp(-ialpha * 0.5 * r2);
-            double rv[3] = {0.0, 0.0, 0.0};
-            double w = 1.0, c = 0.0;
+            const acc_t dx = fatx - A[3 * j], dy = faty - A[3 * j + 1], dz = fatz - A[3 * j + 2];
+            const acc_t r2 = dx * dx + dy * dy + dz * dz;
+            const acc_t E = ACC_EXP(-ialpha * ACC(0.5) * r2);
+            acc_t rv[3] = {ACC(0.0), ACC(0.0), ACC(0.0)};
+            acc_t w = ACC(1.0), c = ACC(0.0);
             if (use_ext) {
                 unit_vec(RV + 3 * j, rv);
-                w = ext == 1 ? 1.0 : 0.0;
+                w = ext == 1 ? ACC(1.0) : ACC(0.0);
                 /* (rotfit + R v_fit) - (ref + v_ref), the sign convention of dx */
-                const double ex = dx + fvtx - rv[0], ey = dy + fvty - rv[1], ez = dz + fvtz - rv[2];
-                const double Ee = iK * exp(-ialpha * 0.5 * (ex * ex + ey * ey + ez * ez));
+                const acc_t ex = dx + fvtx - rv[0], ey = dy + fvty - rv[1], ez = dz + fvtz - rv[2];
+                const acc_t Ee = iK * ACC_EXP(-ialpha * ACC(0.5) * (ex * ex + ey * ey + ez * ez));
                 Oacc += Ee;
                 if (need_grad) {
                     fe[0] += -ialpha * Ee * ex; fe[1] += -ialpha * Ee * ey;
@@ -223,22 +246,22 @@ static void pose_pharm(const float *A, const float *B, const float *RV, const fl
                 }
             } else if (icat == 1 || icat == 2) {
                 unit_vec(RV + 3 * j, rv);
-                const double D = fvtx * rv[0] + fvty * rv[1] + fvtz * rv[2];
+                const acc_t D = fvtx * rv[0] + fvty * rv[1] + fvtz * rv[2];
                 if (icat == 1) {
-                    const double Dcl = D < 0.0 ? 0.0 : (D > 1.0 ? 1.0 : D);
-                    w = (Dcl + 2.0) / 3.0;
-                    c = (D > 0.0 && D < 1.0) ? 1.0 : 0.0;
+                    const acc_t Dcl = D < ACC(0.0) ? ACC(0.0) : (D > ACC(1.0) ? ACC(1.0) : D);
+                    w = (Dcl + ACC(2.0)) / ACC(3.0);
+                    c = (D > ACC(0.0) && D < ACC(1.0)) ? ACC(1.0) : ACC(0.0);
                 } else {
-                    w = (fabs(D) + 2.0) / 3.0;
-                    c = D > 0.0 ? 1.0 : (D < 0.0 ? -1.0 : 0.0);
+                    w = (ACC_ABS(D) + ACC(2.0)) / ACC(3.0);
+                    c = D > ACC(0.0) ? ACC(1.0) : (D < ACC(0.0) ? -ACC(1.0) : ACC(0.0));
                 }
             }
-            const double KwE = iK * w * E;
+            const acc_t KwE = iK * w * E;
             Oacc += KwE;
             if (need_grad) {
-                const double aKwE = -ialpha * KwE;
+                const acc_t aKwE = -ialpha * KwE;
                 f[0] += aKwE * dx; f[1] += aKwE * dy; f[2] += aKwE * dz;
-                const double coeff = (1.0 / 3.0) * iK * E * c;
+                const acc_t coeff = (ACC(1.0) / ACC(3.0)) * iK * E * c;
                 wf[0] += coeff * rv[0]; wf[1] += coeff * rv[1]; wf[2] += coeff * rv[2];
             }
         }
@@ -253,6 +276,8 @@ static void pose_pharm(const float *A, const float *B, const float *RV, const fl
         }
     }
     *O = Oacc;
+    for (int c = 0; c < 4; ++c) dQ_out[c] = dQ[c];
+    for (int c = 0; c < 3; ++c) dT_out[c] = dT[c];
 }
 
 /* ------------------------------------------------------------------------- */
@@ -581,7 +606,7 @@ static void to_double(const float *X, int n, double *out) {
 }
 
 static void transform(const float *X, int n, const float *q, const float *t, double *out) {
-    double R[9];
+    acc_t R[9];
     rotmat(q, R);
     for (int i = 0; i < n; ++i) {
         const double x = X[3 * i], y = X[3 * i + 1], z = X[3 * i + 2];

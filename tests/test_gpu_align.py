@@ -3,6 +3,8 @@ and the oracle.  An alignment counts as equal when its best score is within 1e-4
 reference's; Adam's normalised update amplifies fp32 rounding chaotically once a pose has
 converged, so trajectories are compared step-exact only for the first steps and by best
 score afterwards."""
+import math
+
 import numpy as np
 import pytest
 import torch
@@ -16,13 +18,42 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-4
 
 
-def assert_parity(got, ref, frac=0.75, worst=1e-3):
-    """Best-score parity: most pairs within 1e-4 of the reference, none more than `worst`
-    below it (a higher score is a better alignment found from the same seeds)."""
+def count_bound(c_ctl: int) -> float:
+    """Largest count of rare misses consistent with a control's count (Poisson tolerance)."""
+    return c_ctl + 3.0 * math.sqrt(max(c_ctl, 1)) + 2.0
+
+
+def control_scores(fn, *args, **kw):
+    """Per-pair best scores of the oracle driver ``fn`` run with its overlap sums in float
+    (the precision of the reference's Triton kernels): how far a second correct precision
+    of the same algorithm drifts from the double oracle."""
+    from oracle import _lib
+    with _lib.precision("f32"):
+        return np.asarray(fn(*args, **kw)[0], np.float64)
+
+
+def assert_parity(got, ref, ctl=None, worst=1e-3):
+    """Best-score parity of alignments: a pair is equal when its best score is within 1e-4 of
+    the reference's.  Adam's normalised update amplifies last-bit differences of a small
+    gradient component, so two correct implementations whose sums round differently end a
+    few alignments in different optima (measured at the workloads' sizes in
+    tests/test_gpu_config_parity.py, for this path and for the oracle with float sums
+    alike).  With ``ctl`` (control_scores on the same problem) the misses must be no more
+    frequent than the control's (count_bound) and no pair may fall further below the
+    reference than the control's worst drop (x 1.5, at least ``worst``).  Without a control
+    the measured rate is the allowance: at most 2 % of the pairs + 1 miss, none more than
+    ``worst`` below the reference (a higher score is a better optimum from the same seeds)."""
     got, ref = np.asarray(got, np.float64), np.asarray(ref, np.float64)
-    eq = np.abs(got - ref) <= TOL
-    assert eq.mean() >= frac, (eq.mean(), got - ref)
-    assert np.max(ref - got) <= worst, (got - ref)
+    miss = int(np.sum(np.abs(got - ref) > TOL))
+    drop = float(np.max(ref - got))
+    if ctl is not None:
+        ctl = np.asarray(ctl, np.float64)
+        c_miss = int(np.sum(np.abs(ctl - ref) > TOL))
+        assert miss <= count_bound(c_miss), (miss, c_miss, got - ref, ctl - ref)
+        assert drop <= max(1.5 * float(np.max(ref - ctl)), worst), (got - ref, ctl - ref)
+    else:
+        assert miss <= math.ceil(0.02 * len(got)) + 1, (miss, got - ref)
+        assert drop <= worst, (got - ref)
 
 
 def _t(a, dev, dtype=None):
@@ -48,7 +79,11 @@ def test_shape_align_matches_reference(golden, cuda):
     sc, q, t = al.coarse_fine_align_many(A, B, VAA, VBB, alpha=0.81, steps_fine=80, lr=0.1,
                                          N_real=N, M_real=M, seeds=seeds)
     sc = sc.cpu().numpy()
-    assert_parity(sc, g["shape_score"])
+    from oracle import align as oa
+    ctl = control_scores(oa.align_shape, g["shape_A"], g["shape_B"], g["shape_N"], g["shape_M"],
+                         alpha=0.81, steps=80, lr=0.1,
+                         seeds=(g["shape_seeds_q"], g["shape_seeds_t"]))
+    assert_parity(sc, g["shape_score"], ctl)
     assert (sc[:2] > 0.99).all()
 
 
@@ -87,7 +122,11 @@ def test_esp_align_matches_reference(golden, cuda):
                                              steps_fine=60, lr=0.1, N_real=N, M_real=M,
                                              seeds=seeds)
     sc = sc.cpu().numpy()
-    assert_parity(sc, g["esp_score"])
+    from oracle import align as oa
+    ctl = control_scores(oa.align_esp, g["esp_A"], g["esp_B"], g["esp_CA"], g["esp_CB"],
+                         g["esp_N"], g["esp_M"], alpha=0.81, lam=lam, steps=60, lr=0.1,
+                         seeds=(g["esp_seeds_q"], g["esp_seeds_t"]))
+    assert_parity(sc, g["esp_score"], ctl)
     assert sc[0] > 0.99
 
 
@@ -97,12 +136,13 @@ def test_pharm_align_matches_oracle(golden, cuda):
     args = [g[k] for k in ("pharm_A", "pharm_B", "pharm_RV", "pharm_FV", "pharm_At",
                            "pharm_Bt", "pharm_N", "pharm_M")]
     o_sc, _, _ = oa.align_pharm(*args, num_seeds=16, steps=150, lr=0.1)
+    c_sc = control_scores(oa.align_pharm, *args, num_seeds=16, steps=150, lr=0.1)
     A, B, RV, FV, At, Bt, N, M = [_t(a, cuda) for a in args]
     sc, q, t = al.coarse_fine_pharm_align_many(A, B, RV, FV, At, Bt, num_seeds=16,
                                                steps_fine=150, lr=0.1, N_real=N, M_real=M)
     sc = sc.cpu().numpy()
     assert sc[0] > 0.99
-    assert_parity(sc, o_sc, frac=0.6)
+    assert_parity(sc, o_sc, c_sc)
     # the returned pose reproduces the score in the ORIGINAL frames (fold-back is right)
     from oracle import scores as osc
     R = al._quat_rot(q).cpu().numpy()
@@ -141,8 +181,10 @@ def test_directional_combo_matches_oracle(cuda):
     RV, _ = _pad([m["pharm_vecs"] for m in refs]); FV, _ = _pad([m["pharm_vecs"] for m in fits])
     At, _ = _pad([m["pharm_types"] for m in refs], 8, np.int64)
     Bt, _ = _pad([m["pharm_types"] for m in fits], 8, np.int64)
-    o_sc, _, _ = oa.align_combo(A, B, N, M, PA, PB, RV, FV, At, Bt, PN, PM, alpha=0.81, w=0.5,
-                                directional=True, num_seeds=20, steps=120, lr=0.1)
+    combo_args = (A, B, N, M, PA, PB, RV, FV, At, Bt, PN, PM)
+    combo_kw = dict(alpha=0.81, w=0.5, directional=True, num_seeds=20, steps=120, lr=0.1)
+    o_sc, _, _ = oa.align_combo(*combo_args, **combo_kw)
+    c_sc = control_scores(oa.align_combo, *combo_args, **combo_kw)
     Ad, Bd, Nd, Md = _t(A, cuda), _t(B, cuda), _t(N, cuda), _t(M, cuda)
     VAA = K._batch_self_overlap(Ad, Nd, 0.81)
     VBB = K._batch_self_overlap(Bd, Md, 0.81)
@@ -153,7 +195,7 @@ def test_directional_combo_matches_oracle(cuda):
         M_real_pharm=_t(PM, cuda))
     sc = sc.cpu().numpy()
     assert sc[0] > 0.99
-    assert_parity(sc, o_sc, frac=0.5)
+    assert_parity(sc, o_sc, c_sc)
 
 
 @pytest.mark.parametrize("lpp", [4, 8, 16, 32])

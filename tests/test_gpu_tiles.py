@@ -10,6 +10,7 @@ from fast_shepherd_score_b200 import align as al
 from fast_shepherd_score_b200 import kernels as K
 from fast_shepherd_score_b200 import synthetic as syn
 from fast_shepherd_score_b200.layout import CloudSet
+from test_gpu_align import assert_parity
 
 pytestmark = pytest.mark.gpu
 
@@ -64,7 +65,7 @@ def test_one_and_two_lanes_per_pose(cuda, mode):
         np.testing.assert_allclose(run(lpp, 1).rows[0].cpu().numpy(), base1, rtol=2e-5,
                                    atol=1e-6)
         sc = run(lpp, 40)[0].cpu().numpy()
-        assert np.mean(np.abs(sc - base) <= 1e-4) >= 0.75 and np.max(base - sc) <= 1e-3
+        assert_parity(sc, base)
 
 
 def test_one_and_two_lanes_per_pose_esp_combo(cuda):
