@@ -93,18 +93,27 @@ def tanimoto_packed(ref_pts, ref_off, fit_pts, fit_off, pair_ref, pair_fit, *, a
     return (score, ov) if return_overlaps else score
 
 
+# per device: one int32 arange and one zeros tensor, grown to the largest batch seen; a pair
+# index is a prefix view of one of them, so changing batch sizes allocate nothing new
 _IDX_CACHE: dict = {}
+_IDX_OLD: list = []
 
 
 def _pair_index(B, n_mol, device):
-    """Cached int32 molecule index of each pair: identity, or 0 for a broadcast molecule."""
-    key = (device, B, n_mol)
+    """int32 molecule index of each pair: identity, or 0 for a broadcast molecule (a view of
+    a per-device cached tensor)."""
+    key = (str(device), n_mol == B)
     t = _IDX_CACHE.get(key)
-    if t is None:
-        t = (torch.arange(B, dtype=_i32, device=device) if n_mol == B
-             else torch.zeros(B, dtype=_i32, device=device))
+    if t is None or t.numel() < B:
+        if t is not None:
+            # a captured CUDA graph may hold the old tensor's address: keep it alive (the
+            # sizes grow geometrically, so all of them together stay below twice the last)
+            _IDX_OLD.append(t)
+        n = max(B, 2 * (t.numel() if t is not None else 0))
+        t = (torch.arange(n, dtype=_i32, device=device) if n_mol == B
+             else torch.zeros(n, dtype=_i32, device=device))
         _IDX_CACHE[key] = t
-    return t
+    return t[:B]
 
 
 def _f32c(t):

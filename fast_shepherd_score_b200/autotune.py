@@ -82,7 +82,13 @@ def shape_key(device, mode: str, max_ref: int, max_fit: int, mean_fit: float, n_
             f"|s{n_starts}|p{_bucket(n_pairs)}")
 
 
-def candidates(mode: str, max_fit: int, n_starts: int):
+def candidates(mode: str, max_fit: int, n_starts: int, tensor_cores: bool = None):
+    """The tiles the tuner times.  The tensor-core options (``accumulate`` 2 and 3) are timed
+    only when ``tensor_cores`` is true (default: ``$FSS_AUTOTUNE_TC=1``): on B200 they were
+    measured slower than the FP32 lanes on every workload, so the default sweep leaves them
+    out (they stay selectable explicitly)."""
+    if tensor_cores is None:
+        tensor_cores = os.environ.get("FSS_AUTOTUNE_TC", "0") == "1"
     out = []
     variants = ((1, 2, 3, 4) if mode in ("shape", "esp") else
                 (1, 3) if mode == "esp_combo" else (0,))
@@ -113,7 +119,7 @@ def candidates(mode: str, max_fit: int, n_starts: int):
                 if ch not in (base, 2 * base) and ch <= n_starts:
                     out.append({"lanes_per_pose": lpp, "chunks": ch, "cta_per_sm": 0,
                                 "kernel_variant": var})
-    if mode in ("shape", "esp") and max_fit >= 16:
+    if tensor_cores and mode in ("shape", "esp") and max_fit >= 16:
         base = _auto_chunks(32, n_starts)
         ch4 = -(-n_starts // 4)     # one pose per warp: CTAs of 4 warps
         for acc in (2, 3):

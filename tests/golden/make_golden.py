@@ -76,9 +76,12 @@ def rotated_copy(rng, X, shift=1.0):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("FSS_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", default=os.environ.get("FSS_REFERENCE"),
+                    help="the reference source tree (default: $FSS_REFERENCE)")
     ap.add_argument("--only", default="", help="write only this fixture (e.g. pharm_ext)")
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("give the reference source tree with --reference or $FSS_REFERENCE")
     _install_stub()
     sys.path.insert(0, args.reference)
     if args.only == "pharm_ext":
