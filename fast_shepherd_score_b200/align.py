@@ -303,12 +303,17 @@ def _tuned_tile(mode, shape, ref, fit, ref_ph, fit_ph, pair_ref, pair_fit, seed_
     def run(**tile):
         align_packed(mode, **sub, **tile)
 
-    # small problems: lengthen the sample until one run takes a few ms, so launch latency and
-    # jitter do not decide the ranking (capped at the real step count)
+    # A sample that is the whole batch is tuned at the real step count: the candidate launch
+    # is then the launch itself, and per-launch costs (staging, the last wave) weigh in it as
+    # they will.  A partial sample is lengthened until a run of the library's default tile
+    # takes >= 10 ms (capped at the real step count), so launch jitter does not rank it.
     cands = autotune.candidates(mode, cs_f.max_points, S)
-    ms = autotune.time_once(run, **cands[0])   # an explicit tile: no recursive tuning
-    if ms < 3.0 and sub["steps"] < steps:
-        sub["steps"] = int(min(steps, math.ceil(sub["steps"] * 3.0 / max(ms, 1e-3))))
+    if k >= P:
+        sub["steps"] = int(steps)
+    else:
+        ms = autotune.time_once(run, accumulate=1)   # an explicit tile: no recursive tuning
+        if ms < 10.0 and sub["steps"] < steps:
+            sub["steps"] = int(min(steps, math.ceil(sub["steps"] * 10.0 / max(ms, 1e-3))))
     return autotune.tune(run, key, cands, repeats=3)
 
 

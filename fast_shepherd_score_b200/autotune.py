@@ -165,30 +165,53 @@ def time_once(run, **tile) -> float:
     return e0.elapsed_time(e1)
 
 
-def tune(run, key: str, cands, repeats: int = 2) -> dict:
-    """Time ``run(**tile)`` for each candidate tile; cache and return the fastest."""
-    best, best_ms = None, float("inf")
+def _time(run, c, repeats):
+    ms = []
+    for _ in range(repeats):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        run(**c)
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return ms
+
+
+def _tag(c) -> str:
+    acc = c.get("accumulate", 0)
+    tag = "tc" if acc == 2 else "tce" if acc == 3 else f"v{c.get('kernel_variant', 0)}:"
+    return f"{tag}{c['lanes_per_pose']}x{c['cta_per_sm']}c{c['chunks']}"
+
+
+def tune(run, key: str, cands, repeats: int = 2, finalists: int = 4,
+         final_repeats: int = 5) -> dict:
+    """Time ``run(**tile)`` for each candidate tile (best of ``repeats``), re-time the
+    ``finalists`` fastest ``final_repeats`` more times each, in turns, and cache and return
+    the one with the lowest median of those runs."""
     timings = {}
+    first = []
     for c in cands:
         try:
             run(**c)  # warm (shared-memory attribute, first-launch costs)
-            ms = []
-            for _ in range(repeats):
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record()
-                run(**c)
-                e1.record()
-                e1.synchronize()
-                ms.append(e0.elapsed_time(e1))
-            t = min(ms)
+            t = min(_time(run, c, repeats))
         except (ValueError, RuntimeError):
             continue
-        acc = c.get("accumulate", 0)
-        tag = "tc" if acc == 2 else "tce" if acc == 3 else f"v{c.get('kernel_variant', 0)}:"
-        timings[f"{tag}{c['lanes_per_pose']}x{c['cta_per_sm']}c{c['chunks']}"] = round(t, 4)
-        if t < best_ms:
-            best, best_ms = c, t
+        timings[_tag(c)] = round(t, 4)
+        first.append((t, len(first), c))
+    first.sort(key=lambda x: (x[0], x[1]))
+    best, best_ms = None, float("inf")
+    if first:
+        top = [c for _, _, c in first[:finalists]]
+        runs = {i: [] for i in range(len(top))}
+        for _ in range(final_repeats):      # in turns: slow drifts hit every finalist alike
+            for i, c in enumerate(top):
+                runs[i].extend(_time(run, c, 1))
+        for i, c in enumerate(top):
+            t = float(np.median(runs[i]))
+            timings["final:" + _tag(c)] = round(t, 4)
+            if t < best_ms:
+                best, best_ms = c, t
     if best is None:
         best = {"lanes_per_pose": 0, "chunks": 0, "cta_per_sm": 0}
     rec = dict(best)
