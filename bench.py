@@ -517,7 +517,7 @@ def comparators(wl, raw, dev, n_plain=16, n_graph=256):
     return out
 
 
-def server_bench(dev, duration=20.0, n_lib=1_000_000, load=0.6, seed=7, launch_pairs=32768,
+def server_bench(dev, duration=20.0, n_lib=1_000_000, load=0.6, seed=7, launch_pairs=8192,
                  policy="srpt"):
     """Screening server under a Poisson request stream (bounded run, rank 0).
 
@@ -1044,7 +1044,7 @@ def main(argv=None):
     ap.add_argument("--no-configs", dest="configs", action="store_false",
                     help="skip the short runs of the other workloads (the 'configs' key)")
     ap.add_argument("--server-seconds", type=float, default=20.0)
-    ap.add_argument("--server-launch-pairs", type=int, default=32768,
+    ap.add_argument("--server-launch-pairs", type=int, default=8192,
                     help="largest fused launch of the screening server (pairs)")
     ap.add_argument("--server-policy", default="srpt", choices=["srpt", "fifo"])
     ap.add_argument("--tile", default="", help="fixed tiling instead of the autotuner: "

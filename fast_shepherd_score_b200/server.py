@@ -446,7 +446,7 @@ class ScreenServer(ServeLoop):
 
     def __init__(self, library, *, mode: str = "vol_pharm", starts: int = 20, steps: int = 100,
                  lr: float = 0.1, alpha: float = 0.81, color_weight: float = 0.5,
-                 max_pairs_per_launch: int = 32768, hbm_budget_bytes: Optional[int] = None,
+                 max_pairs_per_launch: int = 8192, hbm_budget_bytes: Optional[int] = None,
                  lanes_per_pose: int = 8, max_in_flight: int = 2, slice_pairs: int = 8192,
                  ids=None, device=None, tile: Optional[dict] = None, policy: str = "srpt",
                  aging_s: float = 0.25, center_queries: bool = False):
