@@ -59,6 +59,9 @@ constexpr int kMaxThreads = 320;  // 10 warps
 //   2  4 fit points per lane, unrolled 4x, register budget of one 320-thread CTA per SM:
 //      no spills, fewer resident warps (small clouds, whose poses are tail-heavy)
 //   3  4 fit points per lane, unrolled 4x, <= 96 registers
+//   4  8 fit points per lane, unrolled 2x, register budget of one 320-thread CTA per SM: one
+//      pass over the reference cloud for every fit cloud of up to 8 x lanes-per-pose points
+//      (small molecules, whose second pass would run mostly empty register tiles)
 template <int VAR>
 struct AlignVariant;
 template <>
@@ -69,6 +72,8 @@ template <>
 struct AlignVariant<2> { static constexpr int kJB2 = 2, kUnroll = 4, kMinCtas = 1; };
 template <>
 struct AlignVariant<3> { static constexpr int kJB2 = 2, kUnroll = 4, kMinCtas = 2; };
+template <>
+struct AlignVariant<4> { static constexpr int kJB2 = 4, kUnroll = 2, kMinCtas = 1; };
 
 // ACC: where the shape/ESP sums run -- 0 FP32 lanes, 1 tensor-core value/gradient sums
 // (fss_mma.cuh), 2 tensor-core exponents (fss_tce.cuh); 1 and 2 need LPP == 32 and a mode

@@ -210,6 +210,19 @@ __device__ __forceinline__ void pose_init(PoseState& s, const float q0[4], const
   s.best = -INFINITY;
 }
 
+#ifndef FSS_TAIL_RCP
+#define FSS_TAIL_RCP 1
+#endif
+
+// x / sqrt(y) of the Adam update
+__device__ __forceinline__ float adam_ratio(float x, float y) {
+#if FSS_TAIL_RCP
+  return x * __frsqrt_rn(y);
+#else
+  return x / sqrtf(y);
+#endif
+}
+
 // Best-pose tracking (pre-update pose) + tangent-projected Adam on q, plain Adam on t,
 // quaternion renormalisation: cpu_fused.py:68-108 / shape_triton.py:253-368.
 __device__ __forceinline__ void adam_tail(PoseState& s, float score, const float gq[4],
@@ -221,33 +234,50 @@ __device__ __forceinline__ void adam_tail(PoseState& s, float score, const float
 #pragma unroll
     for (int i = 0; i < 3; ++i) s.bt[i] = s.t[i];
   }
+  // x / sqrt(y) as x * (correctly rounded 1/sqrt(y)): one rounding more than the quotient of
+  // the reference, and a fraction of the instructions of an IEEE square root and division
+  // (FSS_TAIL_RCP=0 builds the quotient form)
   const float radial = gq[0] * s.q[0] + gq[1] * s.q[1] + gq[2] * s.q[2] + gq[3] * s.q[3];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const float d = gq[i] - s.q[i] * radial;
     s.mq[i] = kBeta1 * s.mq[i] + (1.f - kBeta1) * d;
     s.vq[i] = kBeta2 * s.vq[i] + (1.f - kBeta2) * d * d;
-    s.q[i] = s.q[i] - lr * s.mq[i] / sqrtf(s.vq[i] + kAdamEps);
+    s.q[i] = s.q[i] - adam_ratio(lr * s.mq[i], s.vq[i] + kAdamEps);
   }
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
     const float d = gt[i];
     s.mt[i] = kBeta1 * s.mt[i] + (1.f - kBeta1) * d;
     s.vt[i] = kBeta2 * s.vt[i] + (1.f - kBeta2) * d * d;
-    s.t[i] = s.t[i] - lr * s.mt[i] / sqrtf(s.vt[i] + kAdamEps);
+    s.t[i] = s.t[i] - adam_ratio(lr * s.mt[i], s.vt[i] + kAdamEps);
   }
-  float qn = sqrtf(s.q[0] * s.q[0] + s.q[1] * s.q[1] + s.q[2] * s.q[2] + s.q[3] * s.q[3]);
-  qn = qn < 1e-12f ? 1e-12f : qn;
+  // renormalise: q / max(|q|, 1e-12)
+  const float n2 = s.q[0] * s.q[0] + s.q[1] * s.q[1] + s.q[2] * s.q[2] + s.q[3] * s.q[3];
+#if FSS_TAIL_RCP
+  const float inv = __frsqrt_rn(fmaxf(n2, 1e-24f));
+#pragma unroll
+  for (int i = 0; i < 4; ++i) s.q[i] = s.q[i] * inv;
+#else
+  const float qn = fmaxf(sqrtf(n2), 1e-12f);
 #pragma unroll
   for (int i = 0; i < 4; ++i) s.q[i] = s.q[i] / qn;
+#endif
 }
 
-// Tanimoto score V/(U-V) and its derivative scale U/(U-V)^2 (cpu_fused.py:62-67).
+// Tanimoto score V/(U-V) and its derivative scale U/(U-V)^2 (cpu_fused.py:62-67), from one
+// correctly rounded reciprocal of the denominator.
 __device__ __forceinline__ void tanimoto(float V, float U, float& score, float& scale) {
   float denom = U - V;
   if (denom == 0.f) denom = 1e-12f;
+#if FSS_TAIL_RCP
+  const float r = __frcp_rn(denom);
+  score = V * r;
+  scale = (U * r) * r;
+#else
   score = V / denom;
   scale = U / (denom * denom);
+#endif
 }
 
 // Single-channel step: score, best tracking and Adam from the channel's reduced sums.

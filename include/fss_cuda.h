@@ -172,7 +172,8 @@ typedef struct fss_align_desc {
                               * points per lane, 2 CTAs/SM register budget), 2 wide (6 fit
                               * points per lane, deeper unroll), 3 roomy (4 fit points, one
                               * CTA/SM register budget), 4 unrolled (4 fit points, 4x unroll,
-                              * 2 CTAs/SM budget); 2-4 for modes SHAPE and ESP, 3 also for
+                              * 2 CTAs/SM budget), 5 small-molecule tile (8 fit points, one
+                              * CTA/SM budget); 2-5 for modes SHAPE and ESP, 3 also for
                               * ESP_COMBO */
   int32_t pharm_extended;    /* mode PHARM: 0 cosine-weighted directional features, 1 extended
                               * points (anchor + unit vector) plus anchors, 2 extended points
