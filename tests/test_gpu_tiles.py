@@ -15,8 +15,9 @@ from test_gpu_align import assert_parity
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("variant", [4, 6])
 @pytest.mark.parametrize("mode", ["esp", "shape"])
-def test_rows_independent_of_cta_size(cuda, mode):
+def test_rows_independent_of_cta_size(cuda, mode, variant):
     refs, fits = syn.esp_surface_pairs(16, seed=41, lo=80, hi=160)
     ref = CloudSet.from_arrays([p for p, _ in refs], [c for _, c in refs], device=cuda)
     fit = CloudSet.from_arrays([p for p, _ in fits], [c for _, c in fits], device=cuda)
@@ -27,7 +28,7 @@ def test_rows_independent_of_cta_size(cuda, mode):
     st[:, ::3] += torch.tensor([11.0, 0.0, 0.0], device=cuda)
     kw = dict(ref=ref, fit=fit, pair_ref=idx, pair_fit=idx, seed_q=sq, seed_t=st, steps=30,
               lr=0.1, lam=0.3 * al.LAM_SCALING if mode == "esp" else None, lanes_per_pose=16,
-              kernel_variant=4)
+              kernel_variant=variant)
     rows = [tuple(x.cpu().numpy() for x in al.align_packed(mode, chunks=c, **kw).rows)
             for c in (25, 17, 13, 7, 5)]
     for other in rows[1:]:
