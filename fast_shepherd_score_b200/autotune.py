@@ -11,8 +11,7 @@ Tunables of one launch (``fss_align_desc``):
                   32 lanes per pose)
   kernel_variant  code variant of the FP32-lane loop (shape/ESP modes): 1 base, 2 wide
                   register tile, 3 one-CTA/SM register budget, 4 base tile unrolled 4x,
-                  5 eight-point register tile (small molecules), 6 software-pipelined
-                  reference loop
+                  5 eight-point register tile (small molecules)
 
 For a new problem shape the tuner times each candidate on a sample of the batch's pairs
 (the costliest and a spread of the rest) for a few Adam steps, with CUDA events, and keeps
@@ -94,8 +93,8 @@ def candidates(mode: str, max_fit: int, n_starts: int, tensor_cores: bool = None
     out = []
     # variant 5 (8 fit points per lane) only where it saves a pass over the reference cloud:
     # fit clouds of at most 8 x 8 lanes' points
-    variants = ((1, 2, 3, 4, 5, 6) if mode in ("shape", "esp") and max_fit <= 64 else
-                (1, 2, 3, 4, 6) if mode in ("shape", "esp") else
+    variants = ((1, 2, 3, 4, 5) if mode in ("shape", "esp") and max_fit <= 64 else
+                (1, 2, 3, 4) if mode in ("shape", "esp") else
                 (1, 3) if mode == "esp_combo" else (0,))
     for lpp in LANES:
         if mode != "pharm" and lpp > 4 and lpp // 2 >= max(max_fit, 1):

@@ -203,10 +203,10 @@ int align_launch(const fss_align_desc* d, cudaStream_t st) {
                                       "mode PHARM, tversky_sigma in [0, 1])");
   if (tc && d->lanes_per_pose != 0 && d->lanes_per_pose != 32)
     return set_error(FSS_ERR_INVALID, "fss_align: tensor-core sums use 32 lanes per pose");
-  if (d->kernel_variant < 0 || d->kernel_variant > 6 ||
+  if (d->kernel_variant < 0 || d->kernel_variant > 5 ||
       (pharm && d->kernel_variant > 1) ||
       (combo && (d->kernel_variant == 2 || d->kernel_variant >= 4)))
-    return set_error(FSS_ERR_INVALID, "fss_align: kernel_variant must be 0..6 (0 or 1 for "
+    return set_error(FSS_ERR_INVALID, "fss_align: kernel_variant must be 0..5 (0 or 1 for "
                                       "modes with a pharmacophore channel, 0, 1 or 3 for "
                                       "ESP_COMBO)");
   // automatic code variant: wide register tile for large clouds, roomy registers for small

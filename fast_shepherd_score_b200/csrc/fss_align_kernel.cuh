@@ -62,23 +62,18 @@ constexpr int kMaxThreads = 320;  // 10 warps
 //   4  8 fit points per lane, unrolled 2x, register budget of one 320-thread CTA per SM: one
 //      pass over the reference cloud for every fit cloud of up to 8 x lanes-per-pose points
 //      (small molecules, whose second pass would run mostly empty register tiles)
-//   5  4 fit points per lane, software-pipelined loop over the reference points (the next
-//      point's exponents formed while this point's ex2 results are accumulated), unrolled
-//      2x, one-CTA/SM register budget
 template <int VAR>
 struct AlignVariant;
 template <>
-struct AlignVariant<0> { static constexpr int kJB2 = 2, kUnroll = 2, kMinCtas = 2; static constexpr bool kPipe = false; };
+struct AlignVariant<0> { static constexpr int kJB2 = 2, kUnroll = 2, kMinCtas = 2; };
 template <>
-struct AlignVariant<1> { static constexpr int kJB2 = 3, kUnroll = 4, kMinCtas = 2; static constexpr bool kPipe = false; };
+struct AlignVariant<1> { static constexpr int kJB2 = 3, kUnroll = 4, kMinCtas = 2; };
 template <>
-struct AlignVariant<2> { static constexpr int kJB2 = 2, kUnroll = 4, kMinCtas = 1; static constexpr bool kPipe = false; };
+struct AlignVariant<2> { static constexpr int kJB2 = 2, kUnroll = 4, kMinCtas = 1; };
 template <>
-struct AlignVariant<3> { static constexpr int kJB2 = 2, kUnroll = 4, kMinCtas = 2; static constexpr bool kPipe = false; };
+struct AlignVariant<3> { static constexpr int kJB2 = 2, kUnroll = 4, kMinCtas = 2; };
 template <>
-struct AlignVariant<4> { static constexpr int kJB2 = 4, kUnroll = 2, kMinCtas = 1; static constexpr bool kPipe = false; };
-template <>
-struct AlignVariant<5> { static constexpr int kJB2 = 2, kUnroll = 2, kMinCtas = 1; static constexpr bool kPipe = true; };
+struct AlignVariant<4> { static constexpr int kJB2 = 4, kUnroll = 2, kMinCtas = 1; };
 
 // ACC: where the shape/ESP sums run -- 0 FP32 lanes, 1 tensor-core value/gradient sums
 // (fss_mma.cuh), 2 tensor-core exponents (fss_tce.cuh); 1 and 2 need LPP == 32 and a mode
@@ -237,7 +232,7 @@ __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
             shape_pose_tce<kEsp>(tce_ref(sP, nbMax), sB, N, M, lane, R, s.t[0], s.t[1], s.t[2],
                                  p.k, p.e, p.inv2k, ms);
           else
-            shape_pose<LPP, kEsp, V::kJB2, V::kUnroll, V::kPipe>(sP, sQc, sB, N, M, lane, R, s.t[0],
+            shape_pose<LPP, kEsp, V::kJB2, V::kUnroll>(sP, sQc, sB, N, M, lane, R, s.t[0],
                                                        s.t[1], s.t[2], p.k, p.e, p.inv2k, ms);
           rs.from(ms, s.q);
           rs.template group_sum<LPP>();

@@ -13,8 +13,7 @@ int launch_align_shape(int lpp, int acc, int var, const AlignParams& prm, int th
     case 2: return dispatch_lanes<FSS_MODE_SHAPE, 2>(lpp, prm, threads, cps, smem, st);
     case 3: return dispatch_lanes<FSS_MODE_SHAPE, 3>(lpp, prm, threads, cps, smem, st);
     case 4: return dispatch_lanes<FSS_MODE_SHAPE, 4>(lpp, prm, threads, cps, smem, st);
-    case 5: return dispatch_lanes<FSS_MODE_SHAPE, 5>(lpp, prm, threads, cps, smem, st);
-    default: return set_error(FSS_ERR_INVALID, "fss_align: kernel_variant must be 0..6");
+    default: return set_error(FSS_ERR_INVALID, "fss_align: kernel_variant must be 0..5");
   }
 }
 

@@ -478,7 +478,7 @@ __device__ __forceinline__ void shape_chunk_plain(const float4* __restrict__ sPd
 
 // Packed chunk: JB2 float2 pairs = 2*JB2 fit points per lane, f32x2 arithmetic, factored
 // exponent.  Returns false (and does nothing) when the factored form could overflow.
-template <int JB2, bool ESP, int UNR, bool PIPE = false>
+template <int JB2, bool ESP, int UNR>
 __device__ __forceinline__ bool shape_chunk_packed(const float4* __restrict__ sPd,
                                                    const float2* __restrict__ sQd,
                                                    const float4* __restrict__ sB, int N, int M,
@@ -511,65 +511,21 @@ __device__ __forceinline__ bool shape_chunk_packed(const float4* __restrict__ sP
   const unsigned own = stride >= 32 ? 0xffffffffu
                                     : ((1u << stride) - 1u) << ((threadIdx.x & 31) & ~(stride - 1));
   if (vote & own) return false;
-  if constexpr (PIPE) {
-    // Software pipeline over the reference points: the exponents of point i + 1 are formed
-    // while the ex2 results of point i are accumulated, so each stretch of the instruction
-    // stream mixes MUFU and FMA work instead of issuing them in bursts.  Same arithmetic, same
-    // order of every sum as the plain loop below.
-    if (N > 0) {
-      float4 a = sPd[0], c = sPd[1];
-      float2 PX = f2(a.x, a.y), PY = f2(a.z, a.w), PZ = f2(c.x, c.y), PW = f2(c.z, c.w);
-      float2 QC = f2(0.f, 0.f);
-      if (ESP) QC = sQd[0];
-      float2 E[JB2];
-#pragma unroll
-      for (int v = 0; v < JB2; ++v) {
-        E[v] = __ffma2_rn(PX, bx[v], __ffma2_rn(PY, by[v], __ffma2_rn(PZ, bz[v], PW)));
-        if (ESP) E[v] = __ffma2_rn(QC, cj[v], E[v]);
-      }
 #pragma unroll UNR
-      for (int i = 0; i < N; ++i) {
-        const int in = i + 1 < N ? i + 1 : i;   // the last point re-reads itself
-        const float4 an = sPd[2 * in], cn = sPd[2 * in + 1];
-        const float2 PXn = f2(an.x, an.y), PYn = f2(an.z, an.w), PZn = f2(cn.x, cn.y),
-                     PWn = f2(cn.z, cn.w);
-        float2 QCn = f2(0.f, 0.f);
-        if (ESP) QCn = sQd[in];
-        float2 g[JB2];
+  for (int i = 0; i < N; ++i) {
+    const float4 a = sPd[2 * i], c = sPd[2 * i + 1];
+    const float2 PX = f2(a.x, a.y), PY = f2(a.z, a.w), PZ = f2(c.x, c.y), PW = f2(c.z, c.w);
+    float2 QC;
+    if (ESP) QC = sQd[i];
 #pragma unroll
-        for (int v = 0; v < JB2; ++v) g[v] = f2(ex2(E[v].x), ex2(E[v].y));
-#pragma unroll
-        for (int v = 0; v < JB2; ++v) {
-          E[v] = __ffma2_rn(PXn, bx[v], __ffma2_rn(PYn, by[v], __ffma2_rn(PZn, bz[v], PWn)));
-          if (ESP) E[v] = __ffma2_rn(QCn, cj[v], E[v]);
-        }
-#pragma unroll
-        for (int v = 0; v < JB2; ++v) {
-          sg[v] = __fadd2_rn(sg[v], g[v]);
-          sx[v] = __ffma2_rn(g[v], PX, sx[v]);
-          sy[v] = __ffma2_rn(g[v], PY, sy[v]);
-          sz[v] = __ffma2_rn(g[v], PZ, sz[v]);
-        }
-        PX = PXn; PY = PYn; PZ = PZn;
-      }
-    }
-  } else {
-#pragma unroll UNR
-    for (int i = 0; i < N; ++i) {
-      const float4 a = sPd[2 * i], c = sPd[2 * i + 1];
-      const float2 PX = f2(a.x, a.y), PY = f2(a.z, a.w), PZ = f2(c.x, c.y), PW = f2(c.z, c.w);
-      float2 QC;
-      if (ESP) QC = sQd[i];
-#pragma unroll
-      for (int v = 0; v < JB2; ++v) {
-        float2 E = __ffma2_rn(PX, bx[v], __ffma2_rn(PY, by[v], __ffma2_rn(PZ, bz[v], PW)));
-        if (ESP) E = __ffma2_rn(QC, cj[v], E);
-        const float2 g = f2(ex2(E.x), ex2(E.y));
-        sg[v] = __fadd2_rn(sg[v], g);
-        sx[v] = __ffma2_rn(g, PX, sx[v]);
-        sy[v] = __ffma2_rn(g, PY, sy[v]);
-        sz[v] = __ffma2_rn(g, PZ, sz[v]);
-      }
+    for (int v = 0; v < JB2; ++v) {
+      float2 E = __ffma2_rn(PX, bx[v], __ffma2_rn(PY, by[v], __ffma2_rn(PZ, bz[v], PW)));
+      if (ESP) E = __ffma2_rn(QC, cj[v], E);
+      const float2 g = f2(ex2(E.x), ex2(E.y));
+      sg[v] = __fadd2_rn(sg[v], g);
+      sx[v] = __ffma2_rn(g, PX, sx[v]);
+      sy[v] = __ffma2_rn(g, PY, sy[v]);
+      sz[v] = __ffma2_rn(g, PZ, sz[v]);
     }
   }
 #pragma unroll
@@ -597,14 +553,14 @@ __device__ __forceinline__ bool shape_chunk_packed(const float4* __restrict__ sP
   return true;
 }
 
-template <int JB2, bool ESP, int UNR, bool PIPE = false>
+template <int JB2, bool ESP, int UNR>
 __device__ __forceinline__ void shape_chunk(const float4* __restrict__ sPd,
                                             const float2* __restrict__ sQd,
                                             const float4* __restrict__ sB, int N, int M, int j0,
                                             int stride, const Rot& R, float tx, float ty,
                                             float tz, float k, float e, float inv2k,
                                             Moments& acc) {
-  if (!shape_chunk_packed<JB2, ESP, UNR, PIPE>(sPd, sQd, sB, N, M, j0, stride, R, tx, ty, tz, k, e, inv2k,
+  if (!shape_chunk_packed<JB2, ESP, UNR>(sPd, sQd, sB, N, M, j0, stride, R, tx, ty, tz, k, e, inv2k,
                                     acc))
     shape_chunk_plain<2 * JB2, ESP>(sPd, sQd, sB, N, M, j0, stride, R, tx, ty, tz, k, e, inv2k,
                                     acc);
@@ -612,7 +568,7 @@ __device__ __forceinline__ void shape_chunk(const float4* __restrict__ sPd,
 
 // JB2: float2 pairs of fit points per lane per pass (register tile, 2*JB2 points);
 // UNR: unroll depth of the loop over reference points.
-template <int LPP, bool ESP, int JB2 = 2, int UNR = 2, bool PIPE = false>
+template <int LPP, bool ESP, int JB2 = 2, int UNR = 2>
 __device__ __forceinline__ void shape_pose(const float4* __restrict__ sPd,
                                            const float2* __restrict__ sQd,
                                            const float4* __restrict__ sB, int N, int M, int lane,
@@ -623,21 +579,21 @@ __device__ __forceinline__ void shape_pose(const float4* __restrict__ sPd,
   // the warp, which share one pair) runs the same loop; points past M are masked.
   int base = 0;
   for (; base + 2 * JB2 * LPP <= M; base += 2 * JB2 * LPP)
-    shape_chunk<JB2, ESP, UNR, PIPE>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k,
+    shape_chunk<JB2, ESP, UNR>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k,
                                acc);
   // 0..2*JB2 points are left for the group's lane 0: finish with the smallest tile
   const int pairs = ((M - base + LPP - 1) / LPP + 1) / 2;
   if (JB2 >= 4 && pairs == 4) {
-    shape_chunk<(JB2 >= 4 ? 4 : 1), ESP, UNR, PIPE>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty,
+    shape_chunk<(JB2 >= 4 ? 4 : 1), ESP, UNR>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty,
                                               tz, k, e, inv2k, acc);
   } else if (JB2 >= 3 && pairs == 3) {
-    shape_chunk<(JB2 >= 3 ? 3 : 1), ESP, UNR, PIPE>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty,
+    shape_chunk<(JB2 >= 3 ? 3 : 1), ESP, UNR>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty,
                                               tz, k, e, inv2k, acc);
   } else if (pairs == 2) {
-    shape_chunk<2, ESP, UNR, PIPE>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k,
+    shape_chunk<2, ESP, UNR>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k,
                              acc);
   } else if (pairs == 1) {
-    shape_chunk<1, ESP, UNR, PIPE>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k,
+    shape_chunk<1, ESP, UNR>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k,
                              acc);
   }
 }

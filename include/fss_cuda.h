@@ -173,9 +173,8 @@ typedef struct fss_align_desc {
                               * points per lane, deeper unroll), 3 roomy (4 fit points, one
                               * CTA/SM register budget), 4 unrolled (4 fit points, 4x unroll,
                               * 2 CTAs/SM budget), 5 small-molecule tile (8 fit points, one
-                              * CTA/SM budget), 6 software-pipelined reference loop (4 fit
-                              * points, one CTA/SM budget); 2-6 for modes SHAPE and ESP, 3 also
-                              * for ESP_COMBO */
+                              * CTA/SM budget); 2-5 for modes SHAPE and ESP, 3 also for
+                              * ESP_COMBO */
   int32_t pharm_extended;    /* mode PHARM: 0 cosine-weighted directional features, 1 extended
                               * points (anchor + unit vector) plus anchors, 2 extended points
                               * only (extended_points / only_extended of
