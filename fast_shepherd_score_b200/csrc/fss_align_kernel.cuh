@@ -118,6 +118,7 @@ __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
   float2* sRB2 = sRA2 + p.maxNa;
   __shared__ float red[96];
   __shared__ int s_item;
+  __shared__ int s_toff[10];   // first reference pharmacophore of each type
 
   const int tid = threadIdx.x;
   const int grp = tid / LPP, lane = tid % LPP;
@@ -194,7 +195,8 @@ __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
     }
     if (kPharm) {
       if (!kShape) c = block_centroid(p.ref_anc + rp0, Np, red);
-      stage_ref_pharm(p.ref_anc + rp0, p.ref_vec ? p.ref_vec + rp0 : nullptr, Np, c, sRA, sRV);
+      stage_ref_pharm(p.ref_anc + rp0, p.ref_vec ? p.ref_vec + rp0 : nullptr, Np, c, sRA, sRV,
+                      s_toff);
       stage_fit_pharm(Pts(p.fit_anc, p.fit_f16) + fp0, Pts(p.fit_vec, p.fit_f16) + fp0, Mp, sFA,
                       sFV);
     }
@@ -242,7 +244,7 @@ __global__ void __launch_bounds__(kMaxThreads, AlignVariant<VAR>::kMinCtas)
           Moments mc;
           mc.zero();
           pharm_pose<LPP, EXT>(sRA, sRV, sFA, sFV, Np, Mp, lane, R, s.t[0], s.t[1], s.t[2], p.tab,
-                          mc);
+                               mc, s_toff);
           Reduced rc;
           rc.from(mc, s.q);
           rc.template group_sum<LPP>();

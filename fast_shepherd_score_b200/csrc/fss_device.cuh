@@ -622,7 +622,8 @@ __device__ __forceinline__ void pharm_pose(const float4* __restrict__ sRA,
                                            const float4* __restrict__ sFA,
                                            const float4* __restrict__ sFV, int N, int M,
                                            int lane, const Rot& R, float tx, float ty, float tz,
-                                           const PharmTables& tab, Moments& acc) {
+                                           const PharmTables& tab, Moments& acc,
+                                           const int* __restrict__ toff = nullptr) {
   for (int j = lane; j < M; j += LPP) {
     const float4 fa = sFA[j];
     const int ityp = __float_as_int(fa.w);
@@ -637,7 +638,9 @@ __device__ __forceinline__ void pharm_pose(const float4* __restrict__ sRA,
     const bool ext = EXT != 0 && (ityp == 0 || ityp == 1);  // acceptor, donor
     float fx = 0.f, fy = 0.f, fz = 0.f, wx = 0.f, wy = 0.f, wz = 0.f, o = 0.f;
     float ex = 0.f, ey = 0.f, ez = 0.f;  // force at the extended point (EXT)
-    for (int i = 0; i < N; ++i) {
+    // reference features grouped by type (stage_ref_pharm with toff): only this type's range
+    const int i0 = toff ? toff[ityp] : 0, i1 = toff ? toff[ityp + 1] : N;
+    for (int i = i0; i < i1; ++i) {
       const float4 ra = sRA[i];
       if (__float_as_int(ra.w) != ityp) continue;
       const float dx = ra.x - ax, dy = ra.y - ay, dz = ra.z - az;  // ref - rotfit

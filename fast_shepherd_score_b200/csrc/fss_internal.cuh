@@ -123,17 +123,39 @@ __device__ __forceinline__ float clamp_type(float w) {
   return __int_as_float((t < 0 || t > 8) ? 8 : t);
 }
 
-// Reference pharmacophores: anchors centred on c (type bits kept), unit vectors.
+// Reference pharmacophores: anchors centred on c (type bits kept), unit vectors.  With `toff`
+// the features are stored grouped by type -- a stable counting sort, so the features of one
+// type keep their order -- and toff[t] is the first feature of type t (toff[9] = n): the typed
+// overlap then visits only a fit feature's same-type reference features, in the order of the
+// ungrouped loop, so its sums are unchanged.
 __device__ __forceinline__ void stage_ref_pharm(const Pts ga, const Pts gv, int n, float3 c,
-                                                float4* sA, float4* sV) {
+                                                float4* sA, float4* sV, int* toff = nullptr) {
+  auto type_of = [&](int j) { return __float_as_int(clamp_type(ga.anchor(j).w)); };
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     const float4 a = ga.anchor(i);
-    sA[i] = make_float4(a.x - c.x, a.y - c.y, a.z - c.z, clamp_type(a.w));
+    const float tw = clamp_type(a.w);
+    int pos = i;
+    if (toff) {
+      const int t = __float_as_int(tw);
+      pos = 0;
+      for (int j = 0; j < n; ++j) {
+        const int u = type_of(j);
+        pos += (u < t || (u == t && j < i)) ? 1 : 0;
+      }
+    }
+    sA[pos] = make_float4(a.x - c.x, a.y - c.y, a.z - c.z, tw);
     if (gv) {
       const float4 v = gv[i];
-      sV[i] = unit4(v.x, v.y, v.z);
+      sV[pos] = unit4(v.x, v.y, v.z);
     } else {
-      sV[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+      sV[pos] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  }
+  if (toff) {
+    for (int t = threadIdx.x; t < 10; t += blockDim.x) {
+      int below = 0;
+      for (int j = 0; j < n; ++j) below += type_of(j) < t ? 1 : 0;
+      toff[t] = below;
     }
   }
 }
