@@ -87,6 +87,13 @@ def dist_env():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
+def e2e_count(warm_ms: float) -> int:
+    """Timed end-to-end calls after the warm-up: at least 3, and for short calls enough to
+    span about a second (at most 21), so that host jitter on a shared machine does not decide
+    a millisecond-scale median."""
+    return max(3, min(21, int(1000.0 / max(warm_ms, 1e-3))))
+
+
 def make_inputs(wl, n_pairs, seed):
     from fast_shepherd_score_b200 import synthetic as syn
     from fast_shepherd_score_b200.api import HostBatch
@@ -315,17 +322,22 @@ def run_cuda(args, wl):
         raise RuntimeError(f"kernel status flags {status}")
 
     # ---- end to end through the host-array API ----------------------------------------
-    e2e_ms = []
     h2d = ref_h.nbytes + fit_h.nbytes + 2 * 4 * n_pairs
     d2h = n_pairs * 8 * 4
-    for i in range((max(1, min(args.steps, 3)) + 1) if args.e2e else 0):
+
+    def e2e_call():
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
-        out = api.align_host(mode, ref_h, fit_h, alpha=wl["alpha"], lam=wl["lam"],
+        res = api.align_host(mode, ref_h, fit_h, alpha=wl["alpha"], lam=wl["lam"],
                              num_seeds=S, steps=wl["steps"], lr=wl["lr"], device=dev)
-        t1 = time.perf_counter()
-        if i:   # first call is a warm-up
-            e2e_ms.append((t1 - t0) * 1e3)
+        return res, (time.perf_counter() - t0) * 1e3
+
+    e2e_ms = []
+    if args.e2e:
+        out, warm_ms = e2e_call()   # warm-up
+        for _ in range(e2e_count(warm_ms)):
+            out, ms = e2e_call()
+            e2e_ms.append(ms)
     e2e_t = torch.tensor([statistics.median(e2e_ms) if e2e_ms else float("nan")], device=dev,
                          dtype=torch.float64)
     if world > 1:
@@ -859,19 +871,25 @@ def run_esp_combo(args, wl):
 
     # end to end: pinned host arrays -> device sets -> align -> scores/poses on the host
     e2e_ms, h2d = [], 0
-    for i in range((max(1, min(args.steps, 3)) + 1) if args.e2e else 0):
+
+    def e2e_call():
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
         r4 = to_dev(host_r)
         f4 = to_dev(host_f)
         sc, q, t = step(r4[0], f4[0], r4[1], f4[1], r4[2], f4[2], r4[3], f4[3])
-        host = torch.cat([sc[:, None], q, t], 1).cpu()
-        t1 = time.perf_counter()
-        if i:
-            e2e_ms.append((t1 - t0) * 1e3)
-        h2d = sum(x.pts.nbytes + x.off.nbytes
-                  for x in (r4[0], r4[1], r4[3], f4[0], f4[1], f4[3])) + \
+        torch.cat([sc[:, None], q, t], 1).cpu()
+        ms = (time.perf_counter() - t0) * 1e3
+        nb = sum(x.pts.nbytes + x.off.nbytes
+                 for x in (r4[0], r4[1], r4[3], f4[0], f4[1], f4[3])) + \
             r4[2].nbytes + f4[2].nbytes
+        return nb, ms
+
+    if args.e2e:
+        h2d, warm_ms = e2e_call()   # warm-up
+        for _ in range(e2e_count(warm_ms)):
+            h2d, ms = e2e_call()
+            e2e_ms.append(ms)
     e2e_t = torch.tensor([statistics.median(e2e_ms) if e2e_ms else float("nan")], device=dev,
                          dtype=torch.float64)
     if world > 1:
