@@ -109,3 +109,67 @@ def test_tversky_rejected_outside_pharm(cuda):
     with pytest.raises(ValueError):
         al.align_packed("shape", ref=ref, fit=ref, pair_ref=idx, pair_fit=idx, seed_q=sq,
                         seed_t=st, steps=1, lr=0.1, similarity="tversky")
+
+
+def test_interleaved_and_out_of_range_types_track_oracle(cuda):
+    """The fused kernel stages the reference features grouped by type and visits only a fit
+    feature's own type; features whose types are interleaved, repeated or out of the 9-entry
+    table (read as Dummy) give the oracle's rows after 1 and 3 steps, in the pharmacophore
+    and the shape + pharmacophore modes."""
+    from oracle import align as oa
+    from fast_shepherd_score_b200 import synthetic as syn
+    rng = np.random.default_rng(17)
+    refs, fits = syn.shape_pharm_pairs(12, seed=17)
+    pool = np.array([-1, 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 12])
+    for m in refs + fits:
+        m["pharm_types"] = rng.choice(pool, size=len(m["pharm_types"])).astype(np.int64)
+    g = lambda ms, k: [m[k] for m in ms]
+
+    def pad(xs, fill=0.0, dtype=np.float32):
+        n = np.array([len(x) for x in xs])
+        out = np.full((len(xs), int(n.max())) + np.asarray(xs[0]).shape[1:], fill, dtype)
+        for i, x in enumerate(xs):
+            out[i, :len(x)] = x
+        return out, n
+
+    table = lambda t: np.where((t < 0) | (t > 8), 8, t)   # out of the table reads as Dummy
+    A, N = pad(g(refs, "pharm_ancs")); B, M = pad(g(fits, "pharm_ancs"))
+    RV, _ = pad(g(refs, "pharm_vecs")); FV, _ = pad(g(fits, "pharm_vecs"))
+    At, _ = pad([table(t) for t in g(refs, "pharm_types")], 8, np.int64)
+    Bt, _ = pad([table(t) for t in g(fits, "pharm_types")], 8, np.int64)
+    mk = lambda ms: PharmSet.from_arrays(g(ms, "pharm_types"), g(ms, "pharm_ancs"),
+                                         g(ms, "pharm_vecs"), device=cuda)
+    ref_ph, fit_ph = mk(refs), mk(fits)
+    idx = torch.arange(12, dtype=torch.int32, device=cuda)
+    # pharmacophore mode: seeds of the centred anchors, as the driver takes them
+    _, Ac = oa.center_anchors(A, N)
+    _, Bc = oa.center_anchors(B, M)
+    sq, st = K.seeds(CloudSet.from_padded(_t(Ac, cuda), _t(N, cuda)),
+                     CloudSet.from_padded(_t(Bc, cuda), _t(M, cuda)), idx, idx, 12)
+    seeds = (sq.cpu().numpy(), st.cpu().numpy())
+    # the raw types (out-of-table ones included) go to the device; the set reads them as Dummy
+    rawt = lambda ms: pad(g(ms, "pharm_types"), 8, np.int64)[0]
+    rph = PharmSet.from_padded(_t(Ac, cuda), _t(rawt(refs), cuda), _t(RV, cuda), _t(N, cuda))
+    fph = PharmSet.from_padded(_t(Bc, cuda), _t(rawt(fits), cuda), _t(FV, cuda), _t(M, cuda))
+    for steps in (1, 3):
+        tol = dict(rtol=2e-5, atol=1e-6) if steps == 1 else dict(rtol=0, atol=5e-5)
+        *_, (best, _, _) = oa.align_pharm(A, B, RV, FV, At, Bt, N, M, seeds=seeds, steps=steps,
+                                          lr=0.1, return_rows=True)
+        res = al.align_packed("pharm", ref_ph=rph, fit_ph=fph, pair_ref=idx, pair_fit=idx,
+                              seed_q=sq, seed_t=st, steps=steps, lr=0.1)
+        np.testing.assert_allclose(res.rows[0].cpu().numpy(), best, **tol)
+    # shape + pharmacophore (the clouds' own frames, seeds on the atoms)
+    X, XN = pad(g(refs, "atom_pos")); Y, YM = pad(g(fits, "atom_pos"))
+    ref = CloudSet.from_arrays(g(refs, "atom_pos"), device=cuda)
+    fit = CloudSet.from_arrays(g(fits, "atom_pos"), device=cuda)
+    sq, st = K.seeds(ref, fit, idx, idx, 12)
+    seeds = (sq.cpu().numpy(), st.cpu().numpy())
+    for steps in (1, 3):
+        tol = dict(rtol=2e-5, atol=1e-6) if steps == 1 else dict(rtol=0, atol=5e-5)
+        *_, (best, _, _) = oa.align_combo(X, Y, XN, YM, A, B, RV, FV, At, Bt, N, M, alpha=0.81,
+                                          w=0.5, directional=True, steps=steps, lr=0.1,
+                                          seeds=seeds, return_rows=True)
+        res = al.align_packed("shape_pharm", ref=ref, fit=fit, ref_ph=ref_ph, fit_ph=fit_ph,
+                              pair_ref=idx, pair_fit=idx, seed_q=sq, seed_t=st, steps=steps,
+                              lr=0.1, alpha=0.81, color_weight=0.5)
+        np.testing.assert_allclose(res.rows[0].cpu().numpy(), best, **tol)
