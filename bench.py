@@ -1086,11 +1086,16 @@ def main(argv=None):
         if line is not None:
             print(json.dumps(line), flush=True)
         return line
-    world, rank, _ = dist_env()
+    world, rank, local = dist_env()
     if world > 1:
         import datetime
+        import torch
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        # this rank's GPU before the process group exists, so NCCL binds its communicator
+        # (and every barrier) to it
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
     try:
         line = run_workload(args, wl)
         if line is not None and args.configs and world == 1:
