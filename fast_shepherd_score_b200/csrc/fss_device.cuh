@@ -425,6 +425,12 @@ __device__ __forceinline__ void step_combo(PoseState& s, const Reduced& ms, floa
 // ---------------------------------------------------------------------------------------
 constexpr float kFactorMax = 96.f;
 
+// An odd last fit point per lane goes to a one-point scalar chunk instead of a half-empty
+// packed pair (0 keeps the packed pair).
+#ifndef FSS_PLAIN_TAIL
+#define FSS_PLAIN_TAIL 1
+#endif
+
 
 template <int JB, bool ESP>
 __device__ __forceinline__ void shape_chunk_plain(const float4* __restrict__ sPd,
@@ -581,8 +587,11 @@ __device__ __forceinline__ void shape_pose(const float4* __restrict__ sPd,
   for (; base + 2 * JB2 * LPP <= M; base += 2 * JB2 * LPP)
     shape_chunk<JB2, ESP, UNR>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k,
                                acc);
-  // 0..2*JB2 points are left for the group's lane 0: finish with the smallest tile
-  const int pairs = ((M - base + LPP - 1) / LPP + 1) / 2;
+  // 0..2*JB2 points per lane are left: whole f32x2 pairs in the smallest packed tile that
+  // holds them, and an odd last point per lane in a scalar chunk (FSS_PLAIN_TAIL), which
+  // costs half the FP32/MUFU pipe time of a packed pair whose second slot would be empty
+  const int ppl = (M - base + LPP - 1) / LPP;
+  const int pairs = FSS_PLAIN_TAIL ? ppl / 2 : (ppl + 1) / 2;
   if (JB2 >= 4 && pairs == 4) {
     shape_chunk<(JB2 >= 4 ? 4 : 1), ESP, UNR>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty,
                                               tz, k, e, inv2k, acc);
@@ -596,6 +605,9 @@ __device__ __forceinline__ void shape_pose(const float4* __restrict__ sPd,
     shape_chunk<1, ESP, UNR>(sPd, sQd, sB, N, M, base + lane, LPP, R, tx, ty, tz, k, e, inv2k,
                              acc);
   }
+  if (FSS_PLAIN_TAIL && (ppl & 1))
+    shape_chunk_plain<1, ESP>(sPd, sQd, sB, N, M, base + lane + 2 * pairs * LPP, LPP, R, tx, ty,
+                              tz, k, e, inv2k, acc);
 }
 
 // ---------------------------------------------------------------------------------------
