@@ -279,7 +279,8 @@ def _tuned_tile(mode, shape, ref, fit, ref_ph, fit_ph, pair_ref, pair_fit, seed_
     S = int(seed_q.shape[1])
     P = int(seed_q.shape[0])
     key = autotune.shape_key(seed_q.device, mode, cs_r.max_points, cs_f.max_points,
-                             float(np.mean(cs_f.counts)) if len(cs_f.counts) else 0.0, S, P)
+                             float(np.mean(cs_f.counts)) if len(cs_f.counts) else 0.0, S, P,
+                             int(steps))
     rec = autotune.lookup(key)
     if rec is not None:
         return rec

@@ -15,8 +15,8 @@ Tunables of one launch (``fss_align_desc``):
 
 For a new problem shape the tuner times each candidate on a sample of the batch's pairs
 (the costliest and a spread of the rest) for a few Adam steps, with CUDA events, and keeps
-the fastest.  Results are cached per (device, mode, size buckets, starts) in memory and in a
-JSON file (``$FSS_AUTOTUNE_CACHE`` or ``~/.cache/fast_shepherd_score_b200/autotune.json``).
+the fastest.  Results are cached per (device, mode, size buckets, starts, pair bucket, step-count
+class) in memory and in a JSON file (``$FSS_AUTOTUNE_CACHE`` or ``~/.cache/fast_shepherd_score_b200/autotune.json``).
 Set ``FSS_AUTOTUNE=0`` to disable tuning (the library's built-in default is then used).
 """
 from __future__ import annotations
@@ -76,11 +76,17 @@ def _bucket(x: int) -> int:
     return 0 if x <= 0 else 1 << int(math.ceil(math.log2(max(int(x), 1))))
 
 
+def steps_class(steps: int) -> int:
+    """0: one step (a scoring pass), 1: up to 16 steps (launch- and tail-dominated), 2: longer
+    runs (throughput-dominated).  A tile tuned for a few steps is a poor choice for 200."""
+    return 0 if steps <= 1 else 1 if steps <= 16 else 2
+
+
 def shape_key(device, mode: str, max_ref: int, max_fit: int, mean_fit: float, n_starts: int,
-              n_pairs: int) -> str:
+              n_pairs: int, steps: int = 200) -> str:
     name = torch.cuda.get_device_name(device).replace(" ", "_")
     return (f"{name}|{mode}|r{_bucket(max_ref)}|f{_bucket(max_fit)}|m{_bucket(int(mean_fit))}"
-            f"|s{n_starts}|p{_bucket(n_pairs)}")
+            f"|s{n_starts}|p{_bucket(n_pairs)}|t{steps_class(steps)}")
 
 
 def candidates(mode: str, max_fit: int, n_starts: int, tensor_cores: bool = None):
