@@ -63,10 +63,14 @@ def align_bytes_per_pair(starts: int, grid_poses: int = 0) -> int:
     return PAIR_BYTES + starts * (ROW_BYTES + SEED_BYTES) + grid_poses * (ROW_BYTES + SEED_BYTES)
 
 
-def budget_bytes(device) -> int:
-    """``SAFETY`` x (free device memory + memory torch holds but does not use)."""
+def budget_bytes(device, need: int = 0) -> int:
+    """``SAFETY`` x (free device memory + memory torch holds but does not use).  When
+    ``SAFETY`` x the free memory alone already covers ``need`` bytes, that is returned without
+    reading torch's allocator statistics (a few hundred microseconds a call)."""
     device = torch.device(device)
     free, _ = torch.cuda.mem_get_info(device)
+    if need and SAFETY * free >= need:
+        return int(SAFETY * free)
     reusable = torch.cuda.memory_reserved(device) - torch.cuda.memory_allocated(device)
     return int(SAFETY * (free + max(0, reusable)))
 
@@ -90,7 +94,8 @@ def run_chunked(n: int, per_item_bytes: int, process: Callable[[int, int], Seque
     if n <= 0:
         return process(0, n)
     if budget is None:
-        budget = budget_bytes(device) if torch.device(device).type == "cuda" else 1 << 62
+        budget = (budget_bytes(device, n * per_item_bytes) if torch.device(device).type == "cuda"
+                  else 1 << 62)
     chunk = max(1, min(n, int(budget // max(1, per_item_bytes))))
     if max_chunk:
         chunk = max(1, min(chunk, int(max_chunk)))
