@@ -29,9 +29,13 @@ def test_headline_metric_string():
 
 @pytest.mark.timeout(600)
 def test_reference_arm_under_torchrun_prints_once(tmp_path):
+    import socket
+    with socket.socket() as sk:      # a free port for the rendezvous
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
     env = dict(os.environ, PYTHONPATH=ROOT, OMP_NUM_THREADS="2")
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2",
-           "--master-addr", "127.0.0.1", "--master-port", "29533",
+           "--master-addr", "127.0.0.1", "--master-port", str(port),
            os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
            "--workload", "vol", "--pairs", "4", "--steps", "1", "--warmup", "0",
            "--cpu-seconds", "0.5"]
