@@ -152,6 +152,16 @@ def ptr(t, dtype=None, name="tensor"):
     return t.data_ptr() if t.numel() else None
 
 
+_RAW_STREAM = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+
+
 def stream_ptr(device=None):
-    """The current torch stream of `device` as a cudaStream_t."""
+    """The current torch stream of `device` as a cudaStream_t.  Read as a raw handle when torch
+    offers it (no Stream object per call: the eager autograd path makes four such calls a
+    step), else through torch.cuda.current_stream."""
+    if _RAW_STREAM is not None:
+        idx = None
+        if device is not None:
+            idx = (device if isinstance(device, torch.device) else torch.device(device)).index
+        return _RAW_STREAM(torch.cuda.current_device() if idx is None else idx)
     return torch.cuda.current_stream(device).cuda_stream
