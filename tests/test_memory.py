@@ -85,3 +85,20 @@ def test_status_mapping():
 def test_bytes_per_pair_counts_rows_and_seeds():
     assert memory.align_bytes_per_pair(50) == memory.PAIR_BYTES + 50 * 60
     assert memory.align_bytes_per_pair(30, 605) == memory.PAIR_BYTES + 635 * 60
+
+
+def test_budget_reads_allocator_statistics_only_when_needed(monkeypatch):
+    """budget_bytes(device, need): free memory alone decides when it covers the call; the
+    memory torch caches but does not use is added only when it does not (fakes for the CUDA
+    queries, no GPU)."""
+    stats = []
+    monkeypatch.setattr(torch.cuda, "mem_get_info", lambda dev=None: (1000, 4000))
+    monkeypatch.setattr(torch.cuda, "memory_reserved", lambda dev=None: stats.append(1) or 900)
+    monkeypatch.setattr(torch.cuda, "memory_allocated", lambda dev=None: 100)
+    assert memory.budget_bytes("cuda:0", need=500) == int(memory.SAFETY * 1000)
+    assert not stats
+    assert memory.budget_bytes("cuda:0", need=5000) == int(memory.SAFETY * (1000 + 800))
+    assert stats
+    stats.clear()
+    assert memory.budget_bytes("cuda:0") == int(memory.SAFETY * 1800)   # no need given
+    assert stats
