@@ -539,7 +539,7 @@ def server_bench(dev, duration=20.0, n_lib=1_000_000, load=0.6, seed=7, launch_p
     ``launch_pairs`` pairs per fused launch, admission ``policy`` ("srpt" or "fifo")."""
     import torch
     from fast_shepherd_score_b200 import align as al, kernels as K, synthetic as syn
-    from fast_shepherd_score_b200.server import ScreenServer, latency_by_decade
+    from fast_shepherd_score_b200.server import ScreenServer, latency_by_decade, slowdown
     t0 = time.perf_counter()
     atoms, ph = syn.library_on_device(n_lib, seed, dev)
     torch.cuda.synchronize(dev)
@@ -599,6 +599,7 @@ def server_bench(dev, duration=20.0, n_lib=1_000_000, load=0.6, seed=7, launch_p
         wall = time.perf_counter() - t_start
         lat = np.array(srv.latencies[3:]) * 1e3      # drop the warm-up and capacity probes
         by_size = latency_by_decade(srv.size_latency[3:])
+        slow = slowdown(srv.size_latency[3:], cap)
         st = srv.stats()
     return {"library": n_lib, "mode": "vol_pharm (shape + directional pharmacophore)",
             "starts": 20, "adam_steps": 100, "request_pairs": "log-uniform [1e3, 1e5]",
@@ -608,7 +609,8 @@ def server_bench(dev, duration=20.0, n_lib=1_000_000, load=0.6, seed=7, launch_p
             "pairs_per_s": round((st["pairs_done"] - n_probe) / wall, 1),
             "p50_ms": round(float(np.percentile(lat, 50)), 2),
             "p99_ms": round(float(np.percentile(lat, 99)), 2),
-            "by_request_size": by_size, "policy": policy, "max_pairs_per_launch": launch_pairs,
+            "by_request_size": by_size, "slowdown": slow,
+            "policy": policy, "max_pairs_per_launch": launch_pairs,
             "max_queue_depth": st["max_queue_depth"], "tile": dict(tile, lanes_per_pose=lpp),
             "library_bytes_per_molecule": round(mol_bytes, 1),
             "library_hbm_gbs_at_capacity": round(cap * mol_bytes / 1e9, 3),

@@ -186,6 +186,25 @@ def latency_by_decade(records) -> dict:
     return out
 
 
+def slowdown(records, capacity_pairs_per_s: float) -> dict:
+    """Latency over the request's own service time at full capacity (pairs / capacity), from
+    (pairs, seconds) records: {"p50", "p99", "by_request_size": {decade: {"p50", "p99"}}}.
+    Unlike raw latency it does not grow with the request's size, so it shows how much waiting
+    the admission order adds for small and large requests alike (1 = served alone at full
+    speed)."""
+    if not records or not capacity_pairs_per_s > 0:
+        return {}
+    sd = [(n, t * capacity_pairs_per_s / max(n, 1)) for n, t in records]
+    out = {"p50": round(percentile([x for _, x in sd], 50), 2),
+           "p99": round(percentile([x for _, x in sd], 99), 2), "by_request_size": {}}
+    for lo in range(0, 9):
+        sel = [x for n, x in sd if 10 ** lo <= n < 10 ** (lo + 1)]
+        if sel:
+            out["by_request_size"][f"1e{lo}-1e{lo + 1}"] = {
+                "p50": round(percentile(sel, 50), 2), "p99": round(percentile(sel, 99), 2)}
+    return out
+
+
 class ServeLoop:
     """The scheduler: admission, continuous batching, retirement, cancellation and deadlines,
     over an engine with ``launch(slices) -> handle`` and ``wait(handle) -> (P, 8) results``

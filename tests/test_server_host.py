@@ -18,7 +18,7 @@ import torch.multiprocessing as mp
 
 from fast_shepherd_score_b200.screen import Hit
 from fast_shepherd_score_b200.server import (Planner, Request, ServeLoop, latency_by_decade,
-                                             merge_hits, merge_topk, shard_ranges)
+                                             merge_hits, merge_topk, shard_ranges, slowdown)
 
 
 def _req(rid, n, k=5, arrival=0.0):
@@ -176,6 +176,15 @@ def test_latency_by_decade():
     rec = [(1500, 0.01), (2000, 0.03), (50_000, 0.2), (99_999, 0.4)]
     d = latency_by_decade(rec)
     assert d["1e3-1e4"]["requests"] == 2 and d["1e4-1e5"]["requests"] == 2
+
+
+def test_slowdown_normalises_by_service_time():
+    # capacity 1000 pairs/s: a 2000-pair request served alone takes 2 s (slowdown 1)
+    rec = [(2000, 2.0), (2000, 4.0), (50_000, 50.0), (50_000, 150.0)]
+    d = slowdown(rec, 1000.0)
+    assert d["by_request_size"]["1e3-1e4"]["p50"] == pytest.approx(1.5)
+    assert d["by_request_size"]["1e4-1e5"]["p99"] == pytest.approx(2.98, abs=0.01)
+    assert slowdown([], 1000.0) == {} and slowdown(rec, 0.0) == {}
 
 
 def test_shard_ranges_and_merge_hits():
