@@ -154,8 +154,10 @@ def align_packed(mode: str, *, pair_ref, pair_fit, seed_q, seed_t, steps: int, l
     if shape and pharm and (ref_ph.n_mol != n_ref or fit_ph.n_mol != n_fit):
         raise ValueError("shape and pharmacophore sets must describe the same molecules")
     if P and validate:
-        lo = int(torch.minimum(pair_ref.min(), pair_fit.min()))
-        if lo < 0 or int(pair_ref.max()) >= n_ref or int(pair_fit.max()) >= n_fit:
+        # one device-to-host read for the four bounds
+        rmin, fmin, rmax, fmax = torch.stack([pair_ref.min(), pair_fit.min(), pair_ref.max(),
+                                              pair_fit.max()]).tolist()
+        if min(rmin, fmin) < 0 or rmax >= n_ref or fmax >= n_fit:
             raise ValueError("pair index outside the molecule tables")
     if shape:
         esp_self = m == _lib.MODE_ESP

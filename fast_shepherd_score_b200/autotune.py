@@ -82,9 +82,22 @@ def steps_class(steps: int) -> int:
     return 0 if steps <= 1 else 1 if steps <= 16 else 2
 
 
+_NAMES: dict = {}
+
+
+def _device_name(device) -> str:
+    """The device's name (queried once per device: every launch builds a key)."""
+    idx = torch.device(device).index
+    idx = torch.cuda.current_device() if idx is None else idx
+    name = _NAMES.get(idx)
+    if name is None:
+        name = _NAMES[idx] = torch.cuda.get_device_name(idx).replace(" ", "_")
+    return name
+
+
 def shape_key(device, mode: str, max_ref: int, max_fit: int, mean_fit: float, n_starts: int,
               n_pairs: int, steps: int = 200) -> str:
-    name = torch.cuda.get_device_name(device).replace(" ", "_")
+    name = _device_name(device)
     return (f"{name}|{mode}|r{_bucket(max_ref)}|f{_bucket(max_fit)}|m{_bucket(int(mean_fit))}"
             f"|s{n_starts}|p{_bucket(n_pairs)}|t{steps_class(steps)}")
 
